@@ -1,0 +1,151 @@
+/*
+ * sac_gpu.h -- C-ABI of the B200 perturbation-MHD hot path (libsacgpu.so).
+ *
+ * The entry points replace the Fortran call surface of the reference's hot path
+ * (drewleonard42/SAC, files cited relative to the project root):
+ *
+ *   sac_create          physini + the method part of readparameters   src/vacphys.mhd0.t:9, src/vacio.t:246-527
+ *   sac_set_grid        setixGixMix + gridsetup1 (dx, dvolume)         src/vacio.t:786-841, src/vacgrid.t:556-661
+ *   sac_set_boundaries  boundsetup (default regions, periodic pairing)  src/vacgrid.t:9-160
+ *   sac_upload          host w(ixG^T,nw) -> resident device state      (the COMMON w of program vac, src/vac.t:12)
+ *   sac_download        resident device state -> host w                (savefile, src/vacio.t:901)
+ *   sac_getboundary     getboundary(t,1,nw,1,ndim,w)                   src/vacgrid.t:195-512
+ *   sac_getdt           vac.t dt block: getdt_courant+getdt+getdt_special src/vac.t:60-70,641-699;
+ *                                                                      src/vacphys.mhd0.t:83; src/vacusr.f:1403
+ *   sac_advect          advect(method,ixG^L,iws,idim^LIM,w1,w)         src/vac.t:364-487
+ *   sac_diag            getdivb + volume means of savefilelog_default  src/vacphys.mhd0.t:106; src/vacio.t:1094
+ *
+ * Conventions
+ *   - Arrays crossing the ABI are Fortran order: w(ix1,ix2,ix3,iw), x1 fastest,
+ *     one contiguous block per variable (SoA), ixGlo=1, exactly the reference's
+ *     COMMON/stack layout (src/vacdef.t:18-23, src/vac.t:12).
+ *   - Strings are Fortran CHARACTER*10 blank-padded (no NUL) where marked
+ *     "f10"; method names may also be NUL-terminated C strings.
+ *   - Every call returns a status; nothing exits or traps.  The Fortran shim maps
+ *     a non-zero status to die() (src/vacio.t:1152).  sac_last_error() holds the text.
+ *   - One context per host thread; a context is not re-entrant.
+ *   - The state stays resident on the device between calls; w1/w2/w3 of the
+ *     reference's advect are device-internal scratch.
+ */
+#ifndef SAC_GPU_H
+#define SAC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SAC_LENTYPE 10 /* CHARACTER*^LENTYPE, src/vacpp.pl:156 */
+#define SAC_NHIB 10    /* nhiB, src/vacdef.t:34 */
+#define SAC_NWMAX 13   /* nw for -d=33 -p=mhd, src/vacpar.t.mhd:9-13 */
+
+typedef int sac_status;
+#define SAC_OK 0
+#define SAC_ERR_ARG 1         /* bad argument (die() in the reference) */
+#define SAC_ERR_STATE 2       /* call out of order (grid/boundaries/state not set) */
+#define SAC_ERR_CUDA 3        /* CUDA runtime error */
+#define SAC_ERR_NOMEM 4       /* device allocation failed */
+#define SAC_ERR_UNSUPPORTED 5 /* option outside the implemented path */
+#define SAC_ERR_NONFINITE 6   /* NaN/Inf met in a reduction */
+#define SAC_ERR_TIMEOUT 7     /* a bounded device wait ran out */
+#define SAC_ERR_NODEVICE 8    /* no usable CUDA device */
+
+/* Storage precision of the perturbed variables (the background is always FP64). */
+#define SAC_PREC_FP64 0
+#define SAC_PREC_FP32 1
+
+/* User modules: the specialsource/getdt_special plug-in of vacusr.t.
+ *   SAC_USR_NONE       no special sources
+ *   SAC_USR_VISCOSITY  hyperdiffusion only, no dt limit     sac/src/vacusr.t.stuart:46-94
+ *   SAC_USR_SLOG       gravity + hyperdiffusion + Gaussian vortex driver,
+ *                      dt limits from viscosity and gravity src/vacusr.f:1255-1421
+ *   SAC_USR_GRAVVISC   gravity + hyperdiffusion, both dt limits (vacusr.gravity.t +
+ *                      vacusr.viscosity.t without a driver)
+ *   SAC_USR_STRAT      gravity + hyperdiffusion + a vertical-velocity driver near the
+ *                      lower x1 boundary (stratified-atmosphere workload)
+ *   SAC_USR_TUBE       gravity + hyperdiffusion + a horizontal-velocity driver near the
+ *                      lower x2 boundary (2D flux-tube workload)              */
+#define SAC_USR_NONE 0
+#define SAC_USR_VISCOSITY 1
+#define SAC_USR_SLOG 2
+#define SAC_USR_GRAVVISC 3
+#define SAC_USR_STRAT 4
+#define SAC_USR_TUBE 5
+
+typedef struct sac_params {
+  /* equation parameters eqpar(1:neqpar+nspecialpar), src/vacpar.t.mhd:26,
+   * src/vacusrpar.f:3-6 */
+  double gamma;   /* eqpar(gamma_) */
+  double eta;     /* eqpar(eta_): must be 0 (resistive module off, -off=resist) */
+  double grav[3]; /* eqpar(grav1_..grav3_) */
+  double nu;      /* eqpar(nu_): hyperdiffusion on when |nu|>smalldouble */
+  /* &paramlist, src/vacio.t:47 */
+  double courantpar;
+  double dtpar;
+  double dtdiffpar;
+  int dtcantgrow;
+  /* &methodlist, src/vacio.t:33 */
+  char typeadvance[SAC_LENTYPE + 1]; /* onestep|twostep|threestep|fourstep|sterck|jameson */
+  char typepred[SAC_LENTYPE + 1];    /* predictor of 'twostep': 'nul' or 'cd4' */
+  int sourceunsplit;                 /* sources added inside centdiff4 (par/DEFAULT:44) */
+  int divbfix;                       /* Powell source; only 0 is implemented */
+  /* plug-in */
+  int user;            /* SAC_USR_* */
+  /* driver parameters.  SAC_USR_STRAT: [0]=amplitude A, [1]=omega, [2],[3]=driver
+   * centre in x2,x3, [4]=horizontal Gaussian width, [5]=x1 centre, [6]=x1 width.
+   * SAC_USR_TUBE: [0]=A, [1]=omega, [2]=x1 centre, [3]=x1 Gaussian width,
+   * [4]=x2 centre, [5]=x2 width.  Unused for the other modules. */
+  double userpar[16];
+  int alias_nu_grav3;  /* reproduce eqpar(nu_)==eqpar(grav3_) (src/vacusrpar.f:4-5) */
+  int precision;       /* SAC_PREC_FP64 | SAC_PREC_FP32 */
+  int device;          /* CUDA ordinal (ignored by the CPU oracle) */
+} sac_params;
+
+typedef struct sac_diag_out {
+  double wmean[SAC_NWMAX]; /* dvolume-weighted means over the mesh (savefilelog_default) */
+  double divb_l2;          /* sqrt(mean (div B)^2) over the mesh, 4th-order getdivb stencil */
+  double divb_linf;        /* max |div B| over the mesh */
+  double maxviscoef;       /* running max of nu over the current step (setnu) */
+  double ctot[3];          /* last c_tot per dimension used by setnu */
+  int nonfinite;           /* 1 if a NaN/Inf was seen in the mesh */
+} sac_diag_out;
+
+typedef struct sac_ctx sac_ctx;
+
+/* Fill p with the reference's defaults (par/DEFAULT + physini). */
+void sac_default_params(sac_params* p);
+
+sac_status sac_create(const sac_params* p, sac_ctx** out);
+
+/* ndim, ndir: -d=NdimNdir.  ixGhi[0..2]: grid extents with ghosts (ixGlo=1; unused
+ * dims 1).  ixM[0..5]: ixMmin1..3, ixMmax1..3 (1-based).  x: x(ixG^T,ndim) Fortran
+ * order; when fullgridini is 0 only the mesh part is read and the ghost coordinates
+ * are extrapolated as gridsetup1 does. */
+sac_status sac_set_grid(sac_ctx* c, int ndim, int ndir, const int ixGhi[3], const int ixM[6],
+                        const double* x, int fullgridini);
+
+/* typeB: CHARACTER*10 typeB(nw,nB) (f10, blank padded), default regions
+ * iB=2*idim-1 (lower) / 2*idim (upper).  ipairB may be NULL (auto pairing). */
+sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* ipairB);
+
+sac_status sac_upload(sac_ctx* c, const double* w);
+sac_status sac_download(sac_ctx* c, double* w);
+sac_status sac_getboundary(sac_ctx* c, double t);
+
+/* On return *dt holds the step of the dt block of the main loop, src/vac.t:61-70
+ * (dtpar, getdt_courant, getdt, getdt_special, dtcantgrow).  it is the step number. */
+sac_status sac_getdt(sac_ctx* c, double* dt, int it);
+
+/* method: typefull1 ('cd4' | 'source' | 'nul'); iws: iws(1:nw+1), iws(nw+1)=count,
+ * or NULL for all advanced variables. */
+sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmin, int idimmax,
+                      double dt, double t, int it);
+
+sac_status sac_diag(sac_ctx* c, sac_diag_out* out);
+sac_status sac_synchronize(sac_ctx* c);
+const char* sac_last_error(const sac_ctx* c);
+void sac_destroy(sac_ctx* c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SAC_GPU_H */

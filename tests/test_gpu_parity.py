@@ -1,0 +1,138 @@
+"""Parity of the CUDA path (libsacgpu.so through the C-ABI) with the CPU oracle.
+
+The bar is the hot path's: FP64 results within 1e-12 relative L2 per variable of
+the oracle after 100 steps (tolerance RTOL below), dt within 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from sac_b200 import abi, params, problems
+
+import _util
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def _pair(P):
+    o = _util.start(Oracle, P)
+    g = _util.start(abi.Context, P)
+    return o, g
+
+
+def _compare(P, o, g, rtol=RTOL):
+    wo = _util.mesh(P, o.download())
+    wg = _util.mesh(P, g.download())
+    err = _util.rel_l2(wg, wo)
+    assert np.isfinite(wg).all()
+    assert err.max() <= rtol, f"{P.name}: rel L2 per variable {err}"
+    return err
+
+
+def _steps(P, nsteps, **kw):
+    o, g = _pair(P)
+    d_o = _util.run(o, nsteps, **kw)
+    d_g = _util.run(g, nsteps, **kw)
+    np.testing.assert_allclose(d_g, d_o, rtol=1e-12, atol=0)
+    return _compare(P, o, g)
+
+
+def test_getboundary_initial_fill():
+    P = problems.random_problem((14, 12), seed=11, types=["cont", "fixed", "periodic", "periodic"])
+    o, g = _pair(P)
+    np.testing.assert_array_equal(g.download(), o.download())
+
+
+@pytest.mark.parametrize("types", [
+    ["cont1", "grad1", "symm", "asymm"],
+    ["fixed1", "contCD4", "symm0", "cont"],
+    ["periodic", "periodic", "fixed", "cont1"],
+])
+def test_boundary_types_2d(types):
+    P = problems.random_problem((12, 10), seed=12, types=types)
+    o, g = _pair(P)
+    np.testing.assert_array_equal(g.download(), o.download())
+    _util.run(o, 5)
+    _util.run(g, 5)
+    _compare(P, o, g)
+
+
+def test_briowu_100_steps():
+    P = problems.brio_wu(nx=128)
+    P.params.user = params.USR_GRAVVISC
+    _steps(P, 100)
+
+
+@pytest.mark.parametrize("ndir", [1, 2, 3])
+def test_random_1d(ndir):
+    P = problems.random_problem((40,), ndir=ndir, seed=3 + ndir)
+    _steps(P, 100)
+
+
+@pytest.mark.parametrize("ndir", [2, 3])
+def test_random_2d(ndir):
+    P = problems.random_problem((20, 16), ndir=ndir, seed=5, types=["cont", "fixed", "periodic", "periodic"])
+    _steps(P, 100)
+
+
+def test_random_3d_mixed_bounds():
+    P = problems.random_problem((12, 10, 8), seed=6, types=["fixed", "cont", "periodic", "periodic", "cont", "symm"])
+    _steps(P, 100)
+
+
+def test_stratified_3d_driver():
+    P = problems.stratified(n=(16, 12, 12), amp=0.05)
+    _steps(P, 100)
+
+
+def test_zero_perturbation_stays_zero():
+    P = problems.stratified(n=(12, 10, 10), amp=0.0)
+    g = _util.start(abi.Context, P)
+    _util.run(g, 20)
+    w = g.download()
+    assert np.all(w[..., : 2 * P.ndir + 2] == 0.0)
+
+
+@pytest.mark.parametrize("method,pred", [("onestep", "nul"), ("twostep", "nul"), ("twostep", "cd4"),
+                                          ("threestep", "nul"), ("sterck", "nul"), ("jameson", "nul")])
+def test_time_integrators(method, pred):
+    P = problems.random_problem((16, 12), seed=7, types=["cont", "cont", "periodic", "periodic"],
+                                typeadvance=method, courantpar=0.2)
+    P.params.typepred = pred.encode()
+    _steps(P, 20)
+
+
+def test_dimensional_splitting():
+    P = problems.random_problem((14, 12), seed=8, types=["cont", "cont", "periodic", "periodic"])
+    _steps(P, 20, idim=[1, 2])
+
+
+def test_slog_driver_with_alias():
+    P = problems.random_problem((10, 8, 8), seed=9, user=params.USR_SLOG)
+    # Slog lengths are in metres (Mm scale), x1 vertical
+    P.x[...] *= 1.0e6
+    P.params.alias_nu_grav3 = 1
+    _steps(P, 10)
+
+
+def test_source_method_only():
+    P = problems.random_problem((16, 12), seed=10, types=["cont", "cont", "periodic", "periodic"])
+    o, g = _pair(P)
+    for k in range(5):
+        dt = 0.01
+        o.advect(dt, 0.01 * k, k, method="source")
+        g.advect(dt, 0.01 * k, k, method="source")
+    _compare(P, o, g)
+
+
+def test_diag_matches_oracle():
+    P = problems.random_problem((12, 10, 8), seed=6, types=["cont", "cont", "periodic", "periodic", "cont", "cont"])
+    o, g = _pair(P)
+    _util.run(o, 3)
+    _util.run(g, 3)
+    do, dg = o.diag(), g.diag()
+    np.testing.assert_allclose(list(dg.wmean)[:P.nw], list(do.wmean)[:P.nw], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(dg.divb_l2, do.divb_l2, rtol=1e-10)
+    np.testing.assert_allclose(dg.divb_linf, do.divb_linf, rtol=1e-10)
