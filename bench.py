@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Benchmark of the perturbation-MHD hot path on B200.
+
+Workload: the 3D gravitationally stratified atmosphere, 128x128x128 mesh cells,
+FP64, RK4 (typeadvance='fourstep'), hyperdiffusion, gravity, bottom velocity
+driver, fixed/open x1 boundaries and periodic x2/x3 (sac_b200.problems.stratified).
+One step = one time step of the reference's main loop: getdt + advect (four RK
+stages with their boundary fills) on the resident state.  Metric: cell-updates
+per second (one mesh cell advanced by one full RK4 step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N>1 the script runs under torch.distributed.run, one process per GPU, each
+advancing its own replica (the path does not shard); timing is the max over
+ranks, value is the whole-job rate.  `--impl reference` times the CPU
+restatement of the reference (oracle/, C++, all host threads) on the same
+workload; rank 0 alone runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from sac_b200 import abi, problems  # noqa: E402
+
+METRIC = "3D MHD cell-updates/s"
+UNIT = "cell-updates/s"
+BYTES_PER_CELL_UPDATE = {"fp64": 1056}  # 14*n_p*s_p + 4*n_b*s_b, n_p=8, n_b=5
+STAGES_PER_STEP = 4
+REF_SAMPLE = (128, 128, 32)  # bounded CPU sample: one RK4 step on an x3 slab of the workload
+
+
+def workload(n=128, precision="fp64"):
+    P = problems.stratified(n=(n, n, n))
+    return P
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(name):
+    p = os.path.join(ROOT, "profiles", name)
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        with open(self.file.name) as f:
+            rows = [r.split(",") for r in f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# the CPU legs (oracle = C++ restatement of the reference)
+# ---------------------------------------------------------------------------
+def cpu_sample(seconds=10.0, max_steps=8):
+    """Cell-updates/s of the oracle on the host cores: one untimed RK4 step, then
+    timed steps until `seconds` elapse, on a REF_SAMPLE slab of the workload."""
+    from oracle import oracle
+
+    P = problems.stratified(n=REF_SAMPLE)
+    o = oracle.Oracle(P.params)
+    o.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
+    o.set_boundaries(P.typeB_packed, P.nB)
+    o.upload(P.w)
+    o.getboundary(0.0)
+    t, it = 0.0, 0
+    dt = o.getdt(it)
+    o.advect(dt, t, it)
+    t += dt
+    it += 1
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps:
+        dt = o.getdt(it)
+        o.advect(dt, t, it)
+        t += dt
+        it += 1
+        n += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    el = time.perf_counter() - t0
+    o.close()
+    return P.ncells * n / el, n, el, oracle.max_threads()
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle import oracle
+
+    oracle.build()
+    P = problems.stratified(n=REF_SAMPLE)
+    o = oracle.Oracle(P.params)
+    o.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
+    o.set_boundaries(P.typeB_packed, P.nB)
+    o.upload(P.w)
+    o.getboundary(0.0)
+    t, it = 0.0, 0
+    for _ in range(args.warmup):
+        dt = o.getdt(it)
+        o.advect(dt, t, it)
+        t += dt
+        it += 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        dt = o.getdt(it)
+        o.advect(dt, t, it)
+        t += dt
+        it += 1
+    el = time.perf_counter() - t0
+    v = P.ncells * args.steps / el
+    cores = oracle.max_threads()
+    sample = (f"one RK4 step (getdt+advect) per step on a {REF_SAMPLE[0]}x{REF_SAMPLE[1]}x{REF_SAMPLE[2]} "
+              f"x3-slab of the 128^3 stratified workload, C++ FP64 restatement of the reference "
+              f"(the Fortran reference cannot be built: no Fortran compiler), OpenMP {cores} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "stratified atmosphere 128^3, FP64, RK4, hyperdiffusion, gravity, driver",
+                   "cells_per_step": P.ncells, "parallelism": "cpu"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def _lib_ext(ctx):
+    lib = ctx.lib
+    lib.sac_get_stream.argtypes = [ctypes.c_void_p]
+    lib.sac_get_stream.restype = ctypes.c_void_p
+    lib.sac_profile.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.sac_profile_read.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_long), ctypes.c_int]
+    lib.sac_kernel_launches.argtypes = [ctypes.c_void_p]
+    lib.sac_kernel_launches.restype = ctypes.c_long
+    return lib
+
+
+def prof_read(lib, h, kind, reset=True):
+    ms, n = ctypes.c_double(), ctypes.c_long()
+    lib.sac_profile_read(h, kind, ctypes.byref(ms), ctypes.byref(n), int(reset))
+    return ms.value, n.value
+
+
+def ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from sac_b200 import build as sbuild
+
+    sbuild.build()
+    torch.cuda.set_device(local_rank)
+    P = workload(args.n)
+    P.params.device = local_rank
+    ctx = abi.Context(P.params)
+    lib = _lib_ext(ctx)
+    ctx.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
+    ctx.set_boundaries(P.typeB_packed, P.nB)
+    ctx.upload(P.w)
+    ctx.getboundary(0.0)
+    stream = torch.cuda.ExternalStream(lib.sac_get_stream(ctx.h), device=local_rank)
+
+    t, it = 0.0, 0
+    for _ in range(args.warmup):
+        dt = ctx.getdt(it)
+        ctx.advect(dt, t, it)
+        t += dt
+        it += 1
+    ctx.synchronize()
+
+    # timed region: K steps, per-kernel events on the library's stream
+    lib.sac_profile(ctx.h, 1)
+    for k in range(5):
+        prof_read(lib, ctx.h, k, reset=True)
+    launches0 = lib.sac_kernel_launches(ctx.h)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            dt = ctx.getdt(it)
+            ctx.advect(dt, t, it)
+            t += dt
+            it += 1
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        dist.barrier()
+    launches = lib.sac_kernel_launches(ctx.h) - launches0
+    kern = {name: prof_read(lib, ctx.h, k) for k, name in enumerate(["stage", "prep", "bound", "courant", "other"])}
+    lib.sac_profile(ctx.h, 0)
+    if world > 1:
+        tt = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    cells = P.ncells
+    value = world * cells * args.steps / (ms / 1e3)
+
+    # end to end through the C-ABI with host buffers: per step upload(w),
+    # getdt, advect, download(w) from/to pinned host memory
+    nbytes = P.nw * int(np.prod(P.ixGhi)) * 8
+    pin = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    hw = pin.numpy().reshape(P.ixGhi + (P.nw,), order="F")
+    hw[...] = ctx.download()
+    e2e_steps = max(3, min(args.steps, 10))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.upload(hw)
+        dt = ctx.getdt(it)
+        ctx.advect(dt, t, it)
+        t += dt
+        it += 1
+        ctx.download(hw)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = world * cells * e2e_steps / e2e_s
+
+    if rank != 0:
+        ctx.close()
+        return 0
+
+    stage_ms, stage_n = kern["stage"]
+    peak, peak_kind = load_peaks()
+    b_launch = BYTES_PER_CELL_UPDATE["fp64"] / STAGES_PER_STEP * cells
+    achieved = b_launch / (stage_ms / stage_n / 1e3) / 1e9 if stage_n else None
+    tr = load_traffic("stage_fp64_traffic.json")
+    traffic = None
+    if tr and tr.get("cells"):
+        traffic = tr["dram_bytes_per_launch"] * cells / tr["cells"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "stratified atmosphere 128^3, FP64, RK4, hyperdiffusion, gravity, driver",
+                   "cells_per_step": cells, "parallelism": f"replicas{world}",
+                   "l2": "no flush: resident state ~0.8 GB per replica, larger than L2",
+                   "step": "getdt + advect (4 RK stages + boundary fills)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": peak_kind, "kernel": "k_stage<3,3> FP64",
+                     "bytes_per_launch": b_launch, "avg_launch_ms": stage_ms / stage_n if stage_n else None},
+        "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                "path": "sac_upload + sac_getdt + sac_advect + sac_download per step, pinned host w"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu:
+        v, n, el, cores = cpu_sample()
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{n} RK4 steps in {el:.1f} s on a {REF_SAMPLE[0]}x{REF_SAMPLE[1]}x"
+                                          f"{REF_SAMPLE[2]} x3-slab of the workload, C++ oracle, OpenMP"}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128, help="mesh cells per dimension (default 128)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        return ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -145,6 +145,24 @@ sac_status sac_synchronize(sac_ctx* c);
 const char* sac_last_error(const sac_ctx* c);
 void sac_destroy(sac_ctx* c);
 
+/* ---- library extensions: no counterpart in the reference ------------------
+ * Stream selection lets a host run the path on its own CUDA stream (or capture
+ * it); profiling brackets every kernel launch with CUDA events on that stream. */
+#define SAC_K_STAGE 0   /* k_update: the per-cell stage update */
+#define SAC_K_PREP 1    /* k_face: derived fields, fluxes, c_tot */
+#define SAC_K_BOUND 2   /* k_bound: ghost-cell resolve */
+#define SAC_K_COURANT 3 /* getdt_courant reduction */
+#define SAC_K_OTHER 4   /* conversions, copies and RK combinations */
+#define SAC_K_NU 5      /* k_nu: setnu face ratios */
+#define SAC_K_COUNT 6
+sac_status sac_set_stream(sac_ctx* c, void* cuda_stream); /* NULL: the context's own stream */
+void* sac_get_stream(const sac_ctx* c);
+sac_status sac_profile(sac_ctx* c, int enable);
+/* synchronises, then returns the summed event time and launch count of kernel
+ * class `kernel` since the last reset (reset != 0 clears after reading) */
+sac_status sac_profile_read(sac_ctx* c, int kernel, double* total_ms, long* launches, int reset);
+long sac_kernel_launches(const sac_ctx* c);
+
 #ifdef __cplusplus
 }
 #endif

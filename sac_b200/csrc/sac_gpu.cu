@@ -1,18 +1,21 @@
 // sac_gpu.cu -- libsacgpu.so: the C-ABI of include/sac_gpu.h on sm_100a.
 //
-// Device state per context (all FP64 in this path):
-//   P[4]  perturbed blocks (rho, m1.., e, b1..) of w, w1, w2, w3, np*ncell each,
-//         Fortran layout w(ix1,ix2,ix3,iw) restricted to the advanced variables;
-//   BG    the static background block (eb, rhob, bg1..), shared by all four;
-//   D     derived per-cell fields of the current stage input (k_prep);
-//   x, dx grid coordinates and cell widths (gridsetup1);
-//   fixB  compact ghost slabs of 'fixed'/'fixed1'/'grad1' regions.
-// One RK4 step (typeadvance='fourstep', src/vac.t:439-455) is four (prep, stage,
-// boundary) triples; the w1 accumulation and the final w+w1 are fused into the
-// stage stores and the boundary pass.
+// Device state per context; S is the storage type of the advanced variables
+// (double, or float for SAC_PREC_FP32):
+//   P[4]  advanced blocks (rho, m1.., e, b1..) of w, w1, w2, w3, np*ncell of S
+//         each, Fortran layout w(ix1,ix2,ix3,iw) restricted to those variables;
+//   BG    the static background block (eb, rhob, bg1..), FP64, shared by all four;
+//   D, F, R  per-stage intermediates of S: derived cell fields, fluxes along each
+//         dimension, setnu face ratios (sac_stage.cuh);
+//   x, dx, 1/dx  grid coordinates and widths (gridsetup1), FP64;
+//   fixB  compact ghost slabs of 'fixed'/'fixed1'/'grad1' regions, FP64.
+// One RK4 step (typeadvance='fourstep', src/vac.t:439-455) is four
+// (k_face, k_nu, k_update, k_bound) sequences; the w1 accumulation and the final
+// w+w1 are fused into the k_update stores and the boundary pass.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -21,6 +24,7 @@
 
 #include "sac_gpu.h"
 #include "sac_kernels.cuh"
+#include "sac_stage_api.h"
 
 using namespace sacgpu;
 
@@ -36,11 +40,18 @@ struct sac_ctx {
   Geom g{};
   bool grid_set = false, bc_set = false, state_set = false, bc_init_done = false;
   int fullgridini = 0;
-  double* P[4] = {nullptr, nullptr, nullptr, nullptr};
+  int prec = SAC_PREC_FP64;
+  size_t es = sizeof(double);  // bytes per stored advanced value
+  void* P[4] = {nullptr, nullptr, nullptr, nullptr};
   double* BG = nullptr;
-  double* D = nullptr;
+  void* D = nullptr;
+  void* F = nullptr;
+  void* R = nullptr;
   double* x = nullptr;
   double* dx = nullptr;
+  double* drv = nullptr;
+  double* stg = nullptr;  // FP64 staging block for FP32 upload/download
+  double drvA = 0.0;
   unsigned long long* red = nullptr;  // 0..2 ctot, 3 maxnu, 4 courant, 5 divb max, 6 divb sq (as double)
   double* fixB = nullptr;
   long fixoff[6] = {0, 0, 0, 0, 0, 0}, slab[6] = {0, 0, 0, 0, 0, 0};
@@ -58,6 +69,17 @@ struct sac_ctx {
   int itmin = 0;
   bool itmin_set = false;
   long kernel_launches = 0;
+  cudaStream_t own_stream = nullptr;
+  // event profiling
+  bool prof = false;
+  struct Rec {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  double prof_ms[SAC_K_COUNT] = {};
+  long prof_n[SAC_K_COUNT] = {};
 };
 
 namespace {
@@ -75,6 +97,52 @@ sac_status fail(sac_ctx* c, sac_status st, const std::string& msg) {
   } while (0)
 
 int np_of(int ndir) { return 2 * ndir + 2; }
+
+cudaEvent_t ev_get(sac_ctx* c) {
+  if (!c->pool.empty()) {
+    cudaEvent_t e = c->pool.back();
+    c->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Bracket one launch with events when profiling is on.
+struct Prof {
+  sac_ctx* c;
+  int kind;
+  cudaEvent_t a = nullptr;
+  Prof(sac_ctx* c_, int k) : c(c_), kind(k) {
+    c->kernel_launches++;
+    if (c->prof) {
+      a = ev_get(c);
+      cudaEventRecord(a, c->stream);
+    }
+  }
+  ~Prof() {
+    if (a) {
+      cudaEvent_t b = ev_get(c);
+      cudaEventRecord(b, c->stream);
+      c->recs.push_back({kind, a, b});
+    }
+  }
+};
+
+void prof_collect(sac_ctx* c) {
+  if (c->recs.empty()) return;
+  cudaStreamSynchronize(c->stream);
+  for (auto& r : c->recs) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    c->prof_ms[r.kind] += ms;
+    c->prof_n[r.kind] += 1;
+    c->pool.push_back(r.a);
+    c->pool.push_back(r.b);
+  }
+  c->recs.clear();
+}
 
 int8_t btype(const std::string& t, bool* ok) {
   *ok = true;
@@ -104,10 +172,11 @@ bool grav_module(int u) {
 void release(sac_ctx* c) {
   for (auto& p : c->P)
     if (p) cudaFree(p), p = nullptr;
-  for (void* p : {(void*)c->BG, (void*)c->D, (void*)c->x, (void*)c->dx, (void*)c->red, (void*)c->fixB,
-                  (void*)c->d_type, (void*)c->d_fixed})
+  for (void* p : {(void*)c->BG, c->D, c->F, c->R, (void*)c->x, (void*)c->dx, (void*)c->drv,
+                  (void*)c->stg, (void*)c->red, (void*)c->fixB, (void*)c->d_type, (void*)c->d_fixed})
     if (p) cudaFree(p);
-  c->BG = c->D = c->x = c->dx = c->fixB = nullptr;
+  c->BG = c->x = c->dx = c->drv = c->stg = c->fixB = nullptr;
+  c->D = c->F = c->R = nullptr;
   c->red = nullptr;
   c->d_type = nullptr;
   c->d_fixed = nullptr;
@@ -116,49 +185,7 @@ void release(sac_ctx* c) {
 // --------------------------------------------------------------------------
 // launch helpers
 // --------------------------------------------------------------------------
-template <int NDIR>
-void launch_prep_t(sac_ctx* c, const double* wp) {
-  const long N = c->g.ncell;
-  const int bs = 256;
-  k_prep<NDIR><<<(unsigned)((N + bs - 1) / bs), bs, 0, c->stream>>>(c->g, wp, c->BG, c->D, c->red, c->par.gamma,
-                                                                    c->g.ndim);
-}
-
-void launch_prep(sac_ctx* c, const double* wp) {
-  switch (c->g.ndir) {
-    case 1: launch_prep_t<1>(c, wp); break;
-    case 2: launch_prep_t<2>(c, wp); break;
-    default: launch_prep_t<3>(c, wp); break;
-  }
-  c->kernel_launches++;
-}
-
-template <int NDIM, int NDIR>
-void launch_stage_t(sac_ctx* c, const StageArgs& a) {
-  dim3 blk, grd;
-  const int n0 = a.g.hi[0] - a.g.lo[0] + 1, n1 = a.g.hi[1] - a.g.lo[1] + 1, n2 = a.g.hi[2] - a.g.lo[2] + 1;
-  if (NDIM == 1)
-    blk = dim3(128, 1, 1);
-  else if (NDIM == 2)
-    blk = dim3(32, 4, 1);
-  else
-    blk = dim3(32, 2, 2);
-  grd = dim3((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, (n2 + blk.z - 1) / blk.z);
-  k_stage<NDIM, NDIR><<<grd, blk, 0, c->stream>>>(a);
-}
-
-void launch_stage(sac_ctx* c, const StageArgs& a) {
-  const int nd = c->g.ndim, nr = c->g.ndir;
-  if (nd == 1 && nr == 1) launch_stage_t<1, 1>(c, a);
-  else if (nd == 1 && nr == 2) launch_stage_t<1, 2>(c, a);
-  else if (nd == 1 && nr == 3) launch_stage_t<1, 3>(c, a);
-  else if (nd == 2 && nr == 2) launch_stage_t<2, 2>(c, a);
-  else if (nd == 2 && nr == 3) launch_stage_t<2, 3>(c, a);
-  else launch_stage_t<3, 3>(c, a);
-  c->kernel_launches++;
-}
-
-BcArgs bc_args(sac_ctx* c, double* A) {
+BcArgs bc_args(sac_ctx* c, void* A) {
   BcArgs b{};
   b.g = c->g;
   b.A = A;
@@ -175,6 +202,7 @@ BcArgs bc_args(sac_ctx* c, double* A) {
   return b;
 }
 
+template <typename S>
 void launch_bound(sac_ctx* c, const BcArgs& b, int nvar) {
   const Geom& g = c->g;
   long ns[3] = {0, 0, 0};
@@ -189,69 +217,76 @@ void launch_bound(sac_ctx* c, const BcArgs& b, int nvar) {
   const long tot = ns[0] + ns[1] + ns[2];
   if (tot == 0) return;
   const int bs = 256;
-  k_bound<<<(unsigned)((tot + bs - 1) / bs), bs, 0, c->stream>>>(b, ns[0], ns[1], ns[2], nvar);
-  c->kernel_launches++;
+  Prof pr(c, SAC_K_BOUND);
+  k_bound<S><<<(unsigned)((tot + bs - 1) / bs), bs, 0, c->stream>>>(b, ns[0], ns[1], ns[2], nvar);
 }
 
-StageArgs stage_args(sac_ctx* c, double qdt, int dmin, int dmax, bool flux_on, double qt, const double* wct,
-                     const double* base, double* out, unsigned mask) {
-  StageArgs a{};
-  a.g = c->g;
-  a.wct_p = wct;
-  a.bgv = c->BG;
-  a.base = base;
-  a.out = out;
-  a.D = c->D;
-  a.dx = c->dx;
-  a.x = c->x;
-  a.ctot = c->red;
-  a.maxnu = c->red + 3;
-  a.qdt = qdt;
-  // sources in centdiff4 carry qdt*(idimmax-idimmin+1)/ndim, src/vaccd.t:73-75;
-  // advect1 'source' passes qdt unchanged
-  a.qdt2 = flux_on ? qdt * ((double)(dmax - dmin) + 1.0) / (double)c->g.ndim : qdt;
-  a.gamma = c->par.gamma;
-  a.t = qt;
-  for (int d = 0; d < 3; ++d) a.grav[d] = (d < c->g.ndim) ? c->par.grav[d] : 0.0;
-  if (c->par.alias_nu_grav3 && c->g.ndim == 3) a.grav[2] = 1.0;
-  std::memcpy(a.up, c->par.userpar, sizeof(a.up));
-  a.dmin = flux_on ? dmin : 1;
-  a.dmax = flux_on ? dmax : 0;
-  a.iwmask = mask;
-  for (int d = 0; d < 3; ++d)
-    for (int s = 0; s < 2; ++s) {
-      a.zero4[d][s] = (d < c->g.ndim) ? 1 : 0;  // single device: no 'mpi' boundaries
-      a.mirror[d][s] = (d < c->g.ndim) ? 1 : 0;
-      a.zero1[d][s] = c->zero1[d][s];
-    }
-  const int u = c->par.user;
-  a.grav_on = (c->par.sourceunsplit && grav_module(u)) ? 1 : 0;
-  a.visc_on = (c->par.sourceunsplit && visc_on(c)) ? 1 : 0;
-  a.driver = DRV_NONE;
-  if (c->par.sourceunsplit) {
-    if (u == SAC_USR_SLOG) a.driver = DRV_SLOG;
-    if (u == SAC_USR_STRAT) a.driver = DRV_STRAT;
-    if (u == SAC_USR_TUBE) a.driver = DRV_TUBE;
-  }
-  a.epi = EPI_PLAIN;
-  return a;
-}
-
-// advect1 (src/vac.t:490-549): out = base + qdt R(wct) then getboundary(out)
-sac_status advect1(sac_ctx* c, const std::string& method, double qdt, int dmin, int dmax, double qt,
-                   const double* wct, const double* base, double* out, unsigned mask, int epi = EPI_PLAIN,
-                   double* aux1 = nullptr, const double* aux2 = nullptr) {
+// advect1 (src/vac.t:490-549): out = base + qdt R(wct), then getboundary(out)
+template <typename S>
+sac_status advect1_t(sac_ctx* c, const std::string& method, double qdt, int dmin, int dmax, double qt,
+                     const void* wct, const void* base, void* out, unsigned mask, int epi, void* aux1,
+                     const void* aux2) {
+  const Geom& g = c->g;
   if (method == "cd4" || method == "source") {
     const bool flux = (method == "cd4");
+    const int u = c->par.user;
+    const bool visc = c->par.sourceunsplit && visc_on(c);
     CK(cudaMemsetAsync(c->red, 0, 3 * sizeof(unsigned long long), c->stream));
-    launch_prep(c, wct);
-    StageArgs a = stage_args(c, qdt, dmin, dmax, flux, qt, wct, base, out, mask);
-    a.epi = epi;
+    Stage2Args a{};
+    a.g = g;
+    a.wct = wct;
+    a.bgv = c->BG;
+    a.base = base;
+    a.out = out;
     a.aux1 = aux1;
     a.aux2 = aux2;
-    launch_stage(c, a);
+    a.D = c->D;
+    a.F = c->F;
+    a.R = c->R;
+    a.dx = c->dx;
+    a.drv = c->drv;
+    a.ctot = c->red;
+    a.maxnu = c->red + 3;
+    a.qdt = qdt;
+    // sources inside centdiff4 carry qdt*(idimmax-idimmin+1)/ndim, src/vaccd.t:73-75;
+    // advect1 'source' passes qdt unchanged
+    a.qdt2 = flux ? qdt * ((double)(dmax - dmin) + 1.0) / (double)g.ndim : qdt;
+    a.gamma = c->par.gamma;
+    for (int d = 0; d < 3; ++d) a.grav[d] = (d < g.ndim) ? c->par.grav[d] : 0.0;
+    if (c->par.alias_nu_grav3 && g.ndim == 3) a.grav[2] = 1.0;
+    a.dmin = flux ? dmin : 1;
+    a.dmax = flux ? dmax : 0;
+    a.iwmask = mask;
+    for (int d = 0; d < 3; ++d)
+      for (int s2 = 0; s2 < 2; ++s2) a.zero1[d][s2] = c->zero1[d][s2];
+    a.grav_on = (c->par.sourceunsplit && grav_module(u)) ? 1 : 0;
+    a.visc_on = visc ? 1 : 0;
+    a.driver = DRV_NONE;
+    if (c->par.sourceunsplit && c->drv) {
+      if (u == SAC_USR_SLOG && g.ndim == 3) {
+        a.driver = DRV_SLOG;  // tdep=SIN(qt*2*pi/s_period), src/vacusr.f:1321
+        a.tdep = std::sin(qt * 2.0 * (double)3.1415926535897932384626433832795f / 240.0);
+      } else if (u == SAC_USR_STRAT || u == SAC_USR_TUBE) {
+        a.driver = (u == SAC_USR_STRAT) ? DRV_STRAT : DRV_TUBE;
+        a.tdep = std::sin(c->par.userpar[1] * qt);
+      }
+      a.drvA = c->drvA;
+    }
+    a.epi = epi;
+    {
+      Prof pr(c, SAC_K_PREP);
+      launch_face<S>(g, wct, c->BG, c->D, c->F, c->red, c->par.gamma, visc ? 1 : 0, c->stream);
+    }
+    if (visc) {
+      Prof pr(c, SAC_K_NU);
+      launch_nu<S>(g, wct, c->D, c->R, c->red, c->stream);
+    }
+    {
+      Prof pr(c, SAC_K_STAGE);
+      launch_update<S>(a, c->stream);
+    }
   } else if (base != out) {
-    CK(cudaMemcpyAsync(out, base, sizeof(double) * c->g.np * c->g.ncell, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(out, base, c->es * g.np * g.ncell, cudaMemcpyDeviceToDevice, c->stream));
   }
   BcArgs b = bc_args(c, out);
   if (epi == EPI_RK4_S3) {
@@ -263,18 +298,28 @@ sac_status advect1(sac_ctx* c, const std::string& method, double qdt, int dmin, 
     b.mode = 2;
     b.aux1 = aux1;
   }
-  launch_bound(c, b, c->g.np);
+  launch_bound<S>(c, b, g.np);
   CK(cudaGetLastError());
   return SAC_OK;
 }
 
-__global__ void k_lin_threestep_a(double* w2, const double* w, const double* w1, long n) {
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    w2[i] = 3 * 0.25 * w[i] + 0.25 * w1[i];
+sac_status advect1(sac_ctx* c, const std::string& method, double qdt, int dmin, int dmax, double qt, const void* wct,
+                   const void* base, void* out, unsigned mask, int epi = EPI_PLAIN, void* aux1 = nullptr,
+                   const void* aux2 = nullptr) {
+  if (c->prec == SAC_PREC_FP32)
+    return advect1_t<float>(c, method, qdt, dmin, dmax, qt, wct, base, out, mask, epi, aux1, aux2);
+  return advect1_t<double>(c, method, qdt, dmin, dmax, qt, wct, base, out, mask, epi, aux1, aux2);
 }
-__global__ void k_lin_threestep_b(double* w, const double* w2, long n) {
+
+template <typename S>
+__global__ void k_lin_threestep_a(S* w2, const S* w, const S* w1, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    w[i] = w[i] / 3 + w2[i] * (2.0 / 3);
+    w2[i] = S(3 * 0.25) * w[i] + S(0.25) * w1[i];
+}
+template <typename S>
+__global__ void k_lin_threestep_b(S* w, const S* w2, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    w[i] = w[i] / S(3) + w2[i] * S(2.0 / 3);
 }
 
 }  // namespace
@@ -303,14 +348,17 @@ sac_status sac_create(const sac_params* p, sac_ctx** out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SAC_ERR_NODEVICE;
   if (p->device < 0 || p->device >= ndev) return SAC_ERR_ARG;
-  if (p->precision != SAC_PREC_FP64) return SAC_ERR_UNSUPPORTED;
+  if (p->precision != SAC_PREC_FP64 && p->precision != SAC_PREC_FP32) return SAC_ERR_UNSUPPORTED;
   sac_ctx* c = new sac_ctx();
   c->par = *p;
+  c->prec = p->precision;
+  c->es = (c->prec == SAC_PREC_FP32) ? sizeof(float) : sizeof(double);
   c->dev = p->device;
   if (cudaSetDevice(c->dev) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     return SAC_ERR_CUDA;
   }
+  c->own_stream = c->stream;
   *out = c;
   return SAC_OK;
 }
@@ -320,7 +368,12 @@ void sac_destroy(sac_ctx* c) {
   cudaSetDevice(c->dev);
   if (c->stream) cudaStreamSynchronize(c->stream);
   release(c);
-  if (c->stream) cudaStreamDestroy(c->stream);
+  for (auto& r : c->recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : c->pool) cudaEventDestroy(e);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
 
@@ -435,16 +488,60 @@ sac_status sac_set_grid(sac_ctx* c, int ndim, int ndir, const int ixGhi[3], cons
     c->mindx2[d] = m2;
   }
   c->h_dx = hdx;
-  const size_t bp = sizeof(double) * g.np * N;
+  // cell offsets inside one block of np (or ndir+3) fields are 32-bit
+  if ((long)std::max(g.np, ndir + 3) * N > 2147483647L)
+    return fail(c, SAC_ERR_UNSUPPORTED, "grid too large for 32-bit in-block indexing");
+  // driver spatial profiles (time independent), evaluated with the host libm as the
+  // oracle does: Slog vortex (src/vacusr.f:1324-1370) or the Gaussian velocity drivers
+  std::vector<double> hdrv;
+  const int u = c->par.user;
+  if ((u == SAC_USR_SLOG && ndim == 3) || u == SAC_USR_STRAT || (u == SAC_USR_TUBE && ndim >= 2)) {
+    hdrv.assign((size_t)2 * N, 0.0);
+    const double* up = c->par.userpar;
+    for (long q = 0; q < N; ++q) {
+      const double x1 = hx[q], x2 = ndim > 1 ? hx[N + q] : 0.0, x3 = ndim > 2 ? hx[2 * N + q] : 0.0;
+      if (u == SAC_USR_SLOG) {
+        const double xc1 = (double)0.1f * 1.0e6, xc2 = 1.0e6, xc3 = 1.0e6, B = (double)0.05f;
+        const double dz = 0.05e6, dxx = 0.5e6, dyy = 0.5e6;
+        const double xx = x2 - xc2, yy = x3 - xc3, zz = x1 - xc1;
+        const double exz = std::exp(-(zz * zz) / (dz * dz)), exx = std::exp(-(xx * xx) / (dxx * dxx)),
+                     exy = std::exp(-(yy * yy) / (dyy * dyy));
+        const double exyz = exx * exy * exz;
+        const double th = std::atan2(yy, xx), ph = std::atan2(1.0, B);
+        const double ux = std::cos(th + ph), uy = std::sin(th + ph);
+        hdrv[q] = (ux / std::sqrt(ux * ux + uy * uy)) * exyz;
+        hdrv[N + q] = (uy / std::sqrt(ux * ux + uy * uy)) * exyz;
+        c->drvA = 10.0;
+      } else if (u == SAC_USR_STRAT) {
+        const double xx = ndim > 1 ? x2 - up[2] : 0.0, yy = ndim > 2 ? x3 - up[3] : 0.0, zz = x1 - up[5];
+        hdrv[q] = std::exp(-(xx * xx + yy * yy) / (up[4] * up[4]));
+        hdrv[N + q] = std::exp(-(zz * zz) / (up[6] * up[6]));
+        c->drvA = up[0];
+      } else {
+        const double zz = x1 - up[2], xx = x2 - up[4];
+        hdrv[q] = std::exp(-(zz * zz) / (up[3] * up[3]));
+        hdrv[N + q] = std::exp(-(xx * xx) / (up[5] * up[5]));
+        c->drvA = up[0];
+      }
+    }
+  }
+  const size_t bp = c->es * g.np * N;
   for (auto& p : c->P) CK(cudaMalloc(&p, bp));
   CK(cudaMalloc(&c->BG, sizeof(double) * (g.nw - g.np) * N));
-  CK(cudaMalloc(&c->D, sizeof(double) * (ndir + 3) * N));
+  CK(cudaMalloc(&c->D, c->es * (ndir + 3) * N));
+  CK(cudaMalloc(&c->F, c->es * (size_t)ndim * g.np * N));
+  CK(cudaMalloc(&c->R, c->es * (size_t)nr_pairs(ndim) * N));
   CK(cudaMalloc(&c->x, sizeof(double) * ndim * N));
   CK(cudaMalloc(&c->dx, sizeof(double) * ndim * N));
+  if (!hdrv.empty()) CK(cudaMalloc(&c->drv, sizeof(double) * 2 * N));
+  if (c->prec == SAC_PREC_FP32) CK(cudaMalloc(&c->stg, sizeof(double) * g.np * N));
   CK(cudaMalloc(&c->red, 8 * sizeof(unsigned long long)));
   CK(cudaMemsetAsync(c->red, 0, 8 * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(c->R, 0, c->es * (size_t)nr_pairs(ndim) * N, c->stream));
   CK(cudaMemcpyAsync(c->x, hx.data(), sizeof(double) * ndim * N, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dx, hdx.data(), sizeof(double) * ndim * N, cudaMemcpyHostToDevice, c->stream));
+  if (!hdrv.empty())
+    CK(cudaMemcpyAsync(c->drv, hdrv.data(), sizeof(double) * 2 * N, cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->grid_set = true;
   c->bc_set = false;
@@ -528,7 +625,13 @@ sac_status sac_upload(sac_ctx* c, const double* w) {
   CK(cudaSetDevice(c->dev));
   const Geom& g = c->g;
   const long N = g.ncell;
-  CK(cudaMemcpyAsync(c->P[0], w, sizeof(double) * g.np * N, cudaMemcpyHostToDevice, c->stream));
+  if (c->prec == SAC_PREC_FP32) {
+    CK(cudaMemcpyAsync(c->stg, w, sizeof(double) * g.np * N, cudaMemcpyHostToDevice, c->stream));
+    Prof pr(c, SAC_K_OTHER);
+    k_convert<float, double><<<592, 256, 0, c->stream>>>((float*)c->P[0], c->stg, (long)g.np * N);
+  } else {
+    CK(cudaMemcpyAsync(c->P[0], w, sizeof(double) * g.np * N, cudaMemcpyHostToDevice, c->stream));
+  }
   CK(cudaMemcpyAsync(c->BG, w + (long)g.np * N, sizeof(double) * (g.nw - g.np) * N, cudaMemcpyHostToDevice,
                      c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -542,7 +645,15 @@ sac_status sac_download(sac_ctx* c, double* w) {
   CK(cudaSetDevice(c->dev));
   const Geom& g = c->g;
   const long N = g.ncell;
-  CK(cudaMemcpyAsync(w, c->P[0], sizeof(double) * g.np * N, cudaMemcpyDeviceToHost, c->stream));
+  if (c->prec == SAC_PREC_FP32) {
+    {
+      Prof pr(c, SAC_K_OTHER);
+      k_convert<double, float><<<592, 256, 0, c->stream>>>(c->stg, (const float*)c->P[0], (long)g.np * N);
+    }
+    CK(cudaMemcpyAsync(w, c->stg, sizeof(double) * g.np * N, cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    CK(cudaMemcpyAsync(w, c->P[0], sizeof(double) * g.np * N, cudaMemcpyDeviceToHost, c->stream));
+  }
   CK(cudaMemcpyAsync(w + (long)g.np * N, c->BG, sizeof(double) * (g.nw - g.np) * N, cudaMemcpyDeviceToHost,
                      c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -558,7 +669,10 @@ sac_status sac_getboundary(sac_ctx* c, double t) {
   const Geom& g = c->g;
   BcArgs b = bc_args(c, c->P[0]);
   b.init = c->bc_init_done ? 0 : 1;
-  launch_bound(c, b, g.nw);
+  if (c->prec == SAC_PREC_FP32)
+    launch_bound<float>(c, b, g.nw);
+  else
+    launch_bound<double>(c, b, g.nw);
   if (!c->bc_init_done) {
     const int nB = 2 * g.ndim;
     for (int iB = 0; iB < nB; ++iB)
@@ -566,8 +680,15 @@ sac_status sac_getboundary(sac_ctx* c, double t) {
         const int8_t ty = c->h_type[iw * nB + iB];
         if ((ty == BT_FIXED || ty == BT_FIXED1 || ty == BT_GRAD1) && !c->h_fixed[iw * nB + iB]) {
           const int bs = 256;
-          k_fixcapture<<<(unsigned)((c->slab[iB] + bs - 1) / bs), bs, 0, c->stream>>>(
-              g, c->P[0], c->BG, c->fixB, c->fixoff[iB], c->slab[iB], iw, iB / 2, iB % 2, ty == BT_GRAD1 ? 1 : 0);
+          Prof pr(c, SAC_K_OTHER);
+          const unsigned nb = (unsigned)((c->slab[iB] + bs - 1) / bs);
+          if (c->prec == SAC_PREC_FP32)
+            k_fixcapture<float><<<nb, bs, 0, c->stream>>>(g, (const float*)c->P[0], c->BG, c->fixB, c->fixoff[iB],
+                                                          c->slab[iB], iw, iB / 2, iB % 2, ty == BT_GRAD1 ? 1 : 0);
+          else
+            k_fixcapture<double><<<nb, bs, 0, c->stream>>>(g, (const double*)c->P[0], c->BG, c->fixB,
+                                                           c->fixoff[iB], c->slab[iB], iw, iB / 2, iB % 2,
+                                                           ty == BT_GRAD1 ? 1 : 0);
           c->h_fixed[iw * nB + iB] = 1;
         }
       }
@@ -600,12 +721,22 @@ sac_status sac_getdt(sac_ctx* c, double* dt, int it) {
       const long nm = (long)(g.hi[0] - g.lo[0] + 1) * (g.hi[1] - g.lo[1] + 1) * (g.hi[2] - g.lo[2] + 1);
       const int bs = 256;
       const unsigned nb = (unsigned)std::min<long>((nm + bs - 1) / bs, 148L * 16);
-      switch (g.ndir) {
-        case 1: k_courant<1><<<nb, bs, 0, c->stream>>>(g, c->P[0], c->BG, c->dx, c->red + 4, c->par.gamma); break;
-        case 2: k_courant<2><<<nb, bs, 0, c->stream>>>(g, c->P[0], c->BG, c->dx, c->red + 4, c->par.gamma); break;
-        default: k_courant<3><<<nb, bs, 0, c->stream>>>(g, c->P[0], c->BG, c->dx, c->red + 4, c->par.gamma); break;
+      {
+      Prof pr(c, SAC_K_COURANT);
+      auto launch = [&](auto S0) {
+        using S = decltype(S0);
+        const S* wp = (const S*)c->P[0];
+        switch (g.ndir) {
+          case 1: k_courant<1, S><<<nb, bs, 0, c->stream>>>(g, wp, c->BG, c->dx, c->red + 4, c->par.gamma); break;
+          case 2: k_courant<2, S><<<nb, bs, 0, c->stream>>>(g, wp, c->BG, c->dx, c->red + 4, c->par.gamma); break;
+          default: k_courant<3, S><<<nb, bs, 0, c->stream>>>(g, wp, c->BG, c->dx, c->red + 4, c->par.gamma); break;
+        }
+      };
+      if (c->prec == SAC_PREC_FP32)
+        launch(0.0f);
+      else
+        launch(0.0);
       }
-      c->kernel_launches++;
       unsigned long long bits = 0;
       CK(cudaMemcpyAsync(&bits, c->red + 4, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
@@ -672,8 +803,8 @@ sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmi
     mask = (1u << g.np) - 1u;
   }
   const int dmin = idimmin - 1, dmax = idimmax - 1;
-  double *w = c->P[0], *w1 = c->P[1], *w2 = c->P[2], *w3 = c->P[3];
-  const size_t bytes = sizeof(double) * g.np * g.ncell;
+  void *w = c->P[0], *w1 = c->P[1], *w2 = c->P[2], *w3 = c->P[3];
+  const size_t bytes = c->es * g.np * g.ncell;
   const std::string ta(c->par.typeadvance);
   sac_status st = SAC_OK;
 #define RUN(x)                    \
@@ -698,9 +829,21 @@ sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmi
     const long n = (long)g.np * g.ncell;
     CK(cudaMemcpyAsync(w1, w, bytes, cudaMemcpyDeviceToDevice, c->stream));
     RUN(advect1(c, m, dt, dmin, dmax, t, w, w1, w1, mask));
-    k_lin_threestep_a<<<592, 256, 0, c->stream>>>(w2, w, w1, n);
+    {
+      Prof pr(c, SAC_K_OTHER);
+      if (c->prec == SAC_PREC_FP32)
+        k_lin_threestep_a<float><<<592, 256, 0, c->stream>>>((float*)w2, (const float*)w, (const float*)w1, n);
+      else
+        k_lin_threestep_a<double><<<592, 256, 0, c->stream>>>((double*)w2, (const double*)w, (const double*)w1, n);
+    }
     RUN(advect1(c, m, dt / 4, dmin, dmax, t + dt / 4, w1, w2, w2, mask));
-    k_lin_threestep_b<<<592, 256, 0, c->stream>>>(w, w2, n);
+    {
+      Prof pr(c, SAC_K_OTHER);
+      if (c->prec == SAC_PREC_FP32)
+        k_lin_threestep_b<float><<<592, 256, 0, c->stream>>>((float*)w, (const float*)w2, n);
+      else
+        k_lin_threestep_b<double><<<592, 256, 0, c->stream>>>((double*)w, (const double*)w2, n);
+    }
     RUN(advect1(c, m, dt * 2.0 / 3, dmin, dmax, t + dt / 3, w2, w, w, mask));
   } else if (ta == "sterck") {
     const double c012 = (double)0.12f;  // default-real literal in src/vac.t:459
@@ -786,5 +929,37 @@ sac_status sac_diag(sac_ctx* c, sac_diag_out* out) {
 
 // Number of kernels this library launched on the context (benchmark accounting).
 long sac_kernel_launches(const sac_ctx* c) { return c ? c->kernel_launches : 0; }
+
+sac_status sac_set_stream(sac_ctx* c, void* stream) {
+  if (!c) return SAC_ERR_ARG;
+  CK(cudaSetDevice(c->dev));
+  CK(cudaStreamSynchronize(c->stream));
+  prof_collect(c);
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return SAC_OK;
+}
+
+void* sac_get_stream(const sac_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+sac_status sac_profile(sac_ctx* c, int enable) {
+  if (!c) return SAC_ERR_ARG;
+  CK(cudaSetDevice(c->dev));
+  prof_collect(c);
+  c->prof = enable != 0;
+  return SAC_OK;
+}
+
+sac_status sac_profile_read(sac_ctx* c, int kernel, double* total_ms, long* launches, int reset) {
+  if (!c || kernel < 0 || kernel >= SAC_K_COUNT) return SAC_ERR_ARG;
+  CK(cudaSetDevice(c->dev));
+  prof_collect(c);
+  if (total_ms) *total_ms = c->prof_ms[kernel];
+  if (launches) *launches = c->prof_n[kernel];
+  if (reset) {
+    c->prof_ms[kernel] = 0;
+    c->prof_n[kernel] = 0;
+  }
+  return SAC_OK;
+}
 
 }  // extern "C"

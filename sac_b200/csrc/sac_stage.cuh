@@ -1,0 +1,519 @@
+// sac_stage.cuh -- the RK stage as three passes that each evaluate a quantity once.
+//
+//   k_face   per cell: rho+rhob, v=m/(rho+rhob), the "173" energy
+//            e-(b^2+m^2/rho)/2, p'_tot (getptotal), the perturbed fluxes of every
+//            advanced variable along every dimension (getflux + transport,
+//            src/vacphys.mhd0.t:147-222, src/vaccd.t:43-46) and the per-dimension
+//            maxima c_tot of getcmax over the mesh (src/vacphys0.t.mhd:77-160).
+//   k_nu     per cell and per (field, dimension) pair of setnu: the face quotient
+//            Q = (c_tot c_hyp max3 d3R)/max5 d1R (0 where max5 d1R is 0) at the
+//            face c+1/2 (src/vacusr.viscosity.t:372-450), so that
+//            nu_R(i) = Q(i) dx(i) and nu_L(i) = Q(i-1) dx(i).
+//   k_update per mesh cell: flux divergence with gradient4's edge zeroing, the
+//            e-equation background work, gravity, the hyperdiffusion terms of
+//            addsource_visc, the user driver and the Runge-Kutta epilogue.
+//
+// S is the storage type of the advanced variables and of D, F and Q.  Every
+// expression is written in the reference's evaluation order.  The FP64
+// instantiation is compiled without contraction and with IEEE division
+// (stage_f64.cu): the reference's hyperdiffusion switch max|d3|/max|d1| is
+// scale-free, so rounding noise at a wave front is amplified to order one, and
+// only bit-faithful arithmetic keeps the device on the reference's trajectory.
+// The FP32 instantiation (stage_f32.cu) may contract and approximate.
+#pragma once
+#include "sac_kernels.cuh"
+#include "sac_stage_api.h"
+
+namespace sacgpu {
+
+
+template <typename S>
+__device__ __forceinline__ S ld(const S* p, int i) {
+  return __ldg(p + i);
+}
+__device__ __forceinline__ double fmaxT(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float fmaxT(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fabsT(double a) { return fabs(a); }
+__device__ __forceinline__ float fabsT(float a) { return fabsf(a); }
+
+// ---------------------------------------------------------------------------
+// k_face (computes in FP64 for both storage types)
+// ---------------------------------------------------------------------------
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_face(Geom g, const S* __restrict__ wp, const double* __restrict__ bgv,
+                                              S* __restrict__ D, S* __restrict__ F, unsigned long long* ctot,
+                                              double gamma, int do_ctot) {
+  __shared__ double sh[32];
+  constexpr int NP = 2 * NDIR + 2, E = NDIR + 1;
+  const int N = (int)g.ncell;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double cm[NDIM];
+#pragma unroll
+  for (int d = 0; d < NDIM; ++d) cm[d] = 0.0;
+  if (c < N) {
+    const double rho = (double)wp[c];
+    const double eb = bgv[c];
+    const double rhob = bgv[N + c];
+    const double rt = rho + rhob;
+    double m[NDIR], b[NDIR], bg[NDIR], v[NDIR];
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) {
+      m[C] = (double)wp[(1 + C) * N + c];
+      b[C] = (double)wp[(E + 1 + C) * N + c];
+      bg[C] = bgv[(2 + C) * N + c];
+    }
+    const double e = (double)wp[E * N + c];
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) v[C] = div_rn(m[C], rt);  // getv / tmp_nu for m
+    double b2 = 0.0, m2 = 0.0, bb = 0.0;
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) {
+      b2 = add_rn(b2, mul_rn(b[C], b[C]));
+      m2 = add_rn(m2, mul_rn(m[C], m[C]));
+      bb = add_rn(bb, mul_rn(b[C], bg[C]));
+    }
+    D[c] = (S)rt;
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) D[(1 + C) * N + c] = (S)v[C];
+    // tmp_nu for iw=173, src/vacusr.viscosity.t:301
+    D[(NDIR + 1) * N + c] = (S)sub_rn(e, mul_rn(0.5, add_rn(b2, div_rn(m2, rt))));
+    // getptotal, src/vacphys0.t.mhd:199-201
+    const double pp = (gamma - 2.0) * (bb + 0.5 * b2);
+    const double ptot = (gamma - 1.0) * (e - 0.5 * m2 / rt) - pp;
+    D[(NDIR + 2) * N + c] = (S)ptot;
+    double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) s1 = s1 + bg[C] * m[C];
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) s2 = s2 + b[C] * m[C];
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+      S* Fd = F + (long)d * NP * N;
+      const double vd = v[d], bd = b[d], bgd = bg[d], md = m[d];
+      Fd[c] = (S)(rhob * md / rt + vd * rho);
+#pragma unroll
+      for (int C = 0; C < NDIR; ++C) {
+        double f;
+        if (C == d)
+          f = (ptot + 0.0) - (b[C] * bgd + bd * bg[C]) - b[C] * bd;
+        else
+          f = -(b[C] * bgd + bd * bg[C]) - b[C] * bd;
+        Fd[(1 + C) * N + c] = (S)(f + vd * m[C]);
+      }
+      const double fe = (md * (ptot + 0.0) - bd * s1 - bgd * s2) / rt + eb * md / rt - bd * s2 / rt;
+      Fd[E * N + c] = (S)(fe + vd * e);
+#pragma unroll
+      for (int C = 0; C < NDIR; ++C)
+        Fd[(E + 1 + C) * N + c] = (C == d) ? (S)0 : (S)(-(v[C] * (bd + bgd)) + vd * bg[C] + vd * b[C]);
+    }
+    if (do_ctot) {
+      const int p0 = c % g.n[0];
+      const int p1 = (c / g.n[0]) % g.n[1];
+      const int p2 = c / (g.n[0] * g.n[1]);
+      const bool mesh = p0 >= g.lo[0] && p0 <= g.hi[0] && p1 >= g.lo[1] && p1 <= g.hi[1] && p2 >= g.lo[2] &&
+                        p2 <= g.hi[2];
+      if (mesh) {
+        // getpthermal, getcsound2, getcmax: src/vacphys0.t.mhd:95-183
+        double q = 0.5 * m2 / rt;
+        q = q + 0.5 * b2 + bb;
+        const double p = (gamma - 1.0) * (e - q);
+        double bgs = 0.0, Bt2 = 0.0;
+#pragma unroll
+        for (int C = 0; C < NDIR; ++C) bgs = bgs + bg[C] * bg[C];
+        const double cs2 = gamma * (p + (gamma - 1.0) * (eb - 0.5 * bgs)) / rt;
+#pragma unroll
+        for (int C = 0; C < NDIR; ++C) {
+          const double B = b[C] + bg[C];
+          Bt2 = Bt2 + B * B;
+        }
+        const double cf2 = Bt2 / rt + cs2;
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+          const double Bd = b[d] + bg[d];
+          cm[d] = sqrt(0.5 * (cf2 + sqrt(cf2 * cf2 - 4.0 * cs2 * (Bd * Bd) / rt))) + fabs(m[d] / rt);
+        }
+      }
+    }
+  }
+  if (do_ctot) {
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) block_max_to(&ctot[d], cm[d], sh);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_nu: face quotients for every setnu pair on the box [lo-1, hi] of each used dim
+// ---------------------------------------------------------------------------
+template <typename S>
+__device__ __forceinline__ S face_quotient(const S* __restrict__ q, int c, int s, int pos, int lo, int hi, S pre) {
+  // q(c-2..c+3) along s; the layer beyond the two ghosts is the mirror image
+  // about the first/last mesh cell (tmp_nuI, src/vacusr.viscosity.t:378-400)
+  S a[6];
+#pragma unroll
+  for (int o = -2; o <= 3; ++o) {
+    int p = pos + o;
+    if (p <= lo - 3) p = lo + 3;
+    if (p >= hi + 3) p = hi - 3;
+    a[o + 2] = ld(q, c + (p - pos) * s);
+  }
+  S d1[5], d3[3];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) d1[j] = fabsT(a[j + 1] - a[j]);  // d1R(c-2+j), :414
+#pragma unroll
+  for (int j = 0; j < 3; ++j)  // d3R(c-1+j), :413
+    d3[j] = fabsT(sub_rn(mul_rn(S(3), sub_rn(a[j + 2], a[j + 1])), sub_rn(a[j + 3], a[j])));
+  const S md3 = fmaxT(fmaxT(d3[0], d3[1]), d3[2]);
+  const S md1 = fmaxT(fmaxT(fmaxT(fmaxT(d1[0], d1[1]), d1[2]), d1[3]), d1[4]);
+  const S r = pre * md3 / md1;  // c_tot*c_hyp*md3R/md1R, :424
+  return (md1 > S(0)) ? r : S(0);
+}
+
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_nu(Geom g, const S* __restrict__ wp, const S* __restrict__ D,
+                                            S* __restrict__ R, const unsigned long long* ctot) {
+  using PR = Pairs<NDIM>;
+  constexpr int E = NDIR + 1;
+  const int N = (int)g.ncell;
+  int ext[3], p[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) ext[d] = (d < NDIM) ? (g.hi[d] - g.lo[d] + 2) : 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ext[0] * ext[1] * ext[2]) return;
+  p[0] = t % ext[0];
+  p[1] = (t / ext[0]) % ext[1];
+  p[2] = t / (ext[0] * ext[1]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) p[d] += (d < NDIM) ? g.lo[d] - 1 : 0;
+  const int c = p[0] + (int)g.st[1] * p[1] + (int)g.st[2] * p[2];
+#pragma unroll
+  for (int k = 0; k < NDIM; ++k) {
+    const int s = (int)g.st[k];
+    const int pos = p[k], lo = g.lo[k], hi = g.hi[k];
+    const double ct = __longlong_as_double((long long)ctot[k]);
+    // c_hyp: 0.04 for rho, the "173" energy and b; 0.4 for the momenta (:284-290)
+    const S p04 = (S)(ct * 0.04), p4 = (S)(ct * 0.4);
+    R[(long)PR::rho(k) * N + c] = face_quotient(wp, c, s, pos, lo, hi, p04);
+    R[(long)PR::e(k) * N + c] = face_quotient(D + (NDIR + 1) * N, c, s, pos, lo, hi, p04);
+#pragma unroll
+    for (int l = 0; l < NDIM; ++l) {
+      R[(long)PR::v(l, k) * N + c] = face_quotient(D + (1 + l) * N, c, s, pos, lo, hi, p4);
+      if (l != k) R[(long)PR::b(l, k) * N + c] = face_quotient(wp + (E + 1 + l) * N, c, s, pos, lo, hi, p04);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_update
+// ---------------------------------------------------------------------------
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
+  using PR = Pairs<NDIM>;
+  using T = S;
+  constexpr int NP = 2 * NDIR + 2, E = NDIR + 1, B0 = NDIR + 1;
+  __shared__ double sh[32];
+  const Geom& g = a.g;
+  const int N = (int)g.ncell;
+  int pos[3];
+  pos[0] = g.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  pos[1] = g.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  pos[2] = g.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
+  const bool active = pos[0] <= g.hi[0] && pos[1] <= g.hi[1] && pos[2] <= g.hi[2];
+  T numax = T(0);
+  if (active) {
+    const int st[3] = {1, (int)g.st[1], (int)g.st[2]};
+    const int c = pos[0] + st[1] * pos[1] + st[2] * pos[2];
+    const S* wp = (const S*)a.wct;
+    const S* D = (const S*)a.D;
+    const S* F = (const S*)a.F;
+    const S* Q = (const S*)a.R;
+    const S* base = (const S*)a.base;
+    const double* bgv = a.bgv;
+    T acc[NP];
+#pragma unroll
+    for (int iw = 0; iw < NP; ++iw) acc[iw] = base[iw * N + c];
+    T dxv[NDIM];
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) dxv[d] = (T)__ldg(a.dx + d * N + c);
+    // gradient4 (src/vacgrid.t:684): -(q(+2) - 8(q(+1)-q(-1)) - q(-2))/dx/12, zero on
+    // the first and last two mesh cells along its dimension (:690-709)
+    bool z4[NDIM];
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) z4[d] = pos[d] <= g.lo[d] + 1 || pos[d] >= g.hi[d] - 1;
+    auto g4 = [&](const S* q, int s, T dxd) {
+      return -(ld(q, c + 2 * s) - T(8) * (ld(q, c + s) - ld(q, c - s)) - ld(q, c - 2 * s)) / dxd / T(12);
+    };
+    const T qdt = (T)a.qdt;
+
+    // --- centdiff4 (src/vaccd.t:35-70) -----------------------------------------
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+      if (d < a.dmin || d > a.dmax) continue;
+      if (!z4[d]) {
+        const S* Fd = F + (long)d * NP * N;
+#pragma unroll
+        for (int iw = 0; iw < NP; ++iw) {
+          if (iw == B0 + 1 + d) continue;  // no flux of b_d along d
+          if (!((a.iwmask >> iw) & 1u)) continue;
+          acc[iw] = acc[iw] - qdt * g4(Fd + iw * N, st[d], dxv[d]);
+        }
+      }
+      if ((a.iwmask >> E) & 1u) {
+        const S* vd = D + (1 + d) * N;
+        if (!z4[d]) {
+          // getptotal_bg, src/vacphys0.t.mhd:221
+          double bgs = 0.0;
+#pragma unroll
+          for (int C = 0; C < NDIR; ++C) bgs = bgs + __ldg(bgv + (2 + C) * N + c) * __ldg(bgv + (2 + C) * N + c);
+          const T fb = (T)((a.gamma - 1.0) * __ldg(bgv + c) - 0.5 * (a.gamma - 2.0) * bgs);
+          acc[E] = acc[E] - qdt * g4(vd, st[d], dxv[d]) * fb;
+        }
+#pragma unroll
+        for (int di = 0; di < NDIM; ++di) {
+          if (di < a.dmin || di > a.dmax || z4[di]) continue;
+          acc[E] = acc[E] + qdt * (T)__ldg(bgv + (2 + di) * N + c) * (T)__ldg(bgv + (2 + d) * N + c) *
+                                g4(vd, st[di], dxv[di]);
+        }
+      }
+    }
+
+    const T q2 = (T)a.qdt2;
+    // --- gravity, src/vacusr.gravity.t:46-78 ---------------------------------------
+    if (a.grav_on) {
+      const T rho = ld(wp, c);
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d)
+        if (((a.iwmask >> (1 + d)) & 1u) && fabs(a.grav[d]) > kSmall)
+          acc[1 + d] = acc[1 + d] + q2 * (T)a.grav[d] * rho;
+      if ((a.iwmask >> E) & 1u) {
+        const T rt = ld(D, c);
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d)
+          if (fabs(a.grav[d]) > kSmall) acc[E] = acc[E] + q2 * (T)a.grav[d] * rho * ld(wp + (1 + d) * N, c) / rt;
+      }
+    }
+
+    // --- hyperdiffusion, src/vacusr.viscosity.t:2-221 --------------------------------
+    if (a.visc_on) {
+      // gradient1* zero rule: edge mesh cells along a non-periodic dimension
+      bool z1[NDIM];
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d)
+        z1[d] = (a.zero1[d][0] && pos[d] == g.lo[d]) || (a.zero1[d][1] && pos[d] == g.hi[d]);
+      auto nus = [&](int ip, int k, int j, T dxk, T& nl, T& nr) {
+        nr = ld(Q + (long)ip * N, j) * dxk;
+        nl = ld(Q + (long)ip * N, j - st[k]) * dxk;
+      };
+      // density and the "173" energy, :45-64
+#pragma unroll
+      for (int pass = 0; pass < 2; ++pass) {
+        const S* q = pass == 0 ? wp : D + (NDIR + 1) * N;
+        const int tgt = pass == 0 ? 0 : E;
+#pragma unroll
+        for (int k = 0; k < NDIM; ++k) {
+          T nl, nr;
+          nus(pass == 0 ? PR::rho(k) : PR::e(k), k, c, dxv[k], nl, nr);
+          numax = fmaxT(numax, fmaxT(nr, nl));
+          const T qc = ld(q, c);
+          const T gL = z1[k] ? T(0) : (qc - ld(q, c - st[k])) / dxv[k];
+          const T gR = z1[k] ? T(0) : (ld(q, c + st[k]) - qc) / dxv[k];
+          const T tL = (nl + T(0)) * gL, tR = (nr + T(0)) * gR;
+          acc[tgt] = acc[tgt] + (tR - tL) / dxv[k] * q2;
+        }
+      }
+      // momentum, :69-133
+      const S* rtf = D;
+#pragma unroll
+      for (int k = 0; k < NDIM; ++k) {
+        const int sk = st[k];
+        const T dxk = dxv[k];
+        const T rC = ld(rtf, c);
+        const T rL = (rC + ld(rtf, c - sk)) / T(2), rR = (ld(rtf, c + sk) + rC) / T(2);
+#pragma unroll
+        for (int l = 0; l < NDIM; ++l) {
+          const S* q = D + (1 + l) * N;  // v_l
+          T nl, nr;
+          nus(PR::v(l, k), k, c, dxk, nl, nr);
+          numax = fmaxT(numax, fmaxT(nr, nl));
+          const T qc = ld(q, c);
+          const T gL = z1[k] ? T(0) : (qc - ld(q, c - sk)) / dxk;
+          const T gR = z1[k] ? T(0) : (ld(q, c + sk) - qc) / dxk;
+          const T tL = (nl + T(0)) * gL, tR = (nr + T(0)) * gR;
+          const S* ml = wp + (1 + l) * N;
+          const T mc = ld(ml, c);
+          const T VL = (mc + ld(ml, c - sk)) / T(2), VR = (ld(ml, c + sk) + mc) / T(2);
+          const T t2m = (rR * tR - rL * tL) / dxk / T(2);
+          const T t2e = (VR * tR - VL * tL) / dxk / T(2);
+          // ii1=0: i=k, ii0=l
+          acc[1 + l] = acc[1 + l] + t2m * q2;
+          acc[E] = acc[E] + t2e * q2;
+          if (l == k) {
+            // ii1=1 with l==k takes the i==k branch a second time
+            acc[1 + l] = acc[1 + l] + t2m * q2;
+            acc[E] = acc[E] + t2e * q2;
+          } else {
+            // ii1=1: i=l, ii0=k
+            const int sl = st[l];
+            T Tm[2], Te[2];
+#pragma unroll
+            for (int sg = 0; sg < 2; ++sg) {
+              const int j = sg ? c + sl : c - sl;
+              const int pl = pos[l] + (sg ? 1 : -1);
+              T H = T(0);
+              if (pl >= g.lo[l] && pl <= g.hi[l]) {  // nu vanishes outside the mesh
+                const T dxkj = (T)__ldg(a.dx + k * N + j);
+                T njl, njr;
+                nus(PR::v(l, k), k, j, dxkj, njl, njr);
+                const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
+                H = gC * (njl + njr + T(2) * T(0)) / T(2) / T(2);
+              }
+              Tm[sg] = ld(rtf, j) * H;
+              Te[sg] = ld(wp + (1 + k) * N, j) * H;
+            }
+            const T dxl = dxv[l];
+            const T tCm = z1[l] ? T(0) : (Tm[1] - Tm[0]) / dxl / T(2);
+            const T tCe = z1[l] ? T(0) : (Te[1] - Te[0]) / dxl / T(2);
+            acc[1 + k] = acc[1 + k] + tCm * q2;
+            acc[E] = acc[E] + tCe * q2;
+          }
+        }
+      }
+      // magnetic field, :139-215
+#pragma unroll
+      for (int k = 0; k < NDIM; ++k)
+#pragma unroll
+        for (int l = 0; l < NDIM; ++l) {
+          if (k == l) continue;
+          const int sk = st[k], sl = st[l];
+          const T dxk = dxv[k];
+          const S* q = wp + (B0 + 1 + l) * N;  // b_l
+          T nl, nr;
+          nus(PR::b(l, k), k, c, dxk, nl, nr);
+          numax = fmaxT(numax, fmaxT(nr, nl));
+          // ii1=0: ii0=k, m=l, sB=-1, j=k (m /= k branch)
+          {
+            T K[2], Ke[2];
+#pragma unroll
+            for (int sg = 0; sg < 2; ++sg) {
+              const int j = sg ? c + sl : c - sl;
+              const int pl = pos[l] + (sg ? 1 : -1);
+              T Kv = T(0);
+              if (pl >= g.lo[l] && pl <= g.hi[l]) {
+                const T dxkj = (T)__ldg(a.dx + k * N + j);
+                T njl, njr;
+                nus(PR::b(l, k), k, j, dxkj, njl, njr);
+                const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
+                Kv = gC * (njl + njr) / T(2);
+              }
+              K[sg] = Kv;
+              Ke[sg] = Kv * ld(wp + (B0 + 1 + k) * N, j);
+            }
+            const T dxl = dxv[l];
+            const T tC = z1[l] ? T(0) : (K[1] - K[0]) / dxl / T(2);
+            const T tCe = z1[l] ? T(0) : (Ke[1] - Ke[0]) / dxl / T(2);
+            acc[B0 + 1 + k] = acc[B0 + 1 + k] + T(-1) * tC * q2;
+            acc[E] = acc[E] + T(-1) * tCe * q2;
+          }
+          // ii1=1: ii0=l, m=k, sB=+1, j=l (m == k branch)
+          {
+            const T qc = ld(q, c), qm = ld(q, c - sk), qp = ld(q, c + sk);
+            const T BL = (qc + qm) / T(2), BR = (qp + qc) / T(2);
+            const T gL = z1[k] ? T(0) : (qc - qm) / dxk;
+            const T gR = z1[k] ? T(0) : (qp - qc) / dxk;
+            const T tL = nl * gL, tR = nr * gR;
+            acc[B0 + 1 + l] = acc[B0 + 1 + l] + T(1) * (tR - tL) / dxk * q2;
+            acc[E] = acc[E] + T(1) * (tR * BR - tL * BL) / dxk * q2;
+          }
+        }
+    }
+
+    // --- user driver: tdep from the host, spatial profiles precomputed there -----------
+    if (a.driver != DRV_NONE) {
+      const T rtn = (T)((double)acc[0] + __ldg(bgv + N + c));
+      if (a.driver == DRV_SLOG) {
+        // src/vacusr.f:1355-1375 (x1 vertical; m2, m3 driven)
+        const T vvx = (T)(__ldg(a.drv + c) * a.tdep * a.drvA);
+        const T vvy = (T)(__ldg(a.drv + N + c) * a.tdep * a.drvA);
+        if (NDIR >= 3) {
+          acc[2] = acc[2] + rtn * vvx * q2;
+          acc[3 % NP] = acc[3 % NP] + rtn * vvy * q2;
+        }
+        acc[E] = acc[E] + rtn * (vvx * vvx + vvy * vvy + T(0) * T(0)) * q2 / T(2);
+      } else {
+        const T v = (T)(a.drvA * a.tdep * __ldg(a.drv + c) * __ldg(a.drv + N + c));
+        const int comp = (a.driver == DRV_STRAT) ? 1 : 2;
+        acc[comp] = acc[comp] + rtn * v * q2;
+        acc[E] = acc[E] + rtn * (v * v) * q2 / T(2);
+      }
+    }
+
+    // --- store with the Runge-Kutta epilogue (src/vac.t:450,454) ---------------------
+    S* out = (S*)a.out;
+    if (a.epi == EPI_PLAIN) {
+#pragma unroll
+      for (int iw = 0; iw < NP; ++iw) out[iw * N + c] = acc[iw];
+    } else if (a.epi == EPI_RK4_S3) {
+      S* w1 = (S*)a.aux1;
+      const S* w2 = (const S*)a.aux2;
+#pragma unroll
+      for (int iw = 0; iw < NP; ++iw) {
+        const T w3 = acc[iw];
+        out[iw * N + c] = w3;
+        w1[iw * N + c] = (w1[iw * N + c] + T(2) * w2[iw * N + c] + w3 - T(4) * base[iw * N + c]) / T(3);
+      }
+    } else {
+      const S* w1 = (const S*)a.aux1;
+#pragma unroll
+      for (int iw = 0; iw < NP; ++iw) out[iw * N + c] = acc[iw] + w1[iw * N + c];
+    }
+  }
+  if (a.visc_on) block_max_to(a.maxnu, (double)numax, sh);
+}
+
+// ---------------------------------------------------------------------------
+// launchers (instantiated per storage type in stage_f64.cu / stage_f32.cu)
+// ---------------------------------------------------------------------------
+template <typename Fn>
+void dispatch_nd(const Geom& g, Fn&& f) {
+  const int nd = g.ndim, nr = g.ndir;
+  if (nd == 1 && nr == 1) f(std::integral_constant<int, 1>{}, std::integral_constant<int, 1>{});
+  else if (nd == 1 && nr == 2) f(std::integral_constant<int, 1>{}, std::integral_constant<int, 2>{});
+  else if (nd == 1 && nr == 3) f(std::integral_constant<int, 1>{}, std::integral_constant<int, 3>{});
+  else if (nd == 2 && nr == 2) f(std::integral_constant<int, 2>{}, std::integral_constant<int, 2>{});
+  else if (nd == 2 && nr == 3) f(std::integral_constant<int, 2>{}, std::integral_constant<int, 3>{});
+  else f(std::integral_constant<int, 3>{}, std::integral_constant<int, 3>{});
+}
+
+template <typename S>
+void launch_face(const Geom& g, const void* wct, const double* bg, void* D, void* F, unsigned long long* ctot,
+                 double gamma, int do_ctot, cudaStream_t st) {
+  const int N = (int)g.ncell;
+  dispatch_nd(g, [&](auto ND, auto NR) {
+    k_face<decltype(ND)::value, decltype(NR)::value, S><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
+        g, (const S*)wct, bg, (S*)D, (S*)F, ctot, gamma, do_ctot);
+  });
+}
+
+template <typename S>
+void launch_nu(const Geom& g, const void* wct, const void* D, void* R, const unsigned long long* ctot,
+               cudaStream_t st) {
+  long nb = 1;
+  for (int d = 0; d < g.ndim; ++d) nb *= (g.hi[d] - g.lo[d] + 2);
+  dispatch_nd(g, [&](auto ND, auto NR) {
+    k_nu<decltype(ND)::value, decltype(NR)::value, S><<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(
+        g, (const S*)wct, (const S*)D, (S*)R, ctot);
+  });
+}
+
+template <typename S>
+void launch_update(const Stage2Args& a, cudaStream_t st) {
+  const Geom& g = a.g;
+  dispatch_nd(g, [&](auto ND, auto NR) {
+    constexpr int NDIM = decltype(ND)::value;
+    dim3 blk = NDIM == 1 ? dim3(256, 1, 1) : (NDIM == 2 ? dim3(32, 8, 1) : dim3(32, 4, 2));
+    const int n0 = g.hi[0] - g.lo[0] + 1, n1 = g.hi[1] - g.lo[1] + 1, n2 = g.hi[2] - g.lo[2] + 1;
+    dim3 grd((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, (n2 + blk.z - 1) / blk.z);
+    k_update<NDIM, decltype(NR)::value, S><<<grd, blk, 0, st>>>(a);
+  });
+}
+
+}  // namespace sacgpu

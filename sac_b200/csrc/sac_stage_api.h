@@ -1,0 +1,71 @@
+// sac_stage_api.h -- host-visible interface of the stage kernels (sac_stage.cuh).
+// The kernels are instantiated per storage type in their own translation units:
+// stage_f64.cu (no contraction, IEEE division) and stage_f32.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "sac_kernels.cuh"
+
+namespace sacgpu {
+
+template <int NDIM>
+struct Pairs {
+  // setnu pairs: rho(k), e173(k), v_l(k) (all l), b_l(k) (l != k)
+  static constexpr int NR = 2 * NDIM + NDIM * NDIM + NDIM * (NDIM - 1);
+  static __host__ __device__ constexpr int rho(int k) { return k; }
+  static __host__ __device__ constexpr int e(int k) { return NDIM + k; }
+  static __host__ __device__ constexpr int v(int l, int k) { return 2 * NDIM + l * NDIM + k; }
+  static __host__ __device__ constexpr int b(int l, int k) {
+    return 2 * NDIM + NDIM * NDIM + l * (NDIM - 1) + (k < l ? k : k - 1);
+  }
+};
+
+inline int nr_pairs(int ndim) { return 2 * ndim + ndim * ndim + ndim * (ndim - 1); }
+
+struct Stage2Args {
+  Geom g;
+  const void* wct;   // S[np][N]   stage input, advanced variables
+  const double* bgv; // double[nb][N] eb, rhob, bg1..
+  const void* base;  // S[np][N]   may alias out
+  void* out;         // S[np][N]
+  void* aux1;        // S[np][N]   RK4 accumulator
+  const void* aux2;  // S[np][N]   w2 for the stage-3 epilogue
+  const void* D;     // S[ndir+3][N] rho+rhob, v.., e173, p'_tot
+  const void* F;     // S[ndim*np][N] fluxes, F[d*np+iw]
+  const void* R;     // S[NR][N]   setnu face quotients
+  const double* dx;  // double[ndim][N]
+  const double* drv; // driver profiles [2][N] or nullptr
+  const unsigned long long* ctot;
+  unsigned long long* maxnu;
+  double qdt, qdt2, gamma, tdep;
+  double grav[3];
+  double drvA;
+  int dmin, dmax;
+  unsigned iwmask;
+  int zero1[3][2];
+  int grav_on, visc_on, driver, epi;
+};
+
+template <typename S>
+void launch_face(const Geom& g, const void* wct, const double* bg, void* D, void* F, unsigned long long* ctot,
+                 double gamma, int do_ctot, cudaStream_t st);
+template <typename S>
+void launch_nu(const Geom& g, const void* wct, const void* D, void* R, const unsigned long long* ctot,
+               cudaStream_t st);
+template <typename S>
+void launch_update(const Stage2Args& a, cudaStream_t st);
+
+extern template void launch_face<double>(const Geom&, const void*, const double*, void*, void*,
+                                         unsigned long long*, double, int, cudaStream_t);
+extern template void launch_face<float>(const Geom&, const void*, const double*, void*, void*,
+                                        unsigned long long*, double, int, cudaStream_t);
+extern template void launch_nu<double>(const Geom&, const void*, const void*, void*, const unsigned long long*,
+                                       cudaStream_t);
+extern template void launch_nu<float>(const Geom&, const void*, const void*, void*, const unsigned long long*,
+                                      cudaStream_t);
+extern template void launch_update<double>(const Stage2Args&, cudaStream_t);
+extern template void launch_update<float>(const Stage2Args&, cudaStream_t);
+
+}  // namespace sacgpu

@@ -1,0 +1,286 @@
+"""Host driver: the main program of the reference, on top of the C-ABI.
+
+Mirrors program vac (src/vac.t:5-158): read the parameters (par/DEFAULT values,
+then vac.par), read the initial snapshot, set up grid and boundaries, then loop
+  save if due -> dt -> stop test -> slowsteps/tmaxexact -> advance -> it, t
+with every compute call going to libsacgpu.so.  Snapshots (.out) and the log
+(.log) are written in the reference's formats (sac_b200.fileio).
+
+    python -m sac_b200.vac vac.par [--user gravvisc|slog|viscosity|strat|tube|none]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import time
+
+import numpy as np
+
+from . import abi, fileio, params
+
+# par/DEFAULT (the reference's default parameter file), the keys this driver uses
+DEFAULT_PAR = """
+ &testlist teststr=' ' /
+ &filelist typefileini='auto' typefileout='auto' typefilelog='default'
+    snapshotini=0 snapshotout=0 fullgridini=F fullgridout=F /
+ &savelist /
+ &stoplist itmax=1000000 tmax=1.D99 tmaxexact=F dtmin=1.D-99 residmin=0.D0 residmax=1.D99 /
+ &methodlist typeadvance='twostep' dimsplit=T typedimsplit='default' sourcesplit=F sourceunsplit=T
+    typesourcesplit='default' divbfix=T smallfix=F /
+ &boundlist extraB=F /
+ &paramlist courantpar=0.8D0 dtcantgrow=F dtdiffpar=0.5D0 dtpar=-1.D0 slowsteps=0 /
+"""
+
+BIG, BIGINT, SMALL = 1e99, 10000000, 1e-99
+USER = {"none": params.USR_NONE, "viscosity": params.USR_VISCOSITY, "slog": params.USR_SLOG,
+        "gravvisc": params.USR_GRAVVISC, "strat": params.USR_STRAT, "tube": params.USR_TUBE}
+
+
+def _list(v, n, fill):
+    if v is None:
+        return [fill] * n
+    v = v if isinstance(v, list) else [v]
+    return (v + [fill] * n)[:n]
+
+
+def eqpar_map(eqpar, names, ndim):
+    """gamma, eta, gravity and nu from eqpar (src/vacpar.t.mhd:26, src/vacusrpar.f:3-6).
+
+    The .ini's variable-name line ends with the eqpar names; when they are present
+    they decide, otherwise the reference's positions grav^D_=neqpar+^D+1, nu_=neqpar+4."""
+    out = {"gamma": float(eqpar[0]), "eta": float(eqpar[1]) if len(eqpar) > 1 else 0.0,
+           "grav": [0.0, 0.0, 0.0], "nu": 0.0}
+    nm = [n.lower() for n in names[-len(eqpar):]] if names else []
+    if len(nm) == len(eqpar) and nm[:1] == ["gamma"]:
+        for v, n in zip(eqpar, nm):
+            if n.startswith("grav") and n[4:].isdigit() and 1 <= int(n[4:]) <= 3:
+                out["grav"][int(n[4:]) - 1] = float(v)
+            elif n == "nu":
+                out["nu"] = float(v)
+        return out
+    for d in range(ndim):
+        if 3 + d < len(eqpar):
+            out["grav"][d] = float(eqpar[3 + d])
+    if len(eqpar) > 5:
+        out["nu"] = float(eqpar[5])
+    return out
+
+
+class Run:
+    def __init__(self, par_text: str, user: str = "gravvisc", default_text: str = DEFAULT_PAR, device=0):
+        pf = params.read_par(default_text, par_text)
+        self.pf = pf
+        g = lambda grp, k, d=None: pf.get(grp, k, d)  # noqa: E731
+        self.filenameini = g("filelist", "filenameini")
+        fn = g("filelist", "filename", ["run.log", "run.out"])
+        self.filename = fn if isinstance(fn, list) else [fn]
+        self.typefileini = g("filelist", "typefileini", "auto")
+        self.typefileout = g("filelist", "typefileout", "auto")
+        self.snapshotini = int(g("filelist", "snapshotini", 0))
+        self.snapshotout = int(g("filelist", "snapshotout", 0))
+        self.fullgridini = bool(g("filelist", "fullgridini", False))
+        self.fullgridout = bool(g("filelist", "fullgridout", False))
+        snap = fileio.read_ini(self.filenameini, self.typefileini, self.snapshotini)
+        if self.typefileout == "auto":
+            self.typefileout = fileio.detect_type(self.filenameini) if self.typefileini == "auto" else self.typefileini
+        self.snap = snap
+        ndim = abs(snap.ndim)
+        nw = snap.nw
+        ndir = (nw - 4) // 3
+        if 3 * ndir + 4 != nw:
+            raise ValueError(f"nw={nw} is not an MHD variable count")
+        self.ndim, self.ndir, self.nw = ndim, ndir, nw
+        nx = tuple(snap.nx)
+        if self.fullgridini:
+            nx = tuple(n - 4 for n in nx)
+        self.nx = nx
+        self.ixGhi = tuple(n + 4 for n in nx)
+        self.ixM = tuple([3] * ndim + [1] * (3 - ndim) + [n + 2 for n in nx] + [1] * (3 - ndim))
+        # full-grid x and w
+        shape = self.ixGhi
+        self.x = np.zeros(shape + (ndim,), order="F")
+        self.w = np.zeros(shape + (nw,), order="F")
+        sl = tuple(slice(None) if self.fullgridini else slice(2, 2 + n) for n in nx)
+        self.x[sl] = snap.x
+        self.w[sl] = snap.w
+        # stop/save lists
+        self.it = int(g("stoplist", "it", snap.it))
+        self.t = float(g("stoplist", "t", snap.t))
+        self.itmax = int(g("stoplist", "itmax", BIGINT))
+        self.tmax = float(g("stoplist", "tmax", BIG))
+        self.tmaxexact = bool(g("stoplist", "tmaxexact", False))
+        self.dtmin = float(g("stoplist", "dtmin", SMALL))
+        self.dtsave = [float(v) for v in _list(g("savelist", "dtsave"), 2, BIG)]
+        self.ditsave = [int(v) for v in _list(g("savelist", "ditsave"), 2, BIGINT)]
+        self.tsave = [[BIG], [BIG]]
+        self.itsave = [[BIGINT], [BIGINT]]
+        for k, v in pf.groups.get("savelist", {}).items():
+            if k.startswith("itsave(") or k.startswith("tsave("):
+                i, f = (int(a) for a in k[k.index("(") + 1:-1].split(","))
+                tgt = self.itsave if k.startswith("itsave") else self.tsave
+                while len(tgt[f - 1]) < i:
+                    tgt[f - 1].append(BIGINT if tgt is self.itsave else BIG)
+                tgt[f - 1][i - 1] = v
+        # methods
+        typefull = _list(g("methodlist", "typefull"), nw, "nul")
+        self.iws = [iw + 1 for iw in range(nw) if typefull[iw] != "nul"]
+        self.method = next((t for t in typefull if t != "nul"), "nul")
+        typeadvance = g("methodlist", "typeadvance", "twostep")
+        typepred = _list(g("methodlist", "typepred"), nw, "default")
+        pred = next((p for p in typepred if p != "nul"), "default")
+        if pred == "default":
+            pred = "nul" if self.method in ("cd4", "cd", "nul") else pred
+        if typeadvance == "twostep" and pred == "nul":
+            typeadvance = "onestep"  # src/vacio.t:502
+        dimsplit = bool(g("methodlist", "dimsplit", True))
+        tds = g("methodlist", "typedimsplit", "default")
+        if tds == "default":
+            tds = "xyyx" if dimsplit else "unsplit"
+        self.typedimsplit = tds
+        self.dimsplit = tds != "unsplit"
+        if bool(g("methodlist", "sourcesplit", False)):
+            raise NotImplementedError("sourcesplit=T is outside the implemented path")
+        ep = eqpar_map(snap.eqpar, snap.varnames.split(), ndim)
+        self.params = params.make_params(
+            gamma=ep["gamma"], eta=ep["eta"], grav=ep["grav"], nu=ep["nu"],
+            courantpar=float(g("paramlist", "courantpar", 0.8)), dtpar=float(g("paramlist", "dtpar", -1.0)),
+            dtdiffpar=float(g("paramlist", "dtdiffpar", 0.5)), dtcantgrow=int(bool(g("paramlist", "dtcantgrow", False))),
+            typeadvance=typeadvance, typepred=pred, sourceunsplit=int(bool(g("methodlist", "sourceunsplit", True))),
+            divbfix=0, user=USER[user], device=device)
+        self.slowsteps = int(g("paramlist", "slowsteps", 0))
+        self.types = params.typeB_from_par(pf, nw, 2 * ndim)
+        self.wnames = g("methodlist", "wnames", snap.varnames)
+        self.fileheadout = snap.header
+        # state of the save logic, src/vac.t:179-184
+        self.tsavelast = [self.t, self.t]
+        self.itsavelast = [self.it, self.it]
+        self.isavet = [0, 0]
+        self.isaveit = [0, 0]
+        self.isaveout = 0
+        self.itmin = self.it
+        self.dt = 0.0
+        self.ctx = abi.Context(self.params)
+        self.ctx.set_grid(ndim, ndir, self.ixGhi, self.ixM, self.x, self.fullgridini)
+        self.ctx.set_boundaries(params.pack_typeB(self.types), 2 * ndim)
+        self.ctx.upload(self.w)
+        self.ctx.getboundary(self.t)
+
+    # -- timetosave, src/vac.t:608-638; savefile, src/vacio.t:901-958 -------------
+    def _tsave(self, ifile, k):
+        lst = self.tsave[ifile]
+        return lst[k] if k < len(lst) else BIG
+
+    def _itsave(self, ifile, k):
+        lst = self.itsave[ifile]
+        return lst[k] if k < len(lst) else BIGINT
+
+    def timetosave(self, ifile):
+        ok = False
+        if self.t >= self._tsave(ifile, self.isavet[ifile]):
+            ok = True
+            self.isavet[ifile] += 1
+        if self.it == self._itsave(ifile, self.isaveit[ifile]):
+            ok = True
+            self.isaveit[ifile] += 1
+        if self.it == self.itsavelast[ifile] + self.ditsave[ifile]:
+            ok = True
+        if self.t >= self.tsavelast[ifile] + self.dtsave[ifile]:
+            ok = True
+        if ok:
+            self.tsavelast[ifile] = self.t
+            self.itsavelast[ifile] = self.it
+        return ok
+
+    def savefile(self, ifile):
+        w = self.ctx.download()
+        if ifile == 1:
+            base = self.filename[1] if len(self.filename) > 1 else "run.out"
+            append = self.out_open
+            if self.snapshotout > 0 and self.isaveout > 0 and self.isaveout % self.snapshotout == 0:
+                self.outname = f"{base}_{self.isaveout + 1}"
+                append = False
+            elif self.outname is None:
+                self.outname = base
+            self.isaveout += 1
+            if self.fullgridout:
+                xs, ws, nx = self.x, w, self.ixGhi
+            else:
+                sl = tuple(slice(2, 2 + n) for n in self.nx)
+                xs, ws, nx = self.x[sl], w[sl], self.nx
+            s = fileio.Snapshot(self.fileheadout, self.it, self.t, self.ndim, len(self.snap.eqpar), self.nw,
+                                tuple(nx), np.asarray(self.snap.eqpar), self.snap.varnames, np.asfortranarray(xs),
+                                np.asfortranarray(ws))
+            if self.typefileout == "ascii":
+                fileio.write_ascii(self.outname, s, append=append)
+            else:
+                fileio.write_binary(self.outname, s, append=append)
+            self.out_open = True
+        else:
+            d = self.ctx.diag()
+            name = self.filename[0]
+            with open(name, "a" if self.log_open else "w") as f:
+                if not self.log_open:
+                    fileio.write_log_header(f, self.fileheadout, self.wnames, False)
+                f.write(fileio.format_log_line(self.it, self.t, self.dt, list(d.wmean)[: self.nw]) + "\n")
+            self.log_open = True
+
+    outname = None
+    out_open = False
+    log_open = False
+
+    # -- the main loop, src/vac.t:55-106 ---------------------------------------------
+    def timetofinish(self):
+        return self.it >= self.itmax or self.t >= self.tmax or self.dt < self.dtmin
+
+    def step(self):
+        for ifile in (0, 1):
+            if self.timetosave(ifile):
+                self.savefile(ifile)
+        dt = self.ctx.getdt(self.it)
+        self.dt = dt
+        if self.timetofinish():
+            return False
+        if self.slowsteps > self.it - self.itmin + 1:
+            dt = dt * (1.0 - (1.0 - (self.it - self.itmin + 1.0) / self.slowsteps) ** 2)
+        if self.tmaxexact:
+            dt = min(dt, self.tmax - self.t + SMALL)
+        self.dt = dt
+        if self.dimsplit and self.ndim > 1:
+            order = range(1, self.ndim + 1)
+            if not ((self.it // 2) * 2 == self.it or self.typedimsplit == "xy"):
+                order = range(self.ndim, 0, -1)
+            for d in order:
+                self.ctx.advect(dt, self.t, self.it, method=self.method, iws=self.iws, idimmin=d, idimmax=d)
+        else:
+            self.ctx.advect(dt, self.t, self.it, method=self.method, iws=self.iws)
+        self.it += 1
+        self.t += dt
+        return True
+
+    def run(self, verbose=True):
+        t0 = time.time()
+        if verbose:
+            print(f"Start Advance {time.time() - t0:10.3f} sec")
+        while self.step():
+            pass
+        for ifile in (0, 1):
+            if self.itsavelast[ifile] < self.it:
+                self.savefile(ifile)
+        if verbose:
+            print(f"Finish Advance {time.time() - t0:10.3f} sec   it={self.it} t={self.t:.6g}")
+        return self
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("par", help="vac.par")
+    ap.add_argument("--user", default="gravvisc", choices=sorted(USER))
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    with open(a.par) as f:
+        Run(f.read(), a.user, device=a.device).run()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

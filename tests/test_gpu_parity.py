@@ -136,3 +136,42 @@ def test_diag_matches_oracle():
     np.testing.assert_allclose(list(dg.wmean)[:P.nw], list(do.wmean)[:P.nw], rtol=1e-12, atol=1e-15)
     np.testing.assert_allclose(dg.divb_l2, do.divb_l2, rtol=1e-10)
     np.testing.assert_allclose(dg.divb_linf, do.divb_linf, rtol=1e-10)
+
+
+# ---------------------------------------------------------------------------
+# FP32-perturbation path: advanced variables stored and updated in FP32,
+# background, pressure/energy recovery and dt in FP64.  Tolerance: 1e-5
+# relative L2 per variable against the FP64 oracle after 100 steps.
+# ---------------------------------------------------------------------------
+FP32_RTOL = 1e-5
+
+
+def _fp32_steps(P, nsteps):
+    o = _util.start(Oracle, P)
+    P.params.precision = params.PREC_FP32
+    g = _util.start(abi.Context, P)
+    P.params.precision = params.PREC_FP64
+    dts = _util.run(o, nsteps)
+    _util.run(g, nsteps, dts=dts)
+    wo = _util.mesh(P, o.download())
+    wg = _util.mesh(P, g.download())
+    err = _util.rel_l2(wg, wo)[: 2 * P.ndir + 2]
+    assert np.isfinite(wg).all()
+    assert err.max() <= FP32_RTOL, f"{P.name}: FP32 rel L2 per variable {err}"
+    return err
+
+
+def test_fp32_stratified_3d():
+    _fp32_steps(problems.stratified(n=(16, 12, 12), amp=0.05), 100)
+
+
+def test_fp32_random_2d():
+    _fp32_steps(problems.random_problem((20, 16), seed=5, types=["cont", "fixed", "periodic", "periodic"]), 100)
+
+
+def test_fp32_zero_perturbation_stays_zero():
+    P = problems.stratified(n=(12, 10, 10), amp=0.0)
+    P.params.precision = params.PREC_FP32
+    g = _util.start(abi.Context, P)
+    _util.run(g, 20)
+    assert np.all(g.download()[..., : 2 * P.ndir + 2] == 0.0)
