@@ -38,7 +38,7 @@ from sac_b200 import abi, problems  # noqa: E402
 
 METRIC = "3D MHD cell-updates/s"
 UNIT = "cell-updates/s"
-BYTES_PER_CELL_UPDATE = {"fp64": 1056}  # 14*n_p*s_p + 4*n_b*s_b, n_p=8, n_b=5
+BYTES_PER_CELL_UPDATE = {"fp64": 1056, "fp32": 608}  # 14*n_p*s_p + 4*n_b*s_b, n_p=8, n_b=5
 STAGES_PER_STEP = 4
 REF_SAMPLE = (128, 128, 32)  # bounded CPU sample: one RK4 step on an x3 slab of the workload
 
@@ -216,6 +216,98 @@ def prof_read(lib, h, kind, reset=True):
     return ms.value, n.value
 
 
+KERNELS = ["update", "face", "bound", "courant", "other", "nu"]  # SAC_K_* order
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Max of a per-rank scalar over all ranks (a no-op for one rank).  The tensor
+    lives on `device` (the rank's GPU under NCCL, the CPU under gloo)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(cells_per_replica: int, steps: int, world: int, seconds: float) -> float:
+    """Whole-job cell-updates/s of `world` replicas that each advanced
+    `cells_per_replica` cells by `steps` steps, timed as the slowest rank."""
+    return world * cells_per_replica * steps / seconds
+
+
+def make_ctx(P, local_rank, precision):
+    from sac_b200 import params as sp
+
+    P.params.device = local_rank
+    P.params.precision = sp.PREC_FP32 if precision == "fp32" else sp.PREC_FP64
+    ctx = abi.Context(P.params)
+    lib = _lib_ext(ctx)
+    ctx.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
+    ctx.set_boundaries(P.typeB_packed, P.nB)
+    ctx.upload(P.w)
+    ctx.getboundary(0.0)
+    return ctx, lib
+
+
+def timed_steps(args, P, ctx, lib, local_rank, world, clocks=True):
+    """W untimed steps, then K steps between a barrier and CUDA events on the
+    library's stream, with per-kernel events and the clock sampler running."""
+    import torch
+    import torch.distributed as dist
+
+    stream = torch.cuda.ExternalStream(lib.sac_get_stream(ctx.h), device=local_rank)
+    t, it = 0.0, 0
+    for _ in range(args.warmup):
+        dt = ctx.getdt(it)
+        ctx.advect(dt, t, it)
+        t += dt
+        it += 1
+    ctx.synchronize()
+    lib.sac_profile(ctx.h, 1)
+    for k in range(len(KERNELS)):
+        prof_read(lib, ctx.h, k, reset=True)
+    launches0 = lib.sac_kernel_launches(ctx.h)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local_rank) if clocks else None
+    if clk:
+        clk.__enter__()
+    e0.record(stream)
+    for _ in range(args.steps):
+        dt = ctx.getdt(it)
+        ctx.advect(dt, t, it)
+        t += dt
+        it += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        dist.barrier()
+    ms = max_over_ranks(ms, world, device=f"cuda:{local_rank}")
+    launches = lib.sac_kernel_launches(ctx.h) - launches0
+    kern = {name: prof_read(lib, ctx.h, k) for k, name in enumerate(KERNELS)}
+    lib.sac_profile(ctx.h, 0)
+    return dict(ms=ms, launches=launches, kern=kern, clocks=clk.summary() if clk else None, t=t, it=it)
+
+
+def roofline(b_cell_update, cells, kern, peak, peak_kind, tr_name, label):
+    upd_ms, upd_n = kern["update"]
+    b_launch = b_cell_update / STAGES_PER_STEP * cells
+    achieved = b_launch / (upd_ms / upd_n / 1e3) / 1e9 if upd_n else None
+    tr = load_traffic(tr_name)
+    traffic = tr["dram_bytes_per_launch"] * cells / tr["cells"] if tr and tr.get("cells") else None
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic, "peak_source": peak_kind,
+            "kernel": label, "bytes_per_launch": b_launch, "avg_launch_ms": upd_ms / upd_n if upd_n else None}
+
+
 def ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -225,53 +317,10 @@ def ours(args, rank, world, local_rank):
     sbuild.build()
     torch.cuda.set_device(local_rank)
     P = workload(args.n)
-    P.params.device = local_rank
-    ctx = abi.Context(P.params)
-    lib = _lib_ext(ctx)
-    ctx.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
-    ctx.set_boundaries(P.typeB_packed, P.nB)
-    ctx.upload(P.w)
-    ctx.getboundary(0.0)
-    stream = torch.cuda.ExternalStream(lib.sac_get_stream(ctx.h), device=local_rank)
-
-    t, it = 0.0, 0
-    for _ in range(args.warmup):
-        dt = ctx.getdt(it)
-        ctx.advect(dt, t, it)
-        t += dt
-        it += 1
-    ctx.synchronize()
-
-    # timed region: K steps, per-kernel events on the library's stream
-    lib.sac_profile(ctx.h, 1)
-    for k in range(5):
-        prof_read(lib, ctx.h, k, reset=True)
-    launches0 = lib.sac_kernel_launches(ctx.h)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            dt = ctx.getdt(it)
-            ctx.advect(dt, t, it)
-            t += dt
-            it += 1
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        dist.barrier()
-    launches = lib.sac_kernel_launches(ctx.h) - launches0
-    kern = {name: prof_read(lib, ctx.h, k) for k, name in enumerate(["stage", "prep", "bound", "courant", "other"])}
-    lib.sac_profile(ctx.h, 0)
-    if world > 1:
-        tt = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
     cells = P.ncells
-    value = world * cells * args.steps / (ms / 1e3)
+    ctx, lib = make_ctx(P, local_rank, "fp64")
+    r64 = timed_steps(args, P, ctx, lib, local_rank, world)
+    value = job_rate(cells, args.steps, world, r64["ms"] / 1e3)
 
     # end to end through the C-ABI with host buffers: per step upload(w),
     # getdt, advect, download(w) from/to pinned host memory
@@ -279,6 +328,7 @@ def ours(args, rank, world, local_rank):
     pin = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
     hw = pin.numpy().reshape(P.ixGhi + (P.nw,), order="F")
     hw[...] = ctx.download()
+    t, it = r64["t"], r64["it"]
     e2e_steps = max(3, min(args.steps, 10))
     if world > 1:
         dist.barrier()
@@ -291,42 +341,40 @@ def ours(args, rank, world, local_rank):
         t += dt
         it += 1
         ctx.download(hw)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([e2e_s], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e = world * cells * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, device=f"cuda:{local_rank}")
+    e2e = job_rate(cells, e2e_steps, world, e2e_s)
+    ctx.close()
+
+    # the FP32-perturbation path on the same workload
+    P32 = workload(args.n)
+    ctx32, lib32 = make_ctx(P32, local_rank, "fp32")
+    r32 = timed_steps(args, P32, ctx32, lib32, local_rank, world, clocks=False)
+    ctx32.close()
+    v32 = job_rate(cells, args.steps, world, r32["ms"] / 1e3)
 
     if rank != 0:
-        ctx.close()
         return 0
-
-    stage_ms, stage_n = kern["stage"]
     peak, peak_kind = load_peaks()
-    b_launch = BYTES_PER_CELL_UPDATE["fp64"] / STAGES_PER_STEP * cells
-    achieved = b_launch / (stage_ms / stage_n / 1e3) / 1e9 if stage_n else None
-    tr = load_traffic("stage_fp64_traffic.json")
-    traffic = None
-    if tr and tr.get("cells"):
-        traffic = tr["dram_bytes_per_launch"] * cells / tr["cells"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": r64["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "stratified atmosphere 128^3, FP64, RK4, hyperdiffusion, gravity, driver",
                    "cells_per_step": cells, "parallelism": f"replicas{world}",
-                   "l2": "no flush: resident state ~0.8 GB per replica, larger than L2",
+                   "l2": "no flush: resident state ~1.6 GB per replica, larger than L2",
                    "step": "getdt + advect (4 RK stages + boundary fills)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "peak_source": peak_kind, "kernel": "k_stage<3,3> FP64",
-                     "bytes_per_launch": b_launch, "avg_launch_ms": stage_ms / stage_n if stage_n else None},
-        "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
+        "roofline": roofline(BYTES_PER_CELL_UPDATE["fp64"], cells, r64["kern"], peak, peak_kind,
+                             "update_fp64_traffic.json", "k_update<3,3,double>"),
+        "kernels_ms_per_step": {k: v[0] / args.steps for k, v in r64["kern"].items()},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                 "path": "sac_upload + sac_getdt + sac_advect + sac_download per step, pinned host w"},
-        "gpu_launches": launches,
-        "clocks": clk.summary(),
+        "gpu_launches": r64["launches"],
+        "clocks": r64["clocks"],
+        "fp32": {"value": v32, "ms_per_step": r32["ms"] / args.steps, "speedup_vs_fp64": v32 / value,
+                 "gpu_launches": r32["launches"],
+                 "kernels_ms_per_step": {k: v[0] / args.steps for k, v in r32["kern"].items()},
+                 "roofline": roofline(BYTES_PER_CELL_UPDATE["fp32"], cells, r32["kern"], peak, peak_kind,
+                                      "update_fp32_traffic.json", "k_update<3,3,float>")},
     }
     if world == 1 and not args.no_cpu:
         v, n, el, cores = cpu_sample()
@@ -334,7 +382,6 @@ def ours(args, rank, world, local_rank):
                                 "sample": f"{n} RK4 steps in {el:.1f} s on a {REF_SAMPLE[0]}x{REF_SAMPLE[1]}x"
                                           f"{REF_SAMPLE[2]} x3-slab of the workload, C++ oracle, OpenMP"}
     print(json.dumps(line), flush=True)
-    ctx.close()
     return 0
 
 

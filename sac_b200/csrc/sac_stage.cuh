@@ -81,30 +81,42 @@ __global__ void __launch_bounds__(256) k_face(Geom g, const S* __restrict__ wp, 
     const double pp = (gamma - 2.0) * (bb + 0.5 * b2);
     const double ptot = (gamma - 1.0) * (e - 0.5 * m2 / rt) - pp;
     D[(NDIR + 2) * N + c] = (S)ptot;
-    double s1 = 0.0, s2 = 0.0;
+    // fluxes in the storage precision's arithmetic (FP64 for the FP64 path; FP32
+    // for the FP32 path, whose pressure/energy recovery above stays FP64)
+    using C_ = S;
+    C_ mC[NDIR], bC[NDIR], bgC[NDIR], vC[NDIR];
 #pragma unroll
-    for (int C = 0; C < NDIR; ++C) s1 = s1 + bg[C] * m[C];
+    for (int C = 0; C < NDIR; ++C) {
+      mC[C] = (C_)m[C];
+      bC[C] = (C_)b[C];
+      bgC[C] = (C_)bg[C];
+      vC[C] = (C_)v[C];
+    }
+    const C_ rtC = (C_)rt, ptC = (C_)ptot, ebC = (C_)eb, eC = (C_)e, rhoC = (C_)rho, rhobC = (C_)rhob;
+    C_ s1 = C_(0), s2 = C_(0);
 #pragma unroll
-    for (int C = 0; C < NDIR; ++C) s2 = s2 + b[C] * m[C];
+    for (int C = 0; C < NDIR; ++C) s1 = s1 + bgC[C] * mC[C];
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) s2 = s2 + bC[C] * mC[C];
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
       S* Fd = F + (long)d * NP * N;
-      const double vd = v[d], bd = b[d], bgd = bg[d], md = m[d];
-      Fd[c] = (S)(rhob * md / rt + vd * rho);
+      const C_ vd = vC[d], bd = bC[d], bgd = bgC[d], md = mC[d];
+      Fd[c] = (S)(rhobC * md / rtC + vd * rhoC);
 #pragma unroll
       for (int C = 0; C < NDIR; ++C) {
-        double f;
+        C_ f;
         if (C == d)
-          f = (ptot + 0.0) - (b[C] * bgd + bd * bg[C]) - b[C] * bd;
+          f = (ptC + C_(0)) - (bC[C] * bgd + bd * bgC[C]) - bC[C] * bd;
         else
-          f = -(b[C] * bgd + bd * bg[C]) - b[C] * bd;
-        Fd[(1 + C) * N + c] = (S)(f + vd * m[C]);
+          f = -(bC[C] * bgd + bd * bgC[C]) - bC[C] * bd;
+        Fd[(1 + C) * N + c] = (S)(f + vd * mC[C]);
       }
-      const double fe = (md * (ptot + 0.0) - bd * s1 - bgd * s2) / rt + eb * md / rt - bd * s2 / rt;
-      Fd[E * N + c] = (S)(fe + vd * e);
+      const C_ fe = (md * (ptC + C_(0)) - bd * s1 - bgd * s2) / rtC + ebC * md / rtC - bd * s2 / rtC;
+      Fd[E * N + c] = (S)(fe + vd * eC);
 #pragma unroll
       for (int C = 0; C < NDIR; ++C)
-        Fd[(E + 1 + C) * N + c] = (C == d) ? (S)0 : (S)(-(v[C] * (bd + bgd)) + vd * bg[C] + vd * b[C]);
+        Fd[(E + 1 + C) * N + c] = (C == d) ? (S)0 : (S)(-(vC[C] * (bd + bgd)) + vd * bgC[C] + vd * bC[C]);
     }
     if (do_ctot) {
       const int p0 = c % g.n[0];
@@ -206,7 +218,7 @@ __global__ void __launch_bounds__(256) k_nu(Geom g, const S* __restrict__ wp, co
 // k_update
 // ---------------------------------------------------------------------------
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
+__global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
   using PR = Pairs<NDIM>;
   using T = S;
   constexpr int NP = 2 * NDIR + 2, E = NDIR + 1, B0 = NDIR + 1;
@@ -222,18 +234,16 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
   if (active) {
     const int st[3] = {1, (int)g.st[1], (int)g.st[2]};
     const int c = pos[0] + st[1] * pos[1] + st[2] * pos[2];
-    const S* wp = (const S*)a.wct;
-    const S* D = (const S*)a.D;
-    const S* F = (const S*)a.F;
-    const S* Q = (const S*)a.R;
+    auto W = [&](int iw) { return (const S*)a.fW[iw]; };
+    auto Df = [&](int i) { return (const S*)a.fD[i]; };
+    auto BG = [&](int i) { return a.fBG[i]; };
     const S* base = (const S*)a.base;
-    const double* bgv = a.bgv;
     T acc[NP];
 #pragma unroll
     for (int iw = 0; iw < NP; ++iw) acc[iw] = base[iw * N + c];
     T dxv[NDIM];
 #pragma unroll
-    for (int d = 0; d < NDIM; ++d) dxv[d] = (T)__ldg(a.dx + d * N + c);
+    for (int d = 0; d < NDIM; ++d) dxv[d] = (T)__ldg(a.fDX[d] + c);
     // gradient4 (src/vacgrid.t:684): -(q(+2) - 8(q(+1)-q(-1)) - q(-2))/dx/12, zero on
     // the first and last two mesh cells along its dimension (:690-709)
     bool z4[NDIM];
@@ -249,29 +259,27 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
     for (int d = 0; d < NDIM; ++d) {
       if (d < a.dmin || d > a.dmax) continue;
       if (!z4[d]) {
-        const S* Fd = F + (long)d * NP * N;
 #pragma unroll
         for (int iw = 0; iw < NP; ++iw) {
           if (iw == B0 + 1 + d) continue;  // no flux of b_d along d
           if (!((a.iwmask >> iw) & 1u)) continue;
-          acc[iw] = acc[iw] - qdt * g4(Fd + iw * N, st[d], dxv[d]);
+          acc[iw] = acc[iw] - qdt * g4((const S*)a.fF[d][iw], st[d], dxv[d]);
         }
       }
       if ((a.iwmask >> E) & 1u) {
-        const S* vd = D + (1 + d) * N;
+        const S* vd = Df(1 + d);
         if (!z4[d]) {
           // getptotal_bg, src/vacphys0.t.mhd:221
           double bgs = 0.0;
 #pragma unroll
-          for (int C = 0; C < NDIR; ++C) bgs = bgs + __ldg(bgv + (2 + C) * N + c) * __ldg(bgv + (2 + C) * N + c);
-          const T fb = (T)((a.gamma - 1.0) * __ldg(bgv + c) - 0.5 * (a.gamma - 2.0) * bgs);
+          for (int C = 0; C < NDIR; ++C) bgs = bgs + __ldg(BG(2 + C) + c) * __ldg(BG(2 + C) + c);
+          const T fb = (T)((a.gamma - 1.0) * __ldg(BG(0) + c) - 0.5 * (a.gamma - 2.0) * bgs);
           acc[E] = acc[E] - qdt * g4(vd, st[d], dxv[d]) * fb;
         }
 #pragma unroll
         for (int di = 0; di < NDIM; ++di) {
           if (di < a.dmin || di > a.dmax || z4[di]) continue;
-          acc[E] = acc[E] + qdt * (T)__ldg(bgv + (2 + di) * N + c) * (T)__ldg(bgv + (2 + d) * N + c) *
-                                g4(vd, st[di], dxv[di]);
+          acc[E] = acc[E] + qdt * (T)__ldg(BG(2 + di) + c) * (T)__ldg(BG(2 + d) + c) * g4(vd, st[di], dxv[di]);
         }
       }
     }
@@ -279,16 +287,16 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
     const T q2 = (T)a.qdt2;
     // --- gravity, src/vacusr.gravity.t:46-78 ---------------------------------------
     if (a.grav_on) {
-      const T rho = ld(wp, c);
+      const T rho = ld(W(0), c);
 #pragma unroll
       for (int d = 0; d < NDIM; ++d)
         if (((a.iwmask >> (1 + d)) & 1u) && fabs(a.grav[d]) > kSmall)
           acc[1 + d] = acc[1 + d] + q2 * (T)a.grav[d] * rho;
       if ((a.iwmask >> E) & 1u) {
-        const T rt = ld(D, c);
+        const T rt = ld(Df(0), c);
 #pragma unroll
         for (int d = 0; d < NDIM; ++d)
-          if (fabs(a.grav[d]) > kSmall) acc[E] = acc[E] + q2 * (T)a.grav[d] * rho * ld(wp + (1 + d) * N, c) / rt;
+          if (fabs(a.grav[d]) > kSmall) acc[E] = acc[E] + q2 * (T)a.grav[d] * rho * ld(W(1 + d), c) / rt;
       }
     }
 
@@ -300,13 +308,14 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
       for (int d = 0; d < NDIM; ++d)
         z1[d] = (a.zero1[d][0] && pos[d] == g.lo[d]) || (a.zero1[d][1] && pos[d] == g.hi[d]);
       auto nus = [&](int ip, int k, int j, T dxk, T& nl, T& nr) {
-        nr = ld(Q + (long)ip * N, j) * dxk;
-        nl = ld(Q + (long)ip * N, j - st[k]) * dxk;
+        const S* Qp = (const S*)a.fQ[ip];
+        nr = ld(Qp, j) * dxk;
+        nl = ld(Qp, j - st[k]) * dxk;
       };
       // density and the "173" energy, :45-64
 #pragma unroll
       for (int pass = 0; pass < 2; ++pass) {
-        const S* q = pass == 0 ? wp : D + (NDIR + 1) * N;
+        const S* q = pass == 0 ? W(0) : Df(NDIR + 1);
         const int tgt = pass == 0 ? 0 : E;
 #pragma unroll
         for (int k = 0; k < NDIM; ++k) {
@@ -321,7 +330,7 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
         }
       }
       // momentum, :69-133
-      const S* rtf = D;
+      const S* rtf = Df(0);
 #pragma unroll
       for (int k = 0; k < NDIM; ++k) {
         const int sk = st[k];
@@ -330,7 +339,7 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
         const T rL = (rC + ld(rtf, c - sk)) / T(2), rR = (ld(rtf, c + sk) + rC) / T(2);
 #pragma unroll
         for (int l = 0; l < NDIM; ++l) {
-          const S* q = D + (1 + l) * N;  // v_l
+          const S* q = Df(1 + l);  // v_l
           T nl, nr;
           nus(PR::v(l, k), k, c, dxk, nl, nr);
           numax = fmaxT(numax, fmaxT(nr, nl));
@@ -338,7 +347,7 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
           const T gL = z1[k] ? T(0) : (qc - ld(q, c - sk)) / dxk;
           const T gR = z1[k] ? T(0) : (ld(q, c + sk) - qc) / dxk;
           const T tL = (nl + T(0)) * gL, tR = (nr + T(0)) * gR;
-          const S* ml = wp + (1 + l) * N;
+          const S* ml = W(1 + l);
           const T mc = ld(ml, c);
           const T VL = (mc + ld(ml, c - sk)) / T(2), VR = (ld(ml, c + sk) + mc) / T(2);
           const T t2m = (rR * tR - rL * tL) / dxk / T(2);
@@ -360,14 +369,14 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
               const int pl = pos[l] + (sg ? 1 : -1);
               T H = T(0);
               if (pl >= g.lo[l] && pl <= g.hi[l]) {  // nu vanishes outside the mesh
-                const T dxkj = (T)__ldg(a.dx + k * N + j);
+                const T dxkj = (T)__ldg(a.fDX[k] + j);
                 T njl, njr;
                 nus(PR::v(l, k), k, j, dxkj, njl, njr);
                 const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
                 H = gC * (njl + njr + T(2) * T(0)) / T(2) / T(2);
               }
               Tm[sg] = ld(rtf, j) * H;
-              Te[sg] = ld(wp + (1 + k) * N, j) * H;
+              Te[sg] = ld(W(1 + k), j) * H;
             }
             const T dxl = dxv[l];
             const T tCm = z1[l] ? T(0) : (Tm[1] - Tm[0]) / dxl / T(2);
@@ -385,7 +394,7 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
           if (k == l) continue;
           const int sk = st[k], sl = st[l];
           const T dxk = dxv[k];
-          const S* q = wp + (B0 + 1 + l) * N;  // b_l
+          const S* q = W(B0 + 1 + l);  // b_l
           T nl, nr;
           nus(PR::b(l, k), k, c, dxk, nl, nr);
           numax = fmaxT(numax, fmaxT(nr, nl));
@@ -398,14 +407,14 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
               const int pl = pos[l] + (sg ? 1 : -1);
               T Kv = T(0);
               if (pl >= g.lo[l] && pl <= g.hi[l]) {
-                const T dxkj = (T)__ldg(a.dx + k * N + j);
+                const T dxkj = (T)__ldg(a.fDX[k] + j);
                 T njl, njr;
                 nus(PR::b(l, k), k, j, dxkj, njl, njr);
                 const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
                 Kv = gC * (njl + njr) / T(2);
               }
               K[sg] = Kv;
-              Ke[sg] = Kv * ld(wp + (B0 + 1 + k) * N, j);
+              Ke[sg] = Kv * ld(W(B0 + 1 + k), j);
             }
             const T dxl = dxv[l];
             const T tC = z1[l] ? T(0) : (K[1] - K[0]) / dxl / T(2);
@@ -428,7 +437,7 @@ __global__ void __launch_bounds__(256) k_update(const Stage2Args a) {
 
     // --- user driver: tdep from the host, spatial profiles precomputed there -----------
     if (a.driver != DRV_NONE) {
-      const T rtn = (T)((double)acc[0] + __ldg(bgv + N + c));
+      const T rtn = (T)((double)acc[0] + __ldg(BG(1) + c));
       if (a.driver == DRV_SLOG) {
         // src/vacusr.f:1355-1375 (x1 vertical; m2, m3 driven)
         const T vvx = (T)(__ldg(a.drv + c) * a.tdep * a.drvA);
@@ -505,7 +514,9 @@ void launch_nu(const Geom& g, const void* wct, const void* D, void* R, const uns
 }
 
 template <typename S>
-void launch_update(const Stage2Args& a, cudaStream_t st) {
+void launch_update(const Stage2Args& a0, cudaStream_t st) {
+  Stage2Args a = a0;
+  fill_field_ptrs(a, sizeof(S));
   const Geom& g = a.g;
   dispatch_nd(g, [&](auto ND, auto NR) {
     constexpr int NDIM = decltype(ND)::value;

@@ -46,7 +46,29 @@ struct Stage2Args {
   unsigned iwmask;
   int zero1[3][2];
   int grav_on, visc_on, driver, epi;
+  // per-field base pointers (filled by fill_field_ptrs), so that a load is one
+  // pointer from parameter space plus the cell offset
+  const void* fF[3][8];   // F[d][iw]
+  const void* fQ[21];     // setnu face quotients per pair
+  const void* fW[8];      // wct per advanced variable
+  const void* fD[6];      // rho+rhob, v.., e173, p'_tot
+  const double* fBG[5];   // eb, rhob, bg..
+  const double* fDX[3];   // dx per dimension
 };
+
+// Fill the per-field pointers of a (np and ndir from g) from the block pointers.
+inline void fill_field_ptrs(Stage2Args& a, size_t es) {
+  const Geom& g = a.g;
+  const long N = g.ncell;
+  auto off = [&](const void* base, long k) { return (const void*)((const char*)base + (size_t)k * N * es); };
+  for (int d = 0; d < 3; ++d)
+    for (int iw = 0; iw < 8; ++iw) a.fF[d][iw] = (d < g.ndim && iw < g.np) ? off(a.F, (long)d * g.np + iw) : nullptr;
+  for (int i = 0; i < 21; ++i) a.fQ[i] = (i < nr_pairs(g.ndim)) ? off(a.R, i) : nullptr;
+  for (int iw = 0; iw < 8; ++iw) a.fW[iw] = (iw < g.np) ? off(a.wct, iw) : nullptr;
+  for (int i = 0; i < 6; ++i) a.fD[i] = (i < g.ndir + 3) ? off(a.D, i) : nullptr;
+  for (int i = 0; i < 5; ++i) a.fBG[i] = (i < g.nw - g.np) ? a.bgv + (size_t)i * N : nullptr;
+  for (int d = 0; d < 3; ++d) a.fDX[d] = (d < g.ndim) ? a.dx + (size_t)d * N : nullptr;
+}
 
 template <typename S>
 void launch_face(const Geom& g, const void* wct, const double* bg, void* D, void* F, unsigned long long* ctot,
