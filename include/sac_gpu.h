@@ -163,6 +163,47 @@ sac_status sac_profile(sac_ctx* c, int enable);
 sac_status sac_profile_read(sac_ctx* c, int kernel, double* total_ms, long* launches, int reset);
 long sac_kernel_launches(const sac_ctx* c);
 
+/* ---- many independent grids (library extension, no Fortran counterpart) ----
+ * A batch advances ninst uneven 1D/2D problems together, each with its own dt,
+ * with typeadvance='fourstep' (the RK4 step of src/vac.t:439-455) and the dt
+ * block of src/vac.t:60-70 per instance.  Every instance is a separate program
+ * vac run: the same parameters (sac_params, shared), its own mesh nx(ndim) with
+ * two ghost layers per side, its own coordinates and state.  Boundary types that
+ * store ghost values (fixed, fixed1, grad1) and the user drivers (slog, strat,
+ * tube) are not available here (SAC_ERR_UNSUPPORTED).
+ *
+ * Host arrays are the instances' Fortran-order blocks one after another:
+ *   x: instance i contributes x(ixG^T,ndim), w: instance i contributes w(ixG^T,nw),
+ *   ixG^T = (nx1+4)[*(nx2+4)].
+ * group_cells bounds the cells of the per-stage intermediates (0: 2^26): the
+ * instances are processed in consecutive groups of at most that many cells.
+ * The step is recorded once as a CUDA graph on the batch's own stream and
+ * replayed by sac_batch_advance; nothing in it synchronises with the host. */
+typedef struct sac_batch sac_batch;
+sac_status sac_batch_create(const sac_params* p, int ndim, int ndir, int ninst, const int* nx, long group_cells,
+                            sac_batch** out);
+sac_status sac_batch_set_grid(sac_batch* b, const double* x);
+/* typeB f10 [nw][2*ndim], the same for every instance */
+sac_status sac_batch_set_boundaries(sac_batch* b, const char* typeB);
+sac_status sac_batch_upload(sac_batch* b, const double* w);
+sac_status sac_batch_download(sac_batch* b, double* w);
+/* the same for instances i0..i0+n-1 only (w holds just their blocks) */
+sac_status sac_batch_upload_range(sac_batch* b, int i0, int n, const double* w);
+sac_status sac_batch_download_range(sac_batch* b, int i0, int n, double* w);
+sac_status sac_batch_getboundary(sac_batch* b);
+/* enqueue nsteps RK4 steps of every instance (asynchronous) */
+sac_status sac_batch_advance(sac_batch* b, int nsteps);
+/* synchronises; per instance t, the last dt and the step count (each may be NULL);
+ * SAC_ERR_NONFINITE when an instance met NaN/Inf in its dt reductions */
+sac_status sac_batch_state(sac_batch* b, double* t, double* dt, int* it);
+sac_status sac_batch_synchronize(sac_batch* b);
+void* sac_batch_get_stream(const sac_batch* b);
+/* time the update pass for each candidate tile shape on this batch and keep the
+ * fastest; tile_xy[2] and ms (per update pass) receive the choice (may be NULL) */
+sac_status sac_batch_tune(sac_batch* b, int* tile_xy, double* ms);
+const char* sac_batch_last_error(const sac_batch* b);
+void sac_batch_destroy(sac_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,7 @@ UNITS = [
     ("sac_gpu.cu", ["--fmad=false"]),
     ("stage_f64.cu", ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("stage_f32.cu", ["--fmad=true", "-prec-div=false", "-ftz=true"]),
+    ("sac_batch.cu", ["--fmad=false"]),
 ]
 
 

@@ -1,0 +1,756 @@
+// sac_batch.cu -- many independent 1D/2D grids advanced together (libsacgpu.so).
+//
+// Thousands of uneven problems share one set of arrays: every instance owns a
+// contiguous full grid (ghosts included) in each field block of the advanced
+// state, the background and the cell widths; the per-stage intermediates (D, F,
+// R) are sized for one group of instances and reused group by group.  Each pass
+// of the stage is one persistent launch whose CTAs walk a tile list built once
+// on the host; per-instance dt, c_tot and max nu live in a device table, so a
+// whole RK4 step (getdt_courant, getdt_visc, four stages with their boundary
+// fills) needs no host round trip and is captured in one CUDA graph.  The tile
+// shape of the update pass is chosen by timing the candidates on the actual batch.
+//
+// Each instance follows exactly the single-grid path (sac_gpu.cu): the same cell
+// bodies, the same ghost resolve, the same dt rules of src/vac.t:61-70.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sac_gpu.h"
+#include "sac_grid.h"
+#include "sac_kernels.cuh"
+#include "sac_stage_api.h"
+
+using namespace sacgpu;
+
+namespace {
+constexpr double kBig = 1.0e99, kSmallD = 1.0e-99;
+
+struct Group {
+  int i0 = 0, i1 = 0;  // instances [i0, i1)
+  long cells = 0;      // cells of the intermediates this group needs
+  InstInfo* d_inst = nullptr;  // instance table with group-local intermediate offsets
+  Tile *d_face = nullptr, *d_nu = nullptr, *d_upd = nullptr;
+  int n_face = 0, n_nu = 0, n_upd = 0;
+  GhostChunk* d_gh = nullptr;
+  int n_gh = 0;
+};
+}  // namespace
+
+struct sac_batch {
+  sac_params par{};
+  std::string err;
+  int dev = 0, prec = SAC_PREC_FP64;
+  size_t es = 8;
+  cudaStream_t stream = nullptr;
+  int ndim = 0, ndir = 0, nw = 0, np = 0, ninst = 0;
+  std::vector<InstInfo> h_inst;  // global offsets, I offsets unused
+  long totP = 0, totX = 0;
+  void* P[4] = {nullptr, nullptr, nullptr, nullptr};
+  double* BG = nullptr;
+  double* dx = nullptr;
+  double* stg = nullptr;
+  InstDyn* d_dyn = nullptr;
+  InstInfo* d_inst = nullptr;  // global table (courant pass, boundaries)
+  Tile* d_cour = nullptr;
+  int n_cour = 0;
+  GhostChunk* d_gh_all = nullptr;
+  int n_gh_all = 0;
+  std::vector<Group> groups;
+  long maxI = 0;
+  void *D = nullptr, *F = nullptr, *R = nullptr;
+  int8_t* d_type = nullptr;
+  int* d_fixed = nullptr;
+  double* d_fixB = nullptr;
+  int pairshift[3][2] = {};
+  int zero1[3][2] = {};
+  dim3 upd_blk = dim3(32, 8, 1);
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool grid_set = false, bc_set = false, state_set = false, bc_init = false;
+  std::vector<double> mindx2, dtgrav;
+};
+
+namespace {
+
+sac_status bfail(sac_batch* b, sac_status st, const std::string& m) {
+  if (b) b->err = m;
+  return st;
+}
+
+#define BK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return bfail(b, SAC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+bool visc_on_b(const sac_batch* b) {
+  if (b->par.user == SAC_USR_SLOG) return true;
+  if (b->par.user == SAC_USR_NONE) return false;
+  return std::fabs(b->par.nu) > kSmallD;
+}
+bool grav_mod(int u) { return u == SAC_USR_SLOG || u == SAC_USR_GRAVVISC || u == SAC_USR_STRAT || u == SAC_USR_TUBE; }
+
+template <typename T>
+sac_status upload_vec(sac_batch* b, T** dptr, const std::vector<T>& v) {
+  if (*dptr) cudaFree(*dptr), *dptr = nullptr;
+  if (v.empty()) return SAC_OK;
+  BK(cudaMalloc(dptr, sizeof(T) * v.size()));
+  BK(cudaMemcpy(*dptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return SAC_OK;
+}
+
+// tiles of shape (tx,ty,tz) covering coordinates lo..hi of every instance in [i0,i1)
+std::vector<Tile> make_tiles(const std::vector<InstInfo>& in, int i0, int i1, int mode, dim3 t) {
+  std::vector<Tile> out;
+  for (int i = i0; i < i1; ++i) {
+    const Geom& g = in[i].g;
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+      if (d >= g.ndim) {
+        lo[d] = hi[d] = 0;
+      } else if (mode == 0) {  // whole grid
+        lo[d] = 0;
+        hi[d] = g.n[d] - 1;
+      } else if (mode == 1) {  // setnu faces
+        lo[d] = g.lo[d] - 1;
+        hi[d] = g.hi[d];
+      } else {  // mesh
+        lo[d] = g.lo[d];
+        hi[d] = g.hi[d];
+      }
+    }
+    for (int z = lo[2]; z <= hi[2]; z += (int)t.z)
+      for (int y = lo[1]; y <= hi[1]; y += (int)t.y)
+        for (int x = lo[0]; x <= hi[0]; x += (int)t.x) out.push_back(Tile{i, {x, y, z}});
+  }
+  return out;
+}
+
+std::vector<GhostChunk> make_ghosts(const std::vector<InstInfo>& in, int i0, int i1) {
+  std::vector<GhostChunk> out;
+  for (int i = i0; i < i1; ++i) {
+    long ns[3];
+    ghost_slabs(in[i].g, ns);
+    const long tot = ns[0] + ns[1] + ns[2];
+    for (long s = 0; s < tot; s += 256) out.push_back(GhostChunk{i, (int)s});
+  }
+  return out;
+}
+
+__global__ void kb_zero(InstDyn* dyn, int n, int what) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (what == 0) {
+    dyn[i].ctot[0] = dyn[i].ctot[1] = dyn[i].ctot[2] = 0ull;
+  } else {
+    dyn[i].courant = 0ull;
+  }
+}
+
+// the dt block of program vac per instance (src/vac.t:61-70): getdt_courant,
+// getdt_visc (src/vacusr.viscosity.t:509-542), getdt_grav (fixed at itmin)
+__global__ void kb_dt(InstDyn* dyn, int n, int ndim, double courantpar, double dtpar, int visc, int grav,
+                      int cantgrow) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  InstDyn& D = dyn[i];
+  double dt;
+  if (dtpar > 0.0) {
+    dt = dtpar;
+  } else {
+    dt = kBig;
+    const double cm = __longlong_as_double((long long)D.courant);
+    if (!(cm == cm) || isinf(cm)) D.bad = 1;
+    if (courantpar > 0.0 && cm > kSmallD) dt = fmin(dt, courantpar / cm);
+    if (grav && visc) {
+      const double mv = __longlong_as_double((long long)D.maxnu);
+      if (!(mv == mv)) D.bad = 1;
+      for (int d = 0; d < ndim; ++d) dt = fmin(dt, 0.25 / ((mv + 0.0) / D.mindx2[d]));
+      D.maxnu = 0ull;
+    }
+    if (grav) dt = fmin(dt, D.dtgrav);
+    if (cantgrow && D.it > 0) dt = fmin(dt, D.dt);  // dtcantgrow, src/vac.t:68
+  }
+  D.dt = dt;
+}
+
+__global__ void kb_time(InstDyn* dyn, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  dyn[i].t += dyn[i].dt;
+  dyn[i].it += 1;
+}
+
+BcArgs bc_proto(sac_batch* b, void* A) {
+  BcArgs a{};
+  a.A = A;
+  a.bgA = b->BG;
+  a.type = b->d_type;
+  a.fixed = b->d_fixed;
+  a.fixB = b->d_fixB;
+  std::memcpy(a.pairshift, b->pairshift, sizeof(a.pairshift));
+  a.sA = b->totP;
+  a.sB = b->totP;
+  return a;
+}
+
+template <typename S>
+void launch_bound_b(sac_batch* b, BcArgs a, int nvar, const GhostChunk* chunks, int n) {
+  if (!n) return;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->dev);
+  const unsigned grid = (unsigned)std::min<long>(n, (long)nsm * 8);
+  kb_bound<S><<<grid, 256, 0, b->stream>>>(a, b->d_inst, chunks, n, nvar);
+}
+
+Stage2Args stage_base(sac_batch* b) {
+  Stage2Args a{};
+  a.g = b->h_inst[0].g;  // ndim, ndir, np, nw (geometry itself comes per instance)
+  a.sP = b->totP;
+  a.sB = b->totP;
+  a.sI = b->maxI;
+  a.sX = b->totX;
+  a.bgv = b->BG;
+  a.D = b->D;
+  a.F = b->F;
+  a.R = b->R;
+  a.dx = b->dx;
+  a.gamma = b->par.gamma;
+  for (int d = 0; d < 3; ++d) a.grav[d] = (d < b->ndim) ? b->par.grav[d] : 0.0;
+  a.dmin = 0;
+  a.dmax = b->ndim - 1;
+  a.iwmask = (1u << b->np) - 1u;
+  for (int d = 0; d < 3; ++d)
+    for (int s = 0; s < 2; ++s) a.zero1[d][s] = b->zero1[d][s];
+  a.grav_on = (b->par.sourceunsplit && grav_mod(b->par.user)) ? 1 : 0;
+  a.visc_on = (b->par.sourceunsplit && visc_on_b(b)) ? 1 : 0;
+  a.driver = DRV_NONE;
+  return a;
+}
+
+// one RK4 step of every instance, src/vac.t:439-455 (enqueued on b->stream)
+template <typename S>
+void enqueue_step(sac_batch* b) {
+  const int nb = (b->ninst + 255) / 256;
+  const int ngrav = grav_mod(b->par.user) ? 1 : 0;
+  kb_zero<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst, 1);
+  BatchStageArgs cb{};
+  cb.a = stage_base(b);
+  cb.a.wct = b->P[0];
+  cb.inst = b->d_inst;
+  cb.dyn = b->d_dyn;
+  cb.tiles = b->d_cour;
+  cb.ntiles = b->n_cour;
+  launch_batch_courant<S>(cb, b->par.gamma, b->stream);
+  kb_dt<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst, b->ndim, b->par.courantpar, b->par.dtpar,
+                                   visc_on_b(b) ? 1 : 0, ngrav, b->par.dtcantgrow ? 1 : 0);
+  void *w = b->P[0], *w1 = b->P[1], *w2 = b->P[2], *w3 = b->P[3];
+  const void* wct[4] = {w, w1, w2, w3};
+  void* out[4] = {w1, w2, w3, w};
+  const int epi[4] = {EPI_PLAIN, EPI_PLAIN, EPI_RK4_S3, EPI_RK4_S4};
+  const bool visc = visc_on_b(b);
+  for (int s = 0; s < 4; ++s) {
+    kb_zero<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst, 0);
+    for (Group& gr : b->groups) {
+      BatchStageArgs sa{};
+      sa.a = stage_base(b);
+      sa.a.wct = wct[s];
+      sa.a.base = w;
+      sa.a.out = out[s];
+      sa.a.aux1 = w1;
+      sa.a.aux2 = w2;
+      sa.a.epi = epi[s];
+      sa.inst = gr.d_inst;
+      sa.dyn = b->d_dyn;
+      sa.stage = s;
+      sa.tiles = gr.d_face;
+      sa.ntiles = gr.n_face;
+      launch_batch_face<S>(sa, b->par.gamma, b->stream);
+      if (visc) {
+        sa.tiles = gr.d_nu;
+        sa.ntiles = gr.n_nu;
+        launch_batch_nu<S>(sa, b->stream);
+      }
+      sa.tiles = gr.d_upd;
+      sa.ntiles = gr.n_upd;
+      launch_batch_update<S>(sa, b->upd_blk, b->stream);
+      BcArgs ba = bc_proto(b, out[s]);
+      if (epi[s] == EPI_RK4_S3) {
+        ba.mode = 1;
+        ba.aux1 = w1;
+        ba.aux2 = w2;
+        ba.basep = w;
+      } else if (epi[s] == EPI_RK4_S4) {
+        ba.mode = 2;
+        ba.aux1 = w1;
+      }
+      launch_bound_b<S>(b, ba, b->np, gr.d_gh, gr.n_gh);
+    }
+  }
+  kb_time<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst);
+}
+
+void drop_graph(sac_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec), b->exec = nullptr;
+  if (b->graph) cudaGraphDestroy(b->graph), b->graph = nullptr;
+}
+
+sac_status build_graph(sac_batch* b) {
+  drop_graph(b);
+  BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  if (b->prec == SAC_PREC_FP32)
+    enqueue_step<float>(b);
+  else
+    enqueue_step<double>(b);
+  BK(cudaStreamEndCapture(b->stream, &b->graph));
+  BK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return SAC_OK;
+}
+
+sac_status build_lists(sac_batch* b) {
+  // a global mesh tile list (courant) and ghost list (boundaries)
+  std::vector<Tile> cour = make_tiles(b->h_inst, 0, b->ninst, 2, dim3(32, 8, 1));
+  std::vector<GhostChunk> gh = make_ghosts(b->h_inst, 0, b->ninst);
+  sac_status st;
+  if ((st = upload_vec(b, &b->d_cour, cour)) != SAC_OK) return st;
+  if ((st = upload_vec(b, &b->d_gh_all, gh)) != SAC_OK) return st;
+  b->n_cour = (int)cour.size();
+  b->n_gh_all = (int)gh.size();
+  for (Group& gr : b->groups) {
+    std::vector<Tile> f = make_tiles(b->h_inst, gr.i0, gr.i1, 0, dim3(32, 8, 1));
+    std::vector<Tile> n = make_tiles(b->h_inst, gr.i0, gr.i1, 1, dim3(32, 8, 1));
+    std::vector<Tile> u = make_tiles(b->h_inst, gr.i0, gr.i1, 2, b->upd_blk);
+    std::vector<GhostChunk> g = make_ghosts(b->h_inst, gr.i0, gr.i1);
+    if ((st = upload_vec(b, &gr.d_face, f)) != SAC_OK) return st;
+    if ((st = upload_vec(b, &gr.d_nu, n)) != SAC_OK) return st;
+    if ((st = upload_vec(b, &gr.d_upd, u)) != SAC_OK) return st;
+    if ((st = upload_vec(b, &gr.d_gh, g)) != SAC_OK) return st;
+    gr.n_face = (int)f.size();
+    gr.n_nu = (int)n.size();
+    gr.n_upd = (int)u.size();
+    gr.n_gh = (int)g.size();
+  }
+  return SAC_OK;
+}
+
+// frees the device arrays; the group ranges stay (they depend on the sizes only)
+void free_all(sac_batch* b) {
+  drop_graph(b);
+  for (auto& p : b->P)
+    if (p) cudaFree(p), p = nullptr;
+  auto fr = [](auto*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+  };
+  fr(b->BG), fr(b->dx), fr(b->stg), fr(b->d_dyn), fr(b->d_inst), fr(b->d_cour), fr(b->d_gh_all);
+  fr(b->D), fr(b->F), fr(b->R), fr(b->d_type), fr(b->d_fixed), fr(b->d_fixB);
+  for (Group& gr : b->groups) fr(gr.d_inst), fr(gr.d_face), fr(gr.d_nu), fr(gr.d_upd), fr(gr.d_gh);
+}
+
+}  // namespace
+
+extern "C" {
+
+sac_status sac_batch_create(const sac_params* p, int ndim, int ndir, int ninst, const int* nx, long group_cells,
+                            sac_batch** out) {
+  if (!p || !nx || !out || ninst < 1) return SAC_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SAC_ERR_NODEVICE;
+  if (ndim < 1 || ndim > 2 || ndir < ndim || ndir > 3) return SAC_ERR_UNSUPPORTED;
+  if (std::string(p->typeadvance) != "fourstep") return SAC_ERR_UNSUPPORTED;
+  if (p->precision != SAC_PREC_FP64 && p->precision != SAC_PREC_FP32) return SAC_ERR_UNSUPPORTED;
+  if (p->user == SAC_USR_SLOG || p->user == SAC_USR_STRAT || p->user == SAC_USR_TUBE) return SAC_ERR_UNSUPPORTED;
+  sac_batch* b = new sac_batch();
+  b->par = *p;
+  b->dev = p->device;
+  b->prec = p->precision;
+  b->es = b->prec == SAC_PREC_FP32 ? 4 : 8;
+  b->ndim = ndim;
+  b->ndir = ndir;
+  b->nw = 3 * ndir + 4;
+  b->np = 2 * ndir + 2;
+  b->ninst = ninst;
+  if (cudaSetDevice(b->dev) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) {
+    delete b;
+    return SAC_ERR_CUDA;
+  }
+  // instance geometry and offsets
+  long off = 0;
+  b->h_inst.resize(ninst);
+  for (int i = 0; i < ninst; ++i) {
+    Geom& g = b->h_inst[i].g;
+    g.ndim = ndim;
+    g.ndir = ndir;
+    g.nw = b->nw;
+    g.np = b->np;
+    for (int d = 0; d < 3; ++d) {
+      g.n[d] = d < ndim ? nx[i * ndim + d] + 4 : 1;
+      g.lo[d] = d < ndim ? 2 : 0;
+      g.hi[d] = d < ndim ? nx[i * ndim + d] + 1 : 0;
+      if (d < ndim && nx[i * ndim + d] < 6) {
+        delete b;
+        return SAC_ERR_ARG;
+      }
+    }
+    g.st[0] = 1;
+    g.st[1] = g.n[0];
+    g.st[2] = (long)g.n[0] * g.n[1];
+    g.ncell = (long)g.n[0] * g.n[1] * g.n[2];
+    b->h_inst[i].o = Offs{off, off, 0, off};
+    off += g.ncell;
+  }
+  b->totP = b->totX = off;
+  if ((long)b->np * off > 2147483647L || (long)(b->nw - b->np) * off > 2147483647L) {
+    // cell offsets inside one block are 32-bit in the stage kernels
+    delete b;
+    return SAC_ERR_UNSUPPORTED;
+  }
+  // groups: consecutive instances with at most group_cells cells of intermediates
+  const long cap = group_cells > 0 ? group_cells : (1L << 26);
+  Group cur;
+  cur.i0 = 0;
+  for (int i = 0; i < ninst; ++i) {
+    const long n = b->h_inst[i].g.ncell;
+    if (cur.cells > 0 && cur.cells + n > cap) {
+      cur.i1 = i;
+      b->groups.push_back(cur);
+      cur = Group();
+      cur.i0 = i;
+    }
+    cur.cells += n;
+  }
+  cur.i1 = ninst;
+  b->groups.push_back(cur);
+  for (const Group& gr : b->groups) b->maxI = std::max(b->maxI, gr.cells);
+  *out = b;
+  return SAC_OK;
+}
+
+void sac_batch_destroy(sac_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->dev);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  free_all(b);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+const char* sac_batch_last_error(const sac_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+// x: the instances' full-grid coordinate blocks x(ixG^T,ndim) one after another
+sac_status sac_batch_set_grid(sac_batch* b, const double* x) {
+  if (!b || !x) return SAC_ERR_ARG;
+  BK(cudaSetDevice(b->dev));
+  const int ndim = b->ndim;
+  std::vector<double> hdx((size_t)ndim * b->totX);
+  b->mindx2.assign((size_t)b->ninst * 3, 0.0);
+  b->dtgrav.assign(b->ninst, kBig);
+  long xoff = 0;
+  for (int i = 0; i < b->ninst; ++i) {
+    const Geom& g = b->h_inst[i].g;
+    std::vector<double> hx1, hdx1;
+    gridsetup1(g.n, g.lo, g.hi, ndim, g.ncell, x + xoff, false, hx1, hdx1);
+    xoff += (long)ndim * g.ncell;
+    double mindx_all = kBig;
+    for (int d = 0; d < ndim; ++d) {
+      double m2 = kBig;
+      for (long c = 0; c < g.ncell; ++c) {
+        hdx[(size_t)d * b->totX + b->h_inst[i].o.X + c] = hdx1[(size_t)d * g.ncell + c];
+        const int p0 = (int)(c % g.n[0]), p1 = (int)((c / g.n[0]) % g.n[1]);
+        if (p0 < g.lo[0] || p0 > g.hi[0] || p1 < g.lo[1] || p1 > g.hi[1]) continue;
+        const double v = hdx1[(size_t)d * g.ncell + c];
+        m2 = std::min(m2, v * v);
+        mindx_all = std::min(mindx_all, v);
+      }
+      b->mindx2[i * 3 + d] = m2;
+    }
+    for (int d = 0; d < ndim; ++d)
+      if (std::fabs(b->par.grav[d]) > 0.0)
+        b->dtgrav[i] = std::min(b->dtgrav[i], 1.0 / std::sqrt(std::fabs(b->par.grav[d]) / mindx_all));
+  }
+  free_all(b);
+  b->grid_set = b->bc_set = b->state_set = b->bc_init = false;
+  const size_t es = b->es;
+  for (auto& p : b->P) BK(cudaMalloc(&p, es * b->np * b->totP));
+  BK(cudaMalloc(&b->BG, sizeof(double) * (b->nw - b->np) * b->totP));
+  BK(cudaMalloc(&b->dx, sizeof(double) * ndim * b->totX));
+  BK(cudaMemcpy(b->dx, hdx.data(), sizeof(double) * hdx.size(), cudaMemcpyHostToDevice));
+  BK(cudaMalloc(&b->D, es * (b->ndir + 3) * b->maxI));
+  BK(cudaMalloc(&b->F, es * (size_t)ndim * b->np * b->maxI));
+  BK(cudaMalloc(&b->R, es * (size_t)nr_pairs(ndim) * b->maxI));
+  BK(cudaMemset(b->R, 0, es * (size_t)nr_pairs(ndim) * b->maxI));
+  if (b->prec == SAC_PREC_FP32) BK(cudaMalloc(&b->stg, sizeof(double) * b->np * b->totP));
+  // instance tables: global and per group (group-local intermediate offsets)
+  sac_status st;
+  if ((st = upload_vec(b, &b->d_inst, b->h_inst)) != SAC_OK) return st;
+  for (Group& gr : b->groups) {
+    std::vector<InstInfo> t = b->h_inst;
+    long ioff = 0;
+    for (int i = gr.i0; i < gr.i1; ++i) {
+      t[i].o.I = ioff;
+      ioff += t[i].g.ncell;
+    }
+    if ((st = upload_vec(b, &gr.d_inst, t)) != SAC_OK) return st;
+  }
+  std::vector<InstDyn> dyn(b->ninst);
+  for (int i = 0; i < b->ninst; ++i) {
+    std::memset(&dyn[i], 0, sizeof(InstDyn));
+    for (int d = 0; d < 3; ++d) dyn[i].mindx2[d] = b->mindx2[i * 3 + d];
+    dyn[i].dtgrav = b->dtgrav[i];
+  }
+  if ((st = upload_vec(b, &b->d_dyn, dyn)) != SAC_OK) return st;
+  if ((st = build_lists(b)) != SAC_OK) return st;
+  b->grid_set = true;
+  return SAC_OK;
+}
+
+// one typeB(nw,2*ndim) shared by every instance; types that store ghost values
+// (fixed, fixed1, grad1) are not available in the batch
+sac_status sac_batch_set_boundaries(sac_batch* b, const char* typeB) {
+  if (!b || !typeB) return SAC_ERR_ARG;
+  if (!b->grid_set) return bfail(b, SAC_ERR_STATE, "sac_batch_set_grid first");
+  BK(cudaSetDevice(b->dev));
+  const int nB = 2 * b->ndim;
+  std::vector<int8_t> ty((size_t)b->nw * nB);
+  std::vector<int> fx((size_t)b->nw * nB, 0);
+  std::vector<std::string> t((size_t)b->nw * nB);
+  for (int iB = 0; iB < nB; ++iB)
+    for (int iw = 0; iw < b->nw; ++iw) {
+      std::string s(typeB + SAC_LENTYPE * ((long)iw + (long)b->nw * iB), SAC_LENTYPE);
+      while (!s.empty() && (s.back() == ' ' || s.back() == '\0')) s.pop_back();
+      int8_t code;
+      if (s == "cont") code = BT_CONT;
+      else if (s == "cont1") code = BT_CONT1;
+      else if (s == "periodic") code = BT_PERIODIC;
+      else if (s == "symm") code = BT_SYMM;
+      else if (s == "symm0") code = BT_SYMM0;
+      else if (s == "asymm") code = BT_ASYMM;
+      else if (s == "contCD4") code = BT_CONTCD4;
+      else return bfail(b, SAC_ERR_UNSUPPORTED, "boundary type '" + s + "' is not available in the batch");
+      ty[iw * nB + iB] = code;
+      t[iw + (long)b->nw * iB] = s;
+    }
+  for (int iB = 0; iB < nB; ++iB)
+    if (t[(long)b->nw * iB] == "periodic" && t[(long)b->nw * (iB ^ 1)] != "periodic")
+      return bfail(b, SAC_ERR_ARG, "Error in BoundSetup: No periodic pair");
+  for (int d = 0; d < b->ndim; ++d)
+    for (int s = 0; s < 2; ++s) {
+      const std::string& t1 = t[(long)b->nw * (2 * d + s)];
+      b->zero1[d][s] = (t1 != "periodic" && t1 != "mpi") ? 1 : 0;
+    }
+  // periodic source offsets are per instance (mesh size): kb_bound reads them
+  // from the geometry, so pairshift here only flags the use
+  sac_status st;
+  if ((st = upload_vec(b, &b->d_type, ty)) != SAC_OK) return st;
+  if ((st = upload_vec(b, &b->d_fixed, fx)) != SAC_OK) return st;
+  if (!b->d_fixB) BK(cudaMalloc(&b->d_fixB, sizeof(double)));
+  b->bc_set = true;
+  return SAC_OK;
+}
+
+// w: the full-grid state blocks w(ixG^T,nw) of instances i0..i0+n-1, one after another
+sac_status sac_batch_upload_range(sac_batch* b, int i0, int n, const double* w) {
+  if (!b || !w || i0 < 0 || n < 0 || i0 + n > (b ? b->ninst : 0)) return SAC_ERR_ARG;
+  if (!b->grid_set) return bfail(b, SAC_ERR_STATE, "sac_batch_set_grid first");
+  if (!n) return SAC_OK;
+  BK(cudaSetDevice(b->dev));
+  const int nb = b->nw - b->np;
+  long woff = 0;
+  double* dst64 = b->prec == SAC_PREC_FP32 ? b->stg : (double*)b->P[0];
+  for (int i = i0; i < i0 + n; ++i) {
+    const long nc = b->h_inst[i].g.ncell, o = b->h_inst[i].o.P;
+    for (int iw = 0; iw < b->np; ++iw)
+      BK(cudaMemcpyAsync(dst64 + (long)iw * b->totP + o, w + woff + (long)iw * nc, sizeof(double) * nc,
+                         cudaMemcpyHostToDevice, b->stream));
+    for (int k = 0; k < nb; ++k)
+      BK(cudaMemcpyAsync(b->BG + (long)k * b->totP + o, w + woff + (long)(b->np + k) * nc, sizeof(double) * nc,
+                         cudaMemcpyHostToDevice, b->stream));
+    woff += (long)b->nw * nc;
+  }
+  if (b->prec == SAC_PREC_FP32) {
+    const long o0 = b->h_inst[i0].o.P, span = woff / b->nw;
+    for (int iw = 0; iw < b->np; ++iw)
+      k_convert<float, double><<<592, 256, 0, b->stream>>>((float*)b->P[0] + (long)iw * b->totP + o0,
+                                                           b->stg + (long)iw * b->totP + o0, span);
+    BK(cudaGetLastError());
+  }
+  BK(cudaStreamSynchronize(b->stream));
+  b->state_set = true;
+  return SAC_OK;
+}
+
+sac_status sac_batch_download_range(sac_batch* b, int i0, int n, double* w) {
+  if (!b || !w || i0 < 0 || n < 0 || i0 + n > (b ? b->ninst : 0)) return SAC_ERR_ARG;
+  if (!b->state_set) return bfail(b, SAC_ERR_STATE, "no state on the device");
+  if (!n) return SAC_OK;
+  BK(cudaSetDevice(b->dev));
+  const int nb = b->nw - b->np;
+  const double* src64 = (const double*)b->P[0];
+  const long o0 = b->h_inst[i0].o.P;
+  const long span = b->h_inst[i0 + n - 1].o.P + b->h_inst[i0 + n - 1].g.ncell - o0;
+  if (b->prec == SAC_PREC_FP32) {
+    for (int iw = 0; iw < b->np; ++iw)
+      k_convert<double, float><<<592, 256, 0, b->stream>>>(b->stg + (long)iw * b->totP + o0,
+                                                           (const float*)b->P[0] + (long)iw * b->totP + o0, span);
+    BK(cudaGetLastError());
+    src64 = b->stg;
+  }
+  long woff = 0;
+  for (int i = i0; i < i0 + n; ++i) {
+    const long nc = b->h_inst[i].g.ncell, o = b->h_inst[i].o.P;
+    for (int iw = 0; iw < b->np; ++iw)
+      BK(cudaMemcpyAsync(w + woff + (long)iw * nc, src64 + (long)iw * b->totP + o, sizeof(double) * nc,
+                         cudaMemcpyDeviceToHost, b->stream));
+    for (int k = 0; k < nb; ++k)
+      BK(cudaMemcpyAsync(w + woff + (long)(b->np + k) * nc, b->BG + (long)k * b->totP + o, sizeof(double) * nc,
+                         cudaMemcpyDeviceToHost, b->stream));
+    woff += (long)b->nw * nc;
+  }
+  BK(cudaStreamSynchronize(b->stream));
+  return SAC_OK;
+}
+
+sac_status sac_batch_upload(sac_batch* b, const double* w) {
+  return b ? sac_batch_upload_range(b, 0, b->ninst, w) : SAC_ERR_ARG;
+}
+
+sac_status sac_batch_download(sac_batch* b, double* w) {
+  return b ? sac_batch_download_range(b, 0, b->ninst, w) : SAC_ERR_ARG;
+}
+
+// getboundary(t,1,nw,1,ndim,w) on every instance
+sac_status sac_batch_getboundary(sac_batch* b) {
+  if (!b) return SAC_ERR_ARG;
+  if (!b->state_set || !b->bc_set) return bfail(b, SAC_ERR_STATE, "state and boundaries must be set");
+  BK(cudaSetDevice(b->dev));
+  BcArgs a = bc_proto(b, b->P[0]);
+  a.init = 1;
+  if (b->prec == SAC_PREC_FP32)
+    launch_bound_b<float>(b, a, b->nw, b->d_gh_all, b->n_gh_all);
+  else
+    launch_bound_b<double>(b, a, b->nw, b->d_gh_all, b->n_gh_all);
+  BK(cudaGetLastError());
+  BK(cudaStreamSynchronize(b->stream));
+  b->bc_init = true;
+  return SAC_OK;
+}
+
+// advance every instance by nsteps RK4 steps with its own dt (graph replays)
+sac_status sac_batch_advance(sac_batch* b, int nsteps) {
+  if (!b || nsteps < 0) return SAC_ERR_ARG;
+  if (!b->bc_init) return bfail(b, SAC_ERR_STATE, "call sac_batch_getboundary first");
+  BK(cudaSetDevice(b->dev));
+  if (!b->exec) {
+    sac_status st = build_graph(b);
+    if (st != SAC_OK) return st;
+  }
+  for (int k = 0; k < nsteps; ++k) BK(cudaGraphLaunch(b->exec, b->stream));
+  BK(cudaGetLastError());
+  return SAC_OK;
+}
+
+// per-instance t, last dt and step count (synchronises); returns
+// SAC_ERR_NONFINITE when any instance met a NaN/Inf in its dt reductions
+sac_status sac_batch_state(sac_batch* b, double* t, double* dt, int* it) {
+  if (!b) return SAC_ERR_ARG;
+  BK(cudaSetDevice(b->dev));
+  std::vector<InstDyn> dyn(b->ninst);
+  BK(cudaMemcpyAsync(dyn.data(), b->d_dyn, sizeof(InstDyn) * b->ninst, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  int bad = 0;
+  for (int i = 0; i < b->ninst; ++i) {
+    if (t) t[i] = dyn[i].t;
+    if (dt) dt[i] = dyn[i].dt;
+    if (it) it[i] = dyn[i].it;
+    bad |= dyn[i].bad;
+  }
+  return bad ? bfail(b, SAC_ERR_NONFINITE, "non-finite wave speed or viscosity in an instance") : SAC_OK;
+}
+
+sac_status sac_batch_synchronize(sac_batch* b) {
+  if (!b) return SAC_ERR_ARG;
+  BK(cudaSetDevice(b->dev));
+  BK(cudaStreamSynchronize(b->stream));
+  return SAC_OK;
+}
+
+void* sac_batch_get_stream(const sac_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+// Autotuner: time the update pass of stage 1 for each candidate tile shape on
+// the actual batch, keep the fastest, rebuild the tile lists and the graph.
+// tile_out[2] receives the chosen shape, ms_out the time per update pass.
+sac_status sac_batch_tune(sac_batch* b, int* tile_out, double* ms_out) {
+  if (!b) return SAC_ERR_ARG;
+  if (!b->bc_init) return bfail(b, SAC_ERR_STATE, "call sac_batch_getboundary first");
+  BK(cudaSetDevice(b->dev));
+  const dim3 cands[] = {dim3(32, 4, 1), dim3(32, 8, 1), dim3(64, 4, 1), dim3(16, 16, 1), dim3(128, 2, 1),
+                        dim3(256, 1, 1)};
+  cudaEvent_t e0, e1;
+  BK(cudaEventCreate(&e0));
+  BK(cudaEventCreate(&e1));
+  double best = 1e300;
+  dim3 bestb = b->upd_blk;
+  for (const dim3& blk : cands) {
+    if (b->ndim == 1 && blk.y != 1) continue;
+    b->upd_blk = blk;
+    sac_status st = build_lists(b);
+    if (st != SAC_OK) return st;
+    auto run = [&]() {
+      for (Group& gr : b->groups) {
+        BatchStageArgs sa{};
+        sa.a = stage_base(b);
+        sa.a.wct = b->P[0];
+        sa.a.base = b->P[0];
+        sa.a.out = b->P[1];
+        sa.a.epi = EPI_PLAIN;
+        sa.inst = gr.d_inst;
+        sa.dyn = b->d_dyn;
+        sa.stage = 0;
+        sa.tiles = gr.d_upd;
+        sa.ntiles = gr.n_upd;
+        if (b->prec == SAC_PREC_FP32)
+          launch_batch_update<float>(sa, blk, b->stream);
+        else
+          launch_batch_update<double>(sa, blk, b->stream);
+      }
+    };
+    run();  // warm-up
+    BK(cudaEventRecord(e0, b->stream));
+    for (int r = 0; r < 3; ++r) run();
+    BK(cudaEventRecord(e1, b->stream));
+    BK(cudaEventSynchronize(e1));
+    float ms = 0;
+    BK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms / 3 < best) {
+      best = ms / 3;
+      bestb = blk;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // the timing runs wrote w1 and max nu; both are rewritten before use, but the
+  // running max nu feeds getdt_visc, so clear it
+  std::vector<InstDyn> dyn(b->ninst);
+  BK(cudaMemcpy(dyn.data(), b->d_dyn, sizeof(InstDyn) * b->ninst, cudaMemcpyDeviceToHost));
+  for (auto& d : dyn) d.maxnu = 0ull;
+  BK(cudaMemcpy(b->d_dyn, dyn.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice));
+  b->upd_blk = bestb;
+  sac_status st = build_lists(b);
+  if (st != SAC_OK) return st;
+  drop_graph(b);
+  if (tile_out) {
+    tile_out[0] = (int)bestb.x;
+    tile_out[1] = (int)bestb.y;
+  }
+  if (ms_out) *ms_out = best;
+  return SAC_OK;
+}
+
+}  // extern "C"

@@ -25,6 +25,7 @@
 #include "sac_gpu.h"
 #include "sac_kernels.cuh"
 #include "sac_stage_api.h"
+#include "sac_grid.h"
 
 using namespace sacgpu;
 
@@ -199,21 +200,16 @@ BcArgs bc_args(sac_ctx* c, void* A) {
   }
   std::memcpy(b.pairshift, c->pairshift, sizeof(b.pairshift));
   b.fullgridini = c->fullgridini;
+  b.sA = b.sB = c->g.ncell;
+  b.oA = b.oB = 0;
   return b;
 }
 
 template <typename S>
 void launch_bound(sac_ctx* c, const BcArgs& b, int nvar) {
   const Geom& g = c->g;
-  long ns[3] = {0, 0, 0};
-  for (int d = 0; d < g.ndim; ++d) {
-    long n = 2L * g.lo[d];
-    for (int e = 0; e < g.ndim; ++e) {
-      if (e < d) n *= g.n[e];
-      if (e > d) n *= (g.hi[e] - g.lo[e] + 1);
-    }
-    ns[d] = n;
-  }
+  long ns[3];
+  ghost_slabs(g, ns);
   const long tot = ns[0] + ns[1] + ns[2];
   if (tot == 0) return;
   const int bs = 256;
@@ -275,11 +271,11 @@ sac_status advect1_t(sac_ctx* c, const std::string& method, double qdt, int dmin
     a.epi = epi;
     {
       Prof pr(c, SAC_K_PREP);
-      launch_face<S>(g, wct, c->BG, c->D, c->F, c->red, c->par.gamma, visc ? 1 : 0, c->stream);
+      launch_face<S>(a, visc ? 1 : 0, c->stream);
     }
     if (visc) {
       Prof pr(c, SAC_K_NU);
-      launch_nu<S>(g, wct, c->D, c->R, c->red, c->stream);
+      launch_nu<S>(a, c->stream);
     }
     {
       Prof pr(c, SAC_K_STAGE);
@@ -410,71 +406,10 @@ sac_status sac_set_grid(sac_ctx* c, int ndim, int ndir, const int ixGhi[3], cons
   g.ncell = (long)g.n[0] * g.n[1] * g.n[2];
   c->fullgridini = fullgridini ? 1 : 0;
   const long N = g.ncell;
-  // gridsetup1 (src/vacgrid.t:585-629): extrapolate x into the ghosts and one layer
-  // beyond, then dx = (x(+1)-x(-1))/2.
-  int qn[3], qo[3];
-  for (int d = 0; d < 3; ++d) {
-    qn[d] = (d < ndim) ? g.n[d] + 2 : 1;
-    qo[d] = (d < ndim) ? 1 : 0;
-  }
-  const long qc = (long)qn[0] * qn[1] * qn[2];
-  std::vector<double> qx((size_t)ndim * qc, 0.0);
-  auto qid = [&](int i, int j, int k) { return (i + qo[0]) + (long)qn[0] * ((j + qo[1]) + (long)qn[1] * (k + qo[2])); };
+  // gridsetup1 (src/vacgrid.t:585-629): extrapolate x into the ghosts, dx = (x(+1)-x(-1))/2
+  std::vector<double> hx, hdx;
+  gridsetup1(g.n, g.lo, g.hi, ndim, N, x, c->fullgridini != 0, hx, hdx);
   auto gid = [&](int i, int j, int k) { return i + g.st[1] * j + g.st[2] * k; };
-  for (int jd = 0; jd < ndim; ++jd)
-    for (int k = 0; k < g.n[2]; ++k)
-      for (int j = 0; j < g.n[1]; ++j)
-        for (int i = 0; i < g.n[0]; ++i) qx[jd * qc + qid(i, j, k)] = x[jd * N + gid(i, j, k)];
-  for (int d = 0; d < ndim; ++d) {
-    int lo3[3], hi3[3];
-    for (int e = 0; e < 3; ++e) {
-      lo3[e] = (e < ndim) ? -1 : 0;
-      hi3[e] = (e < ndim) ? g.n[e] : 0;
-    }
-    for (int side = 0; side < 2; ++side) {
-      int a, b, ixe, ixf;
-      if (side == 0) {
-        b = g.n[d];
-        a = c->fullgridini ? g.n[d] : g.hi[d] + 1;
-        ixe = a - 1;
-        ixf = ixe - 1;
-      } else {
-        a = -1;
-        b = c->fullgridini ? -1 : g.lo[d] - 1;
-        ixe = b + 1;
-        ixf = ixe + 1;
-      }
-      for (int jd = 0; jd < ndim; ++jd)
-        for (int q = a; q <= b; ++q) {
-          int l2[3] = {lo3[0], lo3[1], lo3[2]}, h2[3] = {hi3[0], hi3[1], hi3[2]};
-          l2[d] = h2[d] = q;
-          for (int k = l2[2]; k <= h2[2]; ++k)
-            for (int j = l2[1]; j <= h2[1]; ++j)
-              for (int i = l2[0]; i <= h2[0]; ++i) {
-                int ie[3] = {i, j, k}, iff[3] = {i, j, k};
-                ie[d] = ixe;
-                iff[d] = ixf;
-                const int n = std::abs(ixe - q);
-                qx[jd * qc + qid(i, j, k)] = (double)(1 + n) * qx[jd * qc + qid(ie[0], ie[1], ie[2])] -
-                                             (double)n * qx[jd * qc + qid(iff[0], iff[1], iff[2])];
-              }
-        }
-    }
-  }
-  std::vector<double> hx((size_t)ndim * N), hdx((size_t)ndim * N);
-  for (int jd = 0; jd < ndim; ++jd)
-    for (int k = 0; k < g.n[2]; ++k)
-      for (int j = 0; j < g.n[1]; ++j)
-        for (int i = 0; i < g.n[0]; ++i) hx[jd * N + gid(i, j, k)] = qx[jd * qc + qid(i, j, k)];
-  for (int d = 0; d < ndim; ++d)
-    for (int k = 0; k < g.n[2]; ++k)
-      for (int j = 0; j < g.n[1]; ++j)
-        for (int i = 0; i < g.n[0]; ++i) {
-          int p[3] = {i, j, k}, m[3] = {i, j, k};
-          p[d] += 1;
-          m[d] -= 1;
-          hdx[d * N + gid(i, j, k)] = 0.5 * (qx[d * qc + qid(p[0], p[1], p[2])] - qx[d * qc + qid(m[0], m[1], m[2])]);
-        }
   c->mindx_all = bigdouble;
   for (int d = 0; d < ndim; ++d) {
     double m2 = bigdouble;

@@ -34,6 +34,40 @@ struct Geom {
   long ncell;
 };
 
+// Offsets of one grid's blocks inside the arrays of the four families: advanced
+// state (P: w, w1, w2, w3), background (B), per-stage intermediates (I: D, F, R)
+// and grid (X: dx, driver profiles).  A single grid has all offsets 0.
+struct Offs {
+  long P, B, I, X;
+};
+
+// ---- many independent grids (the batched path) -----------------------------
+struct InstInfo {
+  Geom g;  // the grid of this instance
+  Offs o;  // where its blocks start
+};
+
+// per-instance values the device updates during a step
+struct InstDyn {
+  double dt, t;
+  double mindx2[3];  // min over the mesh of dx^2 per dimension (getdt_visc)
+  double dtgrav;     // getdt_grav, fixed at the first step
+  unsigned long long ctot[3], maxnu, courant;  // bits of non-negative maxima
+  int it, bad;       // step counter; set when a reduction met NaN/Inf
+};
+
+// one unit of work: a tile of blockDim cells starting at p (local coordinates)
+struct Tile {
+  int inst;
+  int p[3];
+};
+
+// 256 consecutive ghost cells of one instance (ghost-slab enumeration of k_bound)
+struct GhostChunk {
+  int inst;
+  int start;
+};
+
 // Explicitly rounded arithmetic (never contracted into an FMA).  Used where the
 // reference's rounding must be reproduced bit for bit: the inputs of setnu's
 // max|d3|/max|d1| ratio, which is ill-conditioned where a field is constant up to
@@ -154,6 +188,8 @@ struct BcArgs {
   const double* __restrict__ fixB;  // compact slabs, region iB at fixoff[iB]
   long fixoff[6];
   long slab[6];                     // cells per variable in region iB
+  long sA, oA;                      // field stride and offset of the advanced blocks (A, aux)
+  long sB, oB;                      // field stride and offset of the background block
   int pairshift[3][2];              // periodic source offset along d for lower/upper ghosts
   int init;                         // first call: fixed acts as cont, or keeps the values read (fullgridini)
   int fullgridini;
@@ -175,7 +211,7 @@ __device__ __forceinline__ long fix_index(const Geom& g, int d, bool up, const i
 template <typename S>
 __device__ __forceinline__ double bc_read(const BcArgs& a, int iw, long c) {
   const int np = a.g.np;
-  return iw < np ? (double)((const S*)a.A)[(long)iw * a.g.ncell + c] : a.bgA[(long)(iw - np) * a.g.ncell + c];
+  return iw < np ? (double)((const S*)a.A)[(long)iw * a.sA + a.oA + c] : a.bgA[(long)(iw - np) * a.sB + a.oB + c];
 }
 
 // Value of variable iw at cell p (mesh or ghost).  fixed_leaf/leaf report a chain
@@ -241,25 +277,36 @@ __device__ double bc_resolve(const BcArgs& a, int iw, const int p[3], bool& fixe
   }
 }
 
+// number of ghost cells in each slab of highest ghost dimension d
+__host__ __device__ inline void ghost_slabs(const Geom& g, long ns[3]) {
+  for (int d = 0; d < 3; ++d) {
+    ns[d] = 0;
+    if (d >= g.ndim) continue;
+    long n = 2L * g.lo[d];
+    for (int e = 0; e < g.ndim; ++e) {
+      if (e < d) n *= g.n[e];
+      if (e > d) n *= (g.hi[e] - g.lo[e] + 1);
+    }
+    ns[d] = n;
+  }
+}
+
 // Ghost cells enumerated slab by slab: slab d holds the cells whose highest ghost
 // dimension is d (all coordinates for dims < d, mesh coordinates for dims > d).
 template <typename S>
-__global__ void k_bound(BcArgs a, long nslab0, long nslab1, long nslab2, int nvar) {
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long tot = nslab0 + nslab1 + nslab2;
-  if (t >= tot) return;
+__device__ void bound_cell(const BcArgs& a, long t, const long ns[3], int nvar) {
   const Geom& g = a.g;
   int d;
   long r;
-  if (t < nslab0) {
+  if (t < ns[0]) {
     d = 0;
     r = t;
-  } else if (t < nslab0 + nslab1) {
+  } else if (t < ns[0] + ns[1]) {
     d = 1;
-    r = t - nslab0;
+    r = t - ns[0];
   } else {
     d = 2;
-    r = t - nslab0 - nslab1;
+    r = t - ns[0] - ns[1];
   }
   int ext[3], off[3];
   for (int e = 0; e < 3; ++e) {
@@ -291,17 +338,47 @@ __global__ void k_bound(BcArgs a, long nslab0, long nslab1, long nslab2, int nva
     const bool pert = iw < g.np;
     S* A = (S*)a.A;
     S* w1 = (S*)a.aux1;
-    if (a.mode == 2 && pert && fl) v = (double)((S)v + w1[(long)iw * g.ncell + leaf]);
+    if (a.mode == 2 && pert && fl) v = (double)((S)v + w1[(long)iw * a.sA + a.oA + leaf]);
     if (pert)
-      A[(long)iw * g.ncell + c] = (S)v;
+      A[(long)iw * a.sA + a.oA + c] = (S)v;
     else
-      a.bgA[(long)(iw - g.np) * g.ncell + c] = v;
+      a.bgA[(long)(iw - g.np) * a.sB + a.oB + c] = v;
     if (a.mode == 1 && pert) {
-      const long o = (long)iw * g.ncell + c;
+      const long o = (long)iw * a.sA + a.oA + c;
       const S* w2 = (const S*)a.aux2;
       const S* w0 = (const S*)a.basep;
       w1[o] = div_rn(sub_rn(add_rn(add_rn(w1[o], S(2) * w2[o]), (S)v), S(4) * w0[o]), S(3));
     }
+  }
+}
+
+template <typename S>
+__global__ void k_bound(BcArgs a, long nslab0, long nslab1, long nslab2, int nvar) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long ns[3] = {nslab0, nslab1, nslab2};
+  if (t >= nslab0 + nslab1 + nslab2) return;
+  bound_cell<S>(a, t, ns, nvar);
+}
+
+// batched: persistent CTAs of 256 threads walk the ghost chunks of all instances
+template <typename S>
+__global__ void __launch_bounds__(256) kb_bound(BcArgs proto, const InstInfo* __restrict__ inst,
+                                                const GhostChunk* __restrict__ chunks, int nchunks, int nvar) {
+  for (int t = blockIdx.x; t < nchunks; t += gridDim.x) {
+    const GhostChunk ch = chunks[t];
+    BcArgs a = proto;
+    a.g = inst[ch.inst].g;
+    a.oA = inst[ch.inst].o.P;
+    a.oB = inst[ch.inst].o.B;
+    for (int d = 0; d < 3; ++d) {  // periodic sources one mesh extent away (src/vacgrid.t:109-120)
+      const int nm = d < a.g.ndim ? a.g.hi[d] - a.g.lo[d] + 1 : 0;
+      a.pairshift[d][0] = nm;
+      a.pairshift[d][1] = -nm;
+    }
+    long ns[3];
+    ghost_slabs(a.g, ns);
+    const long k = (long)ch.start + threadIdx.x;
+    if (k < ns[0] + ns[1] + ns[2]) bound_cell<S>(a, k, ns, nvar);
   }
 }
 

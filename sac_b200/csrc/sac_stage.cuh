@@ -37,32 +37,30 @@ __device__ __forceinline__ double fabsT(double a) { return fabs(a); }
 __device__ __forceinline__ float fabsT(float a) { return fabsf(a); }
 
 // ---------------------------------------------------------------------------
-// k_face (computes in FP64 for both storage types)
+// per-cell bodies (one grid, located by the offsets o)
 // ---------------------------------------------------------------------------
+// k_face body at local cell c; mesh tells whether the getcmax maxima apply there
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256) k_face(Geom g, const S* __restrict__ wp, const double* __restrict__ bgv,
-                                              S* __restrict__ D, S* __restrict__ F, unsigned long long* ctot,
-                                              double gamma, int do_ctot) {
-  __shared__ double sh[32];
-  constexpr int NP = 2 * NDIR + 2, E = NDIR + 1;
-  const int N = (int)g.ncell;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  double cm[NDIM];
-#pragma unroll
-  for (int d = 0; d < NDIM; ++d) cm[d] = 0.0;
-  if (c < N) {
-    const double rho = (double)wp[c];
-    const double eb = bgv[c];
-    const double rhob = bgv[N + c];
+__device__ __forceinline__ void face_cell(const Stage2Args& a, const Offs& o, int c, bool mesh, double gamma,
+                                          double* cm) {
+  constexpr int E = NDIR + 1;
+  auto W = [&](int iw) { return (const S*)a.fW[iw] + o.P; };
+  auto BG = [&](int i) { return a.fBG[i] + o.B; };
+  auto Dw = [&](int i) { return (S*)a.fD[i] + o.I; };
+  auto Fw = [&](int d, int iw) { return (S*)a.fF[d][iw] + o.I; };
+  {
+    const double rho = (double)W(0)[c];
+    const double eb = BG(0)[c];
+    const double rhob = BG(1)[c];
     const double rt = rho + rhob;
     double m[NDIR], b[NDIR], bg[NDIR], v[NDIR];
 #pragma unroll
     for (int C = 0; C < NDIR; ++C) {
-      m[C] = (double)wp[(1 + C) * N + c];
-      b[C] = (double)wp[(E + 1 + C) * N + c];
-      bg[C] = bgv[(2 + C) * N + c];
+      m[C] = (double)W(1 + C)[c];
+      b[C] = (double)W(E + 1 + C)[c];
+      bg[C] = BG(2 + C)[c];
     }
-    const double e = (double)wp[E * N + c];
+    const double e = (double)W(E)[c];
 #pragma unroll
     for (int C = 0; C < NDIR; ++C) v[C] = div_rn(m[C], rt);  // getv / tmp_nu for m
     double b2 = 0.0, m2 = 0.0, bb = 0.0;
@@ -72,15 +70,15 @@ __global__ void __launch_bounds__(256) k_face(Geom g, const S* __restrict__ wp, 
       m2 = add_rn(m2, mul_rn(m[C], m[C]));
       bb = add_rn(bb, mul_rn(b[C], bg[C]));
     }
-    D[c] = (S)rt;
+    Dw(0)[c] = (S)rt;
 #pragma unroll
-    for (int C = 0; C < NDIR; ++C) D[(1 + C) * N + c] = (S)v[C];
+    for (int C = 0; C < NDIR; ++C) Dw(1 + C)[c] = (S)v[C];
     // tmp_nu for iw=173, src/vacusr.viscosity.t:301
-    D[(NDIR + 1) * N + c] = (S)sub_rn(e, mul_rn(0.5, add_rn(b2, div_rn(m2, rt))));
+    Dw(NDIR + 1)[c] = (S)sub_rn(e, mul_rn(0.5, add_rn(b2, div_rn(m2, rt))));
     // getptotal, src/vacphys0.t.mhd:199-201
     const double pp = (gamma - 2.0) * (bb + 0.5 * b2);
     const double ptot = (gamma - 1.0) * (e - 0.5 * m2 / rt) - pp;
-    D[(NDIR + 2) * N + c] = (S)ptot;
+    Dw(NDIR + 2)[c] = (S)ptot;
     // fluxes in the storage precision's arithmetic (FP64 for the FP64 path; FP32
     // for the FP32 path, whose pressure/energy recovery above stays FP64)
     using C_ = S;
@@ -100,9 +98,8 @@ __global__ void __launch_bounds__(256) k_face(Geom g, const S* __restrict__ wp, 
     for (int C = 0; C < NDIR; ++C) s2 = s2 + bC[C] * mC[C];
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
-      S* Fd = F + (long)d * NP * N;
       const C_ vd = vC[d], bd = bC[d], bgd = bgC[d], md = mC[d];
-      Fd[c] = (S)(rhobC * md / rtC + vd * rhoC);
+      Fw(d, 0)[c] = (S)(rhobC * md / rtC + vd * rhoC);
 #pragma unroll
       for (int C = 0; C < NDIR; ++C) {
         C_ f;
@@ -110,21 +107,15 @@ __global__ void __launch_bounds__(256) k_face(Geom g, const S* __restrict__ wp, 
           f = (ptC + C_(0)) - (bC[C] * bgd + bd * bgC[C]) - bC[C] * bd;
         else
           f = -(bC[C] * bgd + bd * bgC[C]) - bC[C] * bd;
-        Fd[(1 + C) * N + c] = (S)(f + vd * mC[C]);
+        Fw(d, 1 + C)[c] = (S)(f + vd * mC[C]);
       }
       const C_ fe = (md * (ptC + C_(0)) - bd * s1 - bgd * s2) / rtC + ebC * md / rtC - bd * s2 / rtC;
-      Fd[E * N + c] = (S)(fe + vd * eC);
+      Fw(d, E)[c] = (S)(fe + vd * eC);
 #pragma unroll
       for (int C = 0; C < NDIR; ++C)
-        Fd[(E + 1 + C) * N + c] = (C == d) ? (S)0 : (S)(-(vC[C] * (bd + bgd)) + vd * bgC[C] + vd * bC[C]);
+        Fw(d, E + 1 + C)[c] = (C == d) ? (S)0 : (S)(-(vC[C] * (bd + bgd)) + vd * bgC[C] + vd * bC[C]);
     }
-    if (do_ctot) {
-      const int p0 = c % g.n[0];
-      const int p1 = (c / g.n[0]) % g.n[1];
-      const int p2 = c / (g.n[0] * g.n[1]);
-      const bool mesh = p0 >= g.lo[0] && p0 <= g.hi[0] && p1 >= g.lo[1] && p1 <= g.hi[1] && p2 >= g.lo[2] &&
-                        p2 <= g.hi[2];
-      if (mesh) {
+    if (mesh) {
         // getpthermal, getcsound2, getcmax: src/vacphys0.t.mhd:95-183
         double q = 0.5 * m2 / rt;
         q = q + 0.5 * b2 + bb;
@@ -144,18 +135,11 @@ __global__ void __launch_bounds__(256) k_face(Geom g, const S* __restrict__ wp, 
           const double Bd = b[d] + bg[d];
           cm[d] = sqrt(0.5 * (cf2 + sqrt(cf2 * cf2 - 4.0 * cs2 * (Bd * Bd) / rt))) + fabs(m[d] / rt);
         }
-      }
     }
-  }
-  if (do_ctot) {
-#pragma unroll
-    for (int d = 0; d < NDIM; ++d) block_max_to(&ctot[d], cm[d], sh);
   }
 }
 
-// ---------------------------------------------------------------------------
-// k_nu: face quotients for every setnu pair on the box [lo-1, hi] of each used dim
-// ---------------------------------------------------------------------------
+// setnu's face quotient from a window of six values of q along one dimension
 template <typename S>
 __device__ __forceinline__ S face_quotient(const S* __restrict__ q, int c, int s, int pos, int lo, int hi, S pre) {
   // q(c-2..c+3) along s; the layer beyond the two ghosts is the mirror image
@@ -180,23 +164,13 @@ __device__ __forceinline__ S face_quotient(const S* __restrict__ q, int c, int s
   return (md1 > S(0)) ? r : S(0);
 }
 
+// k_nu body at local cell c with local coordinates p: every setnu pair's face
+// quotient at c+1/2 along each dimension
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256) k_nu(Geom g, const S* __restrict__ wp, const S* __restrict__ D,
-                                            S* __restrict__ R, const unsigned long long* ctot) {
+__device__ __forceinline__ void nu_cell(const Stage2Args& a, const Geom& g, const Offs& o, int c, const int p[3],
+                                        const unsigned long long* ctot) {
   using PR = Pairs<NDIM>;
   constexpr int E = NDIR + 1;
-  const int N = (int)g.ncell;
-  int ext[3], p[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) ext[d] = (d < NDIM) ? (g.hi[d] - g.lo[d] + 2) : 1;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ext[0] * ext[1] * ext[2]) return;
-  p[0] = t % ext[0];
-  p[1] = (t / ext[0]) % ext[1];
-  p[2] = t / (ext[0] * ext[1]);
-#pragma unroll
-  for (int d = 0; d < 3; ++d) p[d] += (d < NDIM) ? g.lo[d] - 1 : 0;
-  const int c = p[0] + (int)g.st[1] * p[1] + (int)g.st[2] * p[2];
 #pragma unroll
   for (int k = 0; k < NDIM; ++k) {
     const int s = (int)g.st[k];
@@ -204,46 +178,41 @@ __global__ void __launch_bounds__(256) k_nu(Geom g, const S* __restrict__ wp, co
     const double ct = __longlong_as_double((long long)ctot[k]);
     // c_hyp: 0.04 for rho, the "173" energy and b; 0.4 for the momenta (:284-290)
     const S p04 = (S)(ct * 0.04), p4 = (S)(ct * 0.4);
-    R[(long)PR::rho(k) * N + c] = face_quotient(wp, c, s, pos, lo, hi, p04);
-    R[(long)PR::e(k) * N + c] = face_quotient(D + (NDIR + 1) * N, c, s, pos, lo, hi, p04);
+    auto Qw = [&](int ip) { return (S*)a.fQ[ip] + o.I; };
+    auto W = [&](int iw) { return (const S*)a.fW[iw] + o.P; };
+    auto Df = [&](int i) { return (const S*)a.fD[i] + o.I; };
+    Qw(PR::rho(k))[c] = face_quotient(W(0), c, s, pos, lo, hi, p04);
+    Qw(PR::e(k))[c] = face_quotient(Df(NDIR + 1), c, s, pos, lo, hi, p04);
 #pragma unroll
     for (int l = 0; l < NDIM; ++l) {
-      R[(long)PR::v(l, k) * N + c] = face_quotient(D + (1 + l) * N, c, s, pos, lo, hi, p4);
-      if (l != k) R[(long)PR::b(l, k) * N + c] = face_quotient(wp + (E + 1 + l) * N, c, s, pos, lo, hi, p04);
+      Qw(PR::v(l, k))[c] = face_quotient(Df(1 + l), c, s, pos, lo, hi, p4);
+      if (l != k) Qw(PR::b(l, k))[c] = face_quotient(W(E + 1 + l), c, s, pos, lo, hi, p04);
     }
   }
 }
 
-// ---------------------------------------------------------------------------
-// k_update
-// ---------------------------------------------------------------------------
+// k_update body at the mesh cell pos
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
+__device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, const Offs& o, const int pos[3],
+                                            double qdt_d, double qdt2_d, double tdep, double& numax_out) {
   using PR = Pairs<NDIM>;
   using T = S;
   constexpr int NP = 2 * NDIR + 2, E = NDIR + 1, B0 = NDIR + 1;
-  __shared__ double sh[32];
-  const Geom& g = a.g;
-  const int N = (int)g.ncell;
-  int pos[3];
-  pos[0] = g.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  pos[1] = g.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  pos[2] = g.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
-  const bool active = pos[0] <= g.hi[0] && pos[1] <= g.hi[1] && pos[2] <= g.hi[2];
   T numax = T(0);
-  if (active) {
+  {
     const int st[3] = {1, (int)g.st[1], (int)g.st[2]};
     const int c = pos[0] + st[1] * pos[1] + st[2] * pos[2];
-    auto W = [&](int iw) { return (const S*)a.fW[iw]; };
-    auto Df = [&](int i) { return (const S*)a.fD[i]; };
-    auto BG = [&](int i) { return a.fBG[i]; };
-    const S* base = (const S*)a.base;
+    auto W = [&](int iw) { return (const S*)a.fW[iw] + o.P; };
+    auto Df = [&](int i) { return (const S*)a.fD[i] + o.I; };
+    auto BG = [&](int i) { return a.fBG[i] + o.B; };
+    const S* base = (const S*)a.base + o.P;
+    const long sP = a.sP;
     T acc[NP];
 #pragma unroll
-    for (int iw = 0; iw < NP; ++iw) acc[iw] = base[iw * N + c];
+    for (int iw = 0; iw < NP; ++iw) acc[iw] = base[iw * sP + c];
     T dxv[NDIM];
 #pragma unroll
-    for (int d = 0; d < NDIM; ++d) dxv[d] = (T)__ldg(a.fDX[d] + c);
+    for (int d = 0; d < NDIM; ++d) dxv[d] = (T)__ldg(a.fDX[d] + o.X + c);
     // gradient4 (src/vacgrid.t:684): -(q(+2) - 8(q(+1)-q(-1)) - q(-2))/dx/12, zero on
     // the first and last two mesh cells along its dimension (:690-709)
     bool z4[NDIM];
@@ -252,7 +221,7 @@ __global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
     auto g4 = [&](const S* q, int s, T dxd) {
       return -(ld(q, c + 2 * s) - T(8) * (ld(q, c + s) - ld(q, c - s)) - ld(q, c - 2 * s)) / dxd / T(12);
     };
-    const T qdt = (T)a.qdt;
+    const T qdt = (T)qdt_d;
 
     // --- centdiff4 (src/vaccd.t:35-70) -----------------------------------------
 #pragma unroll
@@ -263,7 +232,7 @@ __global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
         for (int iw = 0; iw < NP; ++iw) {
           if (iw == B0 + 1 + d) continue;  // no flux of b_d along d
           if (!((a.iwmask >> iw) & 1u)) continue;
-          acc[iw] = acc[iw] - qdt * g4((const S*)a.fF[d][iw], st[d], dxv[d]);
+          acc[iw] = acc[iw] - qdt * g4((const S*)a.fF[d][iw] + o.I, st[d], dxv[d]);
         }
       }
       if ((a.iwmask >> E) & 1u) {
@@ -284,7 +253,7 @@ __global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
       }
     }
 
-    const T q2 = (T)a.qdt2;
+    const T q2 = (T)qdt2_d;
     // --- gravity, src/vacusr.gravity.t:46-78 ---------------------------------------
     if (a.grav_on) {
       const T rho = ld(W(0), c);
@@ -308,7 +277,7 @@ __global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
       for (int d = 0; d < NDIM; ++d)
         z1[d] = (a.zero1[d][0] && pos[d] == g.lo[d]) || (a.zero1[d][1] && pos[d] == g.hi[d]);
       auto nus = [&](int ip, int k, int j, T dxk, T& nl, T& nr) {
-        const S* Qp = (const S*)a.fQ[ip];
+        const S* Qp = (const S*)a.fQ[ip] + o.I;
         nr = ld(Qp, j) * dxk;
         nl = ld(Qp, j - st[k]) * dxk;
       };
@@ -369,7 +338,7 @@ __global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
               const int pl = pos[l] + (sg ? 1 : -1);
               T H = T(0);
               if (pl >= g.lo[l] && pl <= g.hi[l]) {  // nu vanishes outside the mesh
-                const T dxkj = (T)__ldg(a.fDX[k] + j);
+                const T dxkj = (T)__ldg(a.fDX[k] + o.X + j);
                 T njl, njr;
                 nus(PR::v(l, k), k, j, dxkj, njl, njr);
                 const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
@@ -407,7 +376,7 @@ __global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
               const int pl = pos[l] + (sg ? 1 : -1);
               T Kv = T(0);
               if (pl >= g.lo[l] && pl <= g.hi[l]) {
-                const T dxkj = (T)__ldg(a.fDX[k] + j);
+                const T dxkj = (T)__ldg(a.fDX[k] + o.X + j);
                 T njl, njr;
                 nus(PR::b(l, k), k, j, dxkj, njl, njr);
                 const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
@@ -440,15 +409,15 @@ __global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
       const T rtn = (T)((double)acc[0] + __ldg(BG(1) + c));
       if (a.driver == DRV_SLOG) {
         // src/vacusr.f:1355-1375 (x1 vertical; m2, m3 driven)
-        const T vvx = (T)(__ldg(a.drv + c) * a.tdep * a.drvA);
-        const T vvy = (T)(__ldg(a.drv + N + c) * a.tdep * a.drvA);
+        const T vvx = (T)(__ldg(a.drv + o.X + c) * tdep * a.drvA);
+        const T vvy = (T)(__ldg(a.drv + a.sX + o.X + c) * tdep * a.drvA);
         if (NDIR >= 3) {
           acc[2] = acc[2] + rtn * vvx * q2;
           acc[3 % NP] = acc[3 % NP] + rtn * vvy * q2;
         }
         acc[E] = acc[E] + rtn * (vvx * vvx + vvy * vvy + T(0) * T(0)) * q2 / T(2);
       } else {
-        const T v = (T)(a.drvA * a.tdep * __ldg(a.drv + c) * __ldg(a.drv + N + c));
+        const T v = (T)(a.drvA * tdep * __ldg(a.drv + o.X + c) * __ldg(a.drv + a.sX + o.X + c));
         const int comp = (a.driver == DRV_STRAT) ? 1 : 2;
         acc[comp] = acc[comp] + rtn * v * q2;
         acc[E] = acc[E] + rtn * (v * v) * q2 / T(2);
@@ -456,26 +425,203 @@ __global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
     }
 
     // --- store with the Runge-Kutta epilogue (src/vac.t:450,454) ---------------------
-    S* out = (S*)a.out;
+    S* out = (S*)a.out + o.P;
     if (a.epi == EPI_PLAIN) {
 #pragma unroll
-      for (int iw = 0; iw < NP; ++iw) out[iw * N + c] = acc[iw];
+      for (int iw = 0; iw < NP; ++iw) out[iw * sP + c] = acc[iw];
     } else if (a.epi == EPI_RK4_S3) {
-      S* w1 = (S*)a.aux1;
-      const S* w2 = (const S*)a.aux2;
+      S* w1 = (S*)a.aux1 + o.P;
+      const S* w2 = (const S*)a.aux2 + o.P;
 #pragma unroll
       for (int iw = 0; iw < NP; ++iw) {
         const T w3 = acc[iw];
-        out[iw * N + c] = w3;
-        w1[iw * N + c] = (w1[iw * N + c] + T(2) * w2[iw * N + c] + w3 - T(4) * base[iw * N + c]) / T(3);
+        out[iw * sP + c] = w3;
+        w1[iw * sP + c] = (w1[iw * sP + c] + T(2) * w2[iw * sP + c] + w3 - T(4) * base[iw * sP + c]) / T(3);
       }
     } else {
-      const S* w1 = (const S*)a.aux1;
+      const S* w1 = (const S*)a.aux1 + o.P;
 #pragma unroll
-      for (int iw = 0; iw < NP; ++iw) out[iw * N + c] = acc[iw] + w1[iw * N + c];
+      for (int iw = 0; iw < NP; ++iw) out[iw * sP + c] = acc[iw] + w1[iw * sP + c];
+    }
+    }
+  numax_out = fmax(numax_out, (double)numax);
+}
+
+// ---------------------------------------------------------------------------
+// single-grid kernels
+// ---------------------------------------------------------------------------
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_face(const Stage2Args a, int do_ctot) {
+  __shared__ double sh[32];
+  const Geom& g = a.g;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double cm[NDIM];
+#pragma unroll
+  for (int d = 0; d < NDIM; ++d) cm[d] = 0.0;
+  if (c < (int)g.ncell) {
+    const int p0 = c % g.n[0], p1 = (c / g.n[0]) % g.n[1], p2 = c / (g.n[0] * g.n[1]);
+    const bool mesh = do_ctot && p0 >= g.lo[0] && p0 <= g.hi[0] && p1 >= g.lo[1] && p1 <= g.hi[1] &&
+                      p2 >= g.lo[2] && p2 <= g.hi[2];
+    face_cell<NDIM, NDIR, S>(a, Offs{0, 0, 0, 0}, c, mesh, a.gamma, cm);
+  }
+  if (do_ctot) {
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) block_max_to((unsigned long long*)&a.ctot[d], cm[d], sh);
+  }
+}
+
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_nu(const Stage2Args a) {
+  const Geom& g = a.g;
+  int ext[3], p[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) ext[d] = (d < NDIM) ? (g.hi[d] - g.lo[d] + 2) : 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ext[0] * ext[1] * ext[2]) return;
+  p[0] = t % ext[0];
+  p[1] = (t / ext[0]) % ext[1];
+  p[2] = t / (ext[0] * ext[1]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) p[d] += (d < NDIM) ? g.lo[d] - 1 : 0;
+  const int c = p[0] + (int)g.st[1] * p[1] + (int)g.st[2] * p[2];
+  nu_cell<NDIM, NDIR, S>(a, g, Offs{0, 0, 0, 0}, c, p, a.ctot);
+}
+
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
+  __shared__ double sh[32];
+  const Geom& g = a.g;
+  int pos[3];
+  pos[0] = g.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  pos[1] = g.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  pos[2] = g.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
+  double numax = 0.0;
+  if (pos[0] <= g.hi[0] && pos[1] <= g.hi[1] && pos[2] <= g.hi[2])
+    update_cell<NDIM, NDIR, S>(a, g, Offs{0, 0, 0, 0}, pos, a.qdt, a.qdt2, a.tdep, numax);
+  if (a.visc_on) block_max_to(a.maxnu, numax, sh);
+}
+
+// ---------------------------------------------------------------------------
+// batched kernels: persistent CTAs walk a tile list; each tile belongs to one
+// instance, whose geometry, offsets and dt come from the instance tables
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool tile_cell(const Tile& tl, const Geom& g, const int lo[3], const int hi[3],
+                                          int p[3]) {
+  p[0] = tl.p[0] + threadIdx.x;
+  p[1] = tl.p[1] + threadIdx.y;
+  p[2] = tl.p[2] + threadIdx.z;
+  for (int d = 0; d < 3; ++d)
+    if (p[d] < lo[d] || p[d] > hi[d]) return false;
+  return true;
+}
+
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) kb_face(const BatchStageArgs b, double gamma) {
+  __shared__ double sh[32];
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    const Tile tl = b.tiles[t];
+    const InstInfo& I = b.inst[tl.inst];
+    const Geom& g = I.g;
+    const int lo[3] = {0, 0, 0}, hi[3] = {g.n[0] - 1, g.n[1] - 1, g.n[2] - 1};
+    int p[3];
+    double cm[NDIM];
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) cm[d] = 0.0;
+    if (tile_cell(tl, g, lo, hi, p)) {
+      const int c = p[0] + (int)g.st[1] * p[1] + (int)g.st[2] * p[2];
+      const bool mesh = p[0] >= g.lo[0] && p[0] <= g.hi[0] && p[1] >= g.lo[1] && p[1] <= g.hi[1] &&
+                        p[2] >= g.lo[2] && p[2] <= g.hi[2];
+      face_cell<NDIM, NDIR, S>(b.a, I.o, c, mesh, gamma, cm);
+    }
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) block_max_to(&b.dyn[tl.inst].ctot[d], cm[d], sh);
+  }
+}
+
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) kb_nu(const BatchStageArgs b) {
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    const Tile tl = b.tiles[t];
+    const InstInfo& I = b.inst[tl.inst];
+    const Geom& g = I.g;
+    int lo[3], hi[3], p[3];
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = d < NDIM ? g.lo[d] - 1 : 0;
+      hi[d] = d < NDIM ? g.hi[d] : 0;
+    }
+    if (tile_cell(tl, g, lo, hi, p)) {
+      const int c = p[0] + (int)g.st[1] * p[1] + (int)g.st[2] * p[2];
+      nu_cell<NDIM, NDIR, S>(b.a, g, I.o, c, p, b.dyn[tl.inst].ctot);
     }
   }
-  if (a.visc_on) block_max_to(a.maxnu, (double)numax, sh);
+}
+
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256, 2) kb_update(const BatchStageArgs b) {
+  __shared__ double sh[32];
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    const Tile tl = b.tiles[t];
+    const InstInfo& I = b.inst[tl.inst];
+    const Geom& g = I.g;
+    int p[3];
+    double numax = 0.0;
+    if (tile_cell(tl, g, g.lo, g.hi, p)) {
+      // the RK4 stage steps of advect, src/vac.t:442-452
+      const double dt = b.dyn[tl.inst].dt;
+      const double qdt = b.stage == 0 ? dt / 2 : b.stage == 1 ? dt / 2 : b.stage == 2 ? dt : dt / 6;
+      const double qdt2 = qdt * ((double)(b.a.dmax - b.a.dmin) + 1.0) / (double)g.ndim;
+      update_cell<NDIM, NDIR, S>(b.a, g, I.o, p, qdt, qdt2, 0.0, numax);
+    }
+    if (b.a.visc_on) block_max_to(&b.dyn[tl.inst].maxnu, numax, sh);
+  }
+}
+
+// getdt_courant per instance: max over its mesh of cmax/dx (src/vac.t:667-694)
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) kb_courant(const BatchStageArgs b, double gamma) {
+  __shared__ double sh[32];
+  constexpr int E = NDIR + 1;
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+    const Tile tl = b.tiles[t];
+    const InstInfo& I = b.inst[tl.inst];
+    const Geom& g = I.g;
+    int p[3];
+    double best = 0.0;
+    if (tile_cell(tl, g, g.lo, g.hi, p)) {
+      const int c = p[0] + (int)g.st[1] * p[1] + (int)g.st[2] * p[2];
+      auto W = [&](int iw) { return (double)((const S*)b.a.fW[iw])[I.o.P + c]; };
+      auto BG = [&](int i) { return b.a.fBG[i][I.o.B + c]; };
+      const double rho = W(0), rhob = BG(1), eb = BG(0);
+      const double rt = rho + rhob;
+      double m2 = 0, b2 = 0, bb = 0, bgs = 0, Bt2 = 0;
+#pragma unroll
+      for (int C = 0; C < NDIR; ++C) m2 = m2 + W(1 + C) * W(1 + C);
+#pragma unroll
+      for (int C = 0; C < NDIR; ++C) b2 = b2 + W(E + 1 + C) * W(E + 1 + C);
+#pragma unroll
+      for (int C = 0; C < NDIR; ++C) bb = bb + W(E + 1 + C) * BG(2 + C);
+      double q = 0.5 * m2 / rt;
+      q = q + 0.5 * b2 + bb;
+      const double pr = (gamma - 1.0) * (W(E) - q);
+#pragma unroll
+      for (int C = 0; C < NDIR; ++C) bgs = bgs + BG(2 + C) * BG(2 + C);
+      const double cs2 = gamma * (pr + (gamma - 1.0) * (eb - 0.5 * bgs)) / rt;
+#pragma unroll
+      for (int C = 0; C < NDIR; ++C) {
+        const double B = W(E + 1 + C) + BG(2 + C);
+        Bt2 = Bt2 + B * B;
+      }
+      const double cf2 = Bt2 / rt + cs2;
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) {
+        const double Bd = W(E + 1 + d) + BG(2 + d);
+        const double cmax = sqrt(0.5 * (cf2 + sqrt(cf2 * cf2 - 4.0 * cs2 * (Bd * Bd) / rt))) + fabs(W(1 + d) / rt);
+        const double r = cmax / b.a.fDX[d][I.o.X + c];
+        best = (r != r) ? r : fmax(best, r);
+      }
+    }
+    block_max_to(&b.dyn[tl.inst].courant, best, sh);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -493,23 +639,23 @@ void dispatch_nd(const Geom& g, Fn&& f) {
 }
 
 template <typename S>
-void launch_face(const Geom& g, const void* wct, const double* bg, void* D, void* F, unsigned long long* ctot,
-                 double gamma, int do_ctot, cudaStream_t st) {
-  const int N = (int)g.ncell;
-  dispatch_nd(g, [&](auto ND, auto NR) {
-    k_face<decltype(ND)::value, decltype(NR)::value, S><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
-        g, (const S*)wct, bg, (S*)D, (S*)F, ctot, gamma, do_ctot);
+void launch_face(const Stage2Args& a0, int do_ctot, cudaStream_t st) {
+  Stage2Args a = a0;
+  fill_field_ptrs(a, sizeof(S));
+  const int N = (int)a.g.ncell;
+  dispatch_nd(a.g, [&](auto ND, auto NR) {
+    k_face<decltype(ND)::value, decltype(NR)::value, S><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(a, do_ctot);
   });
 }
 
 template <typename S>
-void launch_nu(const Geom& g, const void* wct, const void* D, void* R, const unsigned long long* ctot,
-               cudaStream_t st) {
+void launch_nu(const Stage2Args& a0, cudaStream_t st) {
+  Stage2Args a = a0;
+  fill_field_ptrs(a, sizeof(S));
   long nb = 1;
-  for (int d = 0; d < g.ndim; ++d) nb *= (g.hi[d] - g.lo[d] + 2);
-  dispatch_nd(g, [&](auto ND, auto NR) {
-    k_nu<decltype(ND)::value, decltype(NR)::value, S><<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(
-        g, (const S*)wct, (const S*)D, (S*)R, ctot);
+  for (int d = 0; d < a.g.ndim; ++d) nb *= (a.g.hi[d] - a.g.lo[d] + 2);
+  dispatch_nd(a.g, [&](auto ND, auto NR) {
+    k_nu<decltype(ND)::value, decltype(NR)::value, S><<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(a);
   });
 }
 
@@ -524,6 +670,57 @@ void launch_update(const Stage2Args& a0, cudaStream_t st) {
     const int n0 = g.hi[0] - g.lo[0] + 1, n1 = g.hi[1] - g.lo[1] + 1, n2 = g.hi[2] - g.lo[2] + 1;
     dim3 grd((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, (n2 + blk.z - 1) / blk.z);
     k_update<NDIM, decltype(NR)::value, S><<<grd, blk, 0, st>>>(a);
+  });
+}
+
+// persistent grid: enough CTAs to fill every SM, each walking the tile list
+inline unsigned persistent_grid(int ntiles, int per_sm) {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long want = (long)nsm * per_sm;
+  return (unsigned)(ntiles < want ? ntiles : want);
+}
+
+template <typename S>
+void launch_batch_face(const BatchStageArgs& b0, double gamma, cudaStream_t st) {
+  BatchStageArgs b = b0;
+  fill_field_ptrs(b.a, sizeof(S));
+  if (!b.ntiles) return;
+  dispatch_nd(b.a.g, [&](auto ND, auto NR) {
+    kb_face<decltype(ND)::value, decltype(NR)::value, S><<<persistent_grid(b.ntiles, 8), dim3(32, 8, 1), 0, st>>>(
+        b, gamma);
+  });
+}
+
+template <typename S>
+void launch_batch_nu(const BatchStageArgs& b0, cudaStream_t st) {
+  BatchStageArgs b = b0;
+  fill_field_ptrs(b.a, sizeof(S));
+  if (!b.ntiles) return;
+  dispatch_nd(b.a.g, [&](auto ND, auto NR) {
+    kb_nu<decltype(ND)::value, decltype(NR)::value, S><<<persistent_grid(b.ntiles, 8), dim3(32, 8, 1), 0, st>>>(b);
+  });
+}
+
+template <typename S>
+void launch_batch_update(const BatchStageArgs& b0, dim3 blk, cudaStream_t st) {
+  BatchStageArgs b = b0;
+  fill_field_ptrs(b.a, sizeof(S));
+  if (!b.ntiles) return;
+  dispatch_nd(b.a.g, [&](auto ND, auto NR) {
+    kb_update<decltype(ND)::value, decltype(NR)::value, S><<<persistent_grid(b.ntiles, 2), blk, 0, st>>>(b);
+  });
+}
+
+template <typename S>
+void launch_batch_courant(const BatchStageArgs& b0, double gamma, cudaStream_t st) {
+  BatchStageArgs b = b0;
+  fill_field_ptrs(b.a, sizeof(S));
+  if (!b.ntiles) return;
+  dispatch_nd(b.a.g, [&](auto ND, auto NR) {
+    kb_courant<decltype(ND)::value, decltype(NR)::value, S>
+        <<<persistent_grid(b.ntiles, 8), dim3(32, 8, 1), 0, st>>>(b, gamma);
   });
 }
 

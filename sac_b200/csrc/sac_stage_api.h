@@ -26,6 +26,7 @@ inline int nr_pairs(int ndim) { return 2 * ndim + ndim * ndim + ndim * (ndim - 1
 
 struct Stage2Args {
   Geom g;
+  long sP, sB, sI, sX;  // field strides of the four families
   const void* wct;   // S[np][N]   stage input, advanced variables
   const double* bgv; // double[nb][N] eb, rhob, bg1..
   const void* base;  // S[np][N]   may alias out
@@ -56,37 +57,64 @@ struct Stage2Args {
   const double* fDX[3];   // dx per dimension
 };
 
-// Fill the per-field pointers of a (np and ndir from g) from the block pointers.
+// Fill the per-field pointers of a from its block pointers and family strides
+// (np, ndir, ndim from a.g; a.sP..a.sX default to g.ncell when zero).
 inline void fill_field_ptrs(Stage2Args& a, size_t es) {
   const Geom& g = a.g;
-  const long N = g.ncell;
-  auto off = [&](const void* base, long k) { return (const void*)((const char*)base + (size_t)k * N * es); };
+  if (!a.sP) a.sP = g.ncell;
+  if (!a.sB) a.sB = g.ncell;
+  if (!a.sI) a.sI = g.ncell;
+  if (!a.sX) a.sX = g.ncell;
+  auto off = [&](const void* base, long k, long s) {
+    return base ? (const void*)((const char*)base + (size_t)k * s * es) : nullptr;
+  };
   for (int d = 0; d < 3; ++d)
-    for (int iw = 0; iw < 8; ++iw) a.fF[d][iw] = (d < g.ndim && iw < g.np) ? off(a.F, (long)d * g.np + iw) : nullptr;
-  for (int i = 0; i < 21; ++i) a.fQ[i] = (i < nr_pairs(g.ndim)) ? off(a.R, i) : nullptr;
-  for (int iw = 0; iw < 8; ++iw) a.fW[iw] = (iw < g.np) ? off(a.wct, iw) : nullptr;
-  for (int i = 0; i < 6; ++i) a.fD[i] = (i < g.ndir + 3) ? off(a.D, i) : nullptr;
-  for (int i = 0; i < 5; ++i) a.fBG[i] = (i < g.nw - g.np) ? a.bgv + (size_t)i * N : nullptr;
-  for (int d = 0; d < 3; ++d) a.fDX[d] = (d < g.ndim) ? a.dx + (size_t)d * N : nullptr;
+    for (int iw = 0; iw < 8; ++iw)
+      a.fF[d][iw] = (d < g.ndim && iw < g.np) ? off(a.F, (long)d * g.np + iw, a.sI) : nullptr;
+  for (int i = 0; i < 21; ++i) a.fQ[i] = (i < nr_pairs(g.ndim)) ? off(a.R, i, a.sI) : nullptr;
+  for (int iw = 0; iw < 8; ++iw) a.fW[iw] = (iw < g.np) ? off(a.wct, iw, a.sP) : nullptr;
+  for (int i = 0; i < 6; ++i) a.fD[i] = (i < g.ndir + 3) ? off(a.D, i, a.sI) : nullptr;
+  for (int i = 0; i < 5; ++i) a.fBG[i] = (i < g.nw - g.np) ? a.bgv + (size_t)i * a.sB : nullptr;
+  for (int d = 0; d < 3; ++d) a.fDX[d] = (d < g.ndim) ? a.dx + (size_t)d * a.sX : nullptr;
 }
 
+struct BatchStageArgs {
+  Stage2Args a;            // pointers/strides of the whole batch (geometry per instance)
+  const InstInfo* inst;
+  InstDyn* dyn;
+  const Tile* tiles;
+  int ntiles;
+  int stage;               // RK4 stage 0..3: qdt = dt/2, dt/2, dt, dt/6
+};
+
 template <typename S>
-void launch_face(const Geom& g, const void* wct, const double* bg, void* D, void* F, unsigned long long* ctot,
-                 double gamma, int do_ctot, cudaStream_t st);
+void launch_face(const Stage2Args& a, int do_ctot, cudaStream_t st);
 template <typename S>
-void launch_nu(const Geom& g, const void* wct, const void* D, void* R, const unsigned long long* ctot,
-               cudaStream_t st);
+void launch_nu(const Stage2Args& a, cudaStream_t st);
 template <typename S>
 void launch_update(const Stage2Args& a, cudaStream_t st);
 
-extern template void launch_face<double>(const Geom&, const void*, const double*, void*, void*,
-                                         unsigned long long*, double, int, cudaStream_t);
-extern template void launch_face<float>(const Geom&, const void*, const double*, void*, void*,
-                                        unsigned long long*, double, int, cudaStream_t);
-extern template void launch_nu<double>(const Geom&, const void*, const void*, void*, const unsigned long long*,
-                                       cudaStream_t);
-extern template void launch_nu<float>(const Geom&, const void*, const void*, void*, const unsigned long long*,
-                                      cudaStream_t);
+template <typename S>
+void launch_batch_face(const BatchStageArgs& b, double gamma, cudaStream_t st);
+template <typename S>
+void launch_batch_nu(const BatchStageArgs& b, cudaStream_t st);
+template <typename S>
+void launch_batch_update(const BatchStageArgs& b, dim3 blk, cudaStream_t st);
+template <typename S>
+void launch_batch_courant(const BatchStageArgs& b, double gamma, cudaStream_t st);
+
+extern template void launch_batch_face<double>(const BatchStageArgs&, double, cudaStream_t);
+extern template void launch_batch_face<float>(const BatchStageArgs&, double, cudaStream_t);
+extern template void launch_batch_nu<double>(const BatchStageArgs&, cudaStream_t);
+extern template void launch_batch_nu<float>(const BatchStageArgs&, cudaStream_t);
+extern template void launch_batch_update<double>(const BatchStageArgs&, dim3, cudaStream_t);
+extern template void launch_batch_update<float>(const BatchStageArgs&, dim3, cudaStream_t);
+extern template void launch_batch_courant<double>(const BatchStageArgs&, double, cudaStream_t);
+extern template void launch_batch_courant<float>(const BatchStageArgs&, double, cudaStream_t);
+extern template void launch_face<double>(const Stage2Args&, int, cudaStream_t);
+extern template void launch_face<float>(const Stage2Args&, int, cudaStream_t);
+extern template void launch_nu<double>(const Stage2Args&, cudaStream_t);
+extern template void launch_nu<float>(const Stage2Args&, cudaStream_t);
 extern template void launch_update<double>(const Stage2Args&, cudaStream_t);
 extern template void launch_update<float>(const Stage2Args&, cudaStream_t);
 

@@ -3,8 +3,11 @@
 #include "sac_stage.cuh"
 
 namespace sacgpu {
-template void launch_face<float>(const Geom&, const void*, const double*, void*, void*, unsigned long long*, double,
-                               int, cudaStream_t);
-template void launch_nu<float>(const Geom&, const void*, const void*, void*, const unsigned long long*, cudaStream_t);
+template void launch_face<float>(const Stage2Args&, int, cudaStream_t);
+template void launch_nu<float>(const Stage2Args&, cudaStream_t);
 template void launch_update<float>(const Stage2Args&, cudaStream_t);
+template void launch_batch_face<float>(const BatchStageArgs&, double, cudaStream_t);
+template void launch_batch_nu<float>(const BatchStageArgs&, cudaStream_t);
+template void launch_batch_update<float>(const BatchStageArgs&, dim3, cudaStream_t);
+template void launch_batch_courant<float>(const BatchStageArgs&, double, cudaStream_t);
 }  // namespace sacgpu

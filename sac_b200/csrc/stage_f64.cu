@@ -3,8 +3,11 @@
 #include "sac_stage.cuh"
 
 namespace sacgpu {
-template void launch_face<double>(const Geom&, const void*, const double*, void*, void*, unsigned long long*, double,
-                               int, cudaStream_t);
-template void launch_nu<double>(const Geom&, const void*, const void*, void*, const unsigned long long*, cudaStream_t);
+template void launch_face<double>(const Stage2Args&, int, cudaStream_t);
+template void launch_nu<double>(const Stage2Args&, cudaStream_t);
 template void launch_update<double>(const Stage2Args&, cudaStream_t);
+template void launch_batch_face<double>(const BatchStageArgs&, double, cudaStream_t);
+template void launch_batch_nu<double>(const BatchStageArgs&, cudaStream_t);
+template void launch_batch_update<double>(const BatchStageArgs&, dim3, cudaStream_t);
+template void launch_batch_courant<double>(const BatchStageArgs&, double, cudaStream_t);
 }  // namespace sacgpu

@@ -249,7 +249,7 @@ def orszag_tang(n=(64, 64), beta=1.0, gamma=5.0 / 3.0, B0=None, nu=1.0, typeadva
     rho = gamma ** 2 * np.ones_like(X)
     vx, vy = -np.sin(2 * math.pi * Y), np.sin(2 * math.pi * X)
     bx, by = B0 * -np.sin(2 * math.pi * Y), B0 * np.sin(4 * math.pi * X)
-    bmean2 = B0 * B0 * 0.5 * 2 / 2 * 2  # <bx^2+by^2> = B0^2 (1/2+1/2)
+    bmean2 = B0 * B0  # <bx^2+by^2> = B0^2 (1/2 + 1/2)
     p = beta * bmean2 / 2.0
     w[..., v["rho"]] = rho
     w[..., v["m0"] + 1] = rho * vx
@@ -257,7 +257,10 @@ def orszag_tang(n=(64, 64), beta=1.0, gamma=5.0 / 3.0, B0=None, nu=1.0, typeadva
     w[..., v["b0"] + 1] = bx
     w[..., v["b0"] + 2] = by
     w[..., v["e"]] = p / (gamma - 1) + 0.5 * rho * (vx ** 2 + vy ** 2) + 0.5 * (bx ** 2 + by ** 2)
-    prm = make_params(gamma=gamma, nu=nu, courantpar=courantpar, typeadvance=typeadvance, user=USR_VISCOSITY)
+    # hyperdiffusion with the viscous dt limit (gravity module, zero gravity)
+    from .params import USR_GRAVVISC
+    prm = make_params(gamma=gamma, nu=nu, courantpar=courantpar, typeadvance=typeadvance, user=USR_GRAVVISC,
+                      grav=(0.0, 0.0, 0.0))
     return Problem(f"ot{n[0]}x{n[1]}", ndim, ndir, tuple(n), prm, x, w,
                    uniform_types(ndim, v["nw"], "periodic"))
 

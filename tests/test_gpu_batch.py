@@ -1,0 +1,150 @@
+"""Parity of the batched path (sac_batch_* of libsacgpu.so) with the CPU oracle.
+
+Every instance of a batch is an independent program-vac run: after n RK4 steps
+with its own dt, each must match the oracle advancing that instance alone
+(FP64: 1e-12 relative L2 per variable and the same time t; FP32: 1e-5)."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from sac_b200 import batch, params, problems
+
+import _util
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+FP32_RTOL = 1e-5
+
+
+def _oracle_run(P, nsteps):
+    o = _util.start(Oracle, P)
+    dts = _util.run(o, nsteps)
+    return o.download(), dts
+
+
+def _batch_of(problems_, prm, group_cells=0):
+    P0 = problems_[0]
+    b = batch.Batch(prm, P0.ndim, P0.ndir, [P.nx for P in problems_], group_cells=group_cells)
+    b.set_grid(np.concatenate([P.x.reshape(-1, order="F") for P in problems_]))
+    b.set_boundaries(P0.typeB)
+    b.upload(np.concatenate([P.w.reshape(-1, order="F") for P in problems_]))
+    b.getboundary()
+    return b
+
+
+def _check(problems_, b, nsteps, rtol):
+    b.advance(nsteps)
+    t, dt, it = b.state()
+    wall = b.download()
+    for i, P in enumerate(problems_):
+        wo, dts = _oracle_run(P, nsteps)
+        wg = b.instance(wall, i)
+        assert it[i] == nsteps
+        err = _util.rel_l2(_util.mesh(P, wg), _util.mesh(P, wo))
+        assert np.isfinite(wg).all()
+        assert err.max() <= rtol, f"instance {i} {P.nx}: rel L2 per variable {err}"
+        # FP32: the viscous dt limit divides by a max of rounding-sensitive
+        # hyperdiffusion coefficients, so dt carries a larger relative error than w
+        dt_tol = RTOL if rtol == RTOL else 1e-4
+        np.testing.assert_allclose(t[i], sum(dts), rtol=dt_tol)
+        np.testing.assert_allclose(dt[i], dts[-1], rtol=dt_tol)
+        # ghost layers too (the boundary fill is part of each stage)
+        np.testing.assert_allclose(wg, wo, rtol=0, atol=max(1e-9, 1e3 * rtol) * np.abs(wo).max())
+
+
+def _ot_problems(sizes, betas, precision=0):
+    out = []
+    for n, beta in zip(sizes, betas):
+        P = problems.orszag_tang(n, beta=beta)
+        P.params = batch.ot_params(precision=precision)
+        out.append(P)
+    return out
+
+
+def test_ot_uneven_fp64():
+    sizes = [(16, 24), (40, 16), (24, 24), (32, 48), (16, 16)]
+    betas = [0.5, 2.0, 10.0, 1.3, 5.0]
+    Ps = _ot_problems(sizes, betas)
+    b = _batch_of(Ps, Ps[0].params)
+    _check(Ps, b, 20, RTOL)
+
+
+def test_ot_generator_matches_problems():
+    gen = batch.OTBatch(4, nx=[(16, 24), (24, 16), (32, 32), (16, 40)], betas=[0.5, 1.0, 4.0, 9.5])
+    Ps = _ot_problems(gen.nx, gen.beta)
+    for i, P in enumerate(Ps):
+        np.testing.assert_array_equal(gen.state(i), P.w)
+        np.testing.assert_array_equal(gen.x(i), P.x)
+    b = gen.make(Ps[0].params)
+    _check(Ps, b, 10, RTOL)
+
+
+def test_groups_split_the_intermediates():
+    sizes = [(16, 24), (40, 16), (24, 24), (32, 48), (16, 16), (20, 28)]
+    Ps = _ot_problems(sizes, [1.0, 2.0, 3.0, 4.0, 5.0, 6.0])
+    b = _batch_of(Ps, Ps[0].params, group_cells=1500)  # several groups
+    _check(Ps, b, 8, RTOL)
+
+
+def test_gravity_viscosity_mixed_bounds_2d():
+    types = ["cont", "cont1", "symm", "asymm"]
+    Ps = [problems.random_problem(n, seed=s, types=types) for n, s in (((14, 12), 1), ((20, 10), 2), ((12, 18), 3))]
+    prm = Ps[0].params
+    for P in Ps:
+        P.params = prm
+    b = _batch_of(Ps, prm)
+    _check(Ps, b, 12, RTOL)
+
+
+def test_1d_instances():
+    Ps = [problems.random_problem((n,), ndir=2, seed=n, types=["cont", "symm"]) for n in (40, 64, 33)]
+    prm = Ps[0].params
+    for P in Ps:
+        P.params = prm
+    b = _batch_of(Ps, prm)
+    _check(Ps, b, 15, RTOL)
+
+
+def test_tuned_tiles_give_the_same_result():
+    sizes = [(48, 40), (64, 24), (24, 56)]
+    Ps = _ot_problems(sizes, [0.7, 3.0, 8.0])
+    b = _batch_of(Ps, Ps[0].params)
+    tile, ms = b.tune()
+    assert tile[0] * tile[1] <= 256 and ms > 0
+    _check(Ps, b, 10, RTOL)
+
+
+def test_advance_in_pieces_equals_one_call():
+    sizes = [(16, 24), (24, 16)]
+    Ps = _ot_problems(sizes, [1.0, 2.0])
+    b1 = _batch_of(Ps, Ps[0].params)
+    b2 = _batch_of(Ps, Ps[0].params)
+    b1.advance(6)
+    for _ in range(3):
+        b2.advance(2)
+    np.testing.assert_array_equal(b1.download(), b2.download())
+    np.testing.assert_array_equal(b1.state()[0], b2.state()[0])
+
+
+def test_ot_uneven_fp32():
+    sizes = [(16, 24), (40, 16), (24, 24)]
+    betas = [0.5, 2.0, 10.0]
+    Ps = _ot_problems(sizes, betas)
+    prm32 = batch.ot_params(precision=params.PREC_FP32)
+    b = _batch_of(Ps, prm32)
+    _check(Ps, b, 10, FP32_RTOL)
+
+
+def test_unsupported_options_are_errors():
+    from sac_b200 import abi
+    prm = batch.ot_params()
+    prm.typeadvance = b"twostep"
+    with pytest.raises(abi.SacError):
+        batch.Batch(prm, 2, 2, [(16, 16)])
+    prm = batch.ot_params()
+    b = batch.Batch(prm, 2, 2, [(16, 16)])
+    P = problems.orszag_tang((16, 16))
+    b.set_grid(P.x.reshape(-1, order="F"))
+    with pytest.raises(abi.SacError):
+        b.set_boundaries([["fixed"] * 10 for _ in range(4)])
