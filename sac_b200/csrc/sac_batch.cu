@@ -395,7 +395,7 @@ sac_status sac_batch_create(const sac_params* p, int ndim, int ndir, int ninst, 
       g.lo[d] = d < ndim ? 2 : 0;
       g.hi[d] = d < ndim ? nx[i * ndim + d] + 1 : 0;
       if (d < ndim && nx[i * ndim + d] < 6) {
-        delete b;
+        sac_batch_destroy(b);
         return SAC_ERR_ARG;
       }
     }
@@ -403,15 +403,14 @@ sac_status sac_batch_create(const sac_params* p, int ndim, int ndir, int ninst, 
     g.st[1] = g.n[0];
     g.st[2] = (long)g.n[0] * g.n[1];
     g.ncell = (long)g.n[0] * g.n[1] * g.n[2];
+    if (g.ncell > 2147483647L) {  // cell indices inside one instance are 32-bit
+      sac_batch_destroy(b);
+      return SAC_ERR_UNSUPPORTED;
+    }
     b->h_inst[i].o = Offs{off, off, 0, off};
     off += g.ncell;
   }
   b->totP = b->totX = off;
-  if ((long)b->np * off > 2147483647L || (long)(b->nw - b->np) * off > 2147483647L) {
-    // cell offsets inside one block are 32-bit in the stage kernels
-    delete b;
-    return SAC_ERR_UNSUPPORTED;
-  }
   // groups: consecutive instances with at most group_cells cells of intermediates
   const long cap = group_cells > 0 ? group_cells : (1L << 26);
   Group cur;
