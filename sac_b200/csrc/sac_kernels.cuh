@@ -115,13 +115,64 @@ __device__ __forceinline__ void block_max_to(unsigned long long* dst, double v, 
 }
 
 // ---------------------------------------------------------------------------
-// k_courant: max over the mesh and dimensions of cmax/dx (getdt_courant), FP64
+// getdt_courant (src/vac.t:641-699), evaluated in FP64
 // ---------------------------------------------------------------------------
+// max over dimensions of cmax/dx at mesh cell (i0,i1,i2); NaN when any is NaN
+template <int NDIR, typename S>
+__device__ __forceinline__ double courant_cell(const Geom& g, const S* __restrict__ wp,
+                                               const double* __restrict__ bgv, const double* __restrict__ dx,
+                                               int i0, int i1, int i2, double gamma) {
+  const long N = g.ncell;
+  const long c = i0 + g.st[1] * i1 + g.st[2] * i2;
+  constexpr int E = NDIR + 1;
+  const double rho = (double)wp[c], rhob = bgv[N + c], eb = bgv[c];
+  const double rt = rho + rhob;
+  double m2 = 0, b2 = 0, bb = 0, bgs = 0, Bt2 = 0;
+  double m[NDIR], b[NDIR];
+#pragma unroll
+  for (int C = 0; C < NDIR; ++C) {
+    m[C] = (double)wp[(1 + C) * N + c];
+    b[C] = (double)wp[(E + 1 + C) * N + c];
+  }
+#pragma unroll
+  for (int C = 0; C < NDIR; ++C) m2 = m2 + m[C] * m[C];
+#pragma unroll
+  for (int C = 0; C < NDIR; ++C) b2 = b2 + b[C] * b[C];
+#pragma unroll
+  for (int C = 0; C < NDIR; ++C) bb = bb + b[C] * bgv[(2 + C) * N + c];
+  double q = 0.5 * m2 / rt;
+  q = q + 0.5 * b2 + bb;
+  const double p = (gamma - 1.0) * ((double)wp[E * N + c] - q);
+#pragma unroll
+  for (int C = 0; C < NDIR; ++C) bgs = bgs + bgv[(2 + C) * N + c] * bgv[(2 + C) * N + c];
+  const double cs2 = gamma * (p + (gamma - 1.0) * (eb - 0.5 * bgs)) / rt;
+#pragma unroll
+  for (int C = 0; C < NDIR; ++C) {
+    double B = b[C] + bgv[(2 + C) * N + c];
+    Bt2 = Bt2 + B * B;
+  }
+  const double cf2 = Bt2 / rt + cs2;
+  double best = 0.0;
+  for (int d = 0; d < g.ndim; ++d) {
+    const double Bd = b[d] + bgv[(2 + d) * N + c];
+    double cmax = sqrt(0.5 * (cf2 + sqrt(cf2 * cf2 - 4.0 * cs2 * (Bd * Bd) / rt))) + fabs(m[d] / rt);
+    double r = cmax / dx[d * N + c];
+    if (r != r) return r;
+    best = fmax(best, r);
+  }
+  return best;
+}
+
+// NaN-sticky running max of non-negative values
+__device__ __forceinline__ double max_sticky(double best, double r) {
+  return (r != r || best != best) ? __longlong_as_double(0x7ff8000000000000ll) : fmax(best, r);
+}
+
+// k_courant: max over the mesh of courant_cell, one atomic per block
 template <int NDIR, typename S>
 __global__ void k_courant(Geom g, const S* __restrict__ wp, const double* __restrict__ bgv,
                           const double* __restrict__ dx, unsigned long long* out, double gamma) {
   __shared__ double sh[32];
-  const long N = g.ncell;
   double best = 0.0;
   const long nm0 = g.hi[0] - g.lo[0] + 1, nm1 = g.hi[1] - g.lo[1] + 1, nm2 = g.hi[2] - g.lo[2] + 1;
   const long tot = nm0 * nm1 * nm2;
@@ -129,42 +180,7 @@ __global__ void k_courant(Geom g, const S* __restrict__ wp, const double* __rest
     const int i0 = g.lo[0] + (int)(t % nm0);
     const int i1 = g.lo[1] + (int)((t / nm0) % nm1);
     const int i2 = g.lo[2] + (int)(t / (nm0 * nm1));
-    const long c = i0 + g.st[1] * i1 + g.st[2] * i2;
-    constexpr int E = NDIR + 1;
-    const double rho = (double)wp[c], rhob = bgv[N + c], eb = bgv[c];
-    const double rt = rho + rhob;
-    double m2 = 0, b2 = 0, bb = 0, bgs = 0, Bt2 = 0;
-    double m[NDIR], b[NDIR];
-#pragma unroll
-    for (int C = 0; C < NDIR; ++C) {
-      m[C] = (double)wp[(1 + C) * N + c];
-      b[C] = (double)wp[(E + 1 + C) * N + c];
-    }
-#pragma unroll
-    for (int C = 0; C < NDIR; ++C) m2 = m2 + m[C] * m[C];
-#pragma unroll
-    for (int C = 0; C < NDIR; ++C) b2 = b2 + b[C] * b[C];
-#pragma unroll
-    for (int C = 0; C < NDIR; ++C) bb = bb + b[C] * bgv[(2 + C) * N + c];
-    double q = 0.5 * m2 / rt;
-    q = q + 0.5 * b2 + bb;
-    const double p = (gamma - 1.0) * ((double)wp[E * N + c] - q);
-#pragma unroll
-    for (int C = 0; C < NDIR; ++C) bgs = bgs + bgv[(2 + C) * N + c] * bgv[(2 + C) * N + c];
-    const double cs2 = gamma * (p + (gamma - 1.0) * (eb - 0.5 * bgs)) / rt;
-#pragma unroll
-    for (int C = 0; C < NDIR; ++C) {
-      double B = b[C] + bgv[(2 + C) * N + c];
-      Bt2 = Bt2 + B * B;
-    }
-    const double cf2 = Bt2 / rt + cs2;
-    for (int d = 0; d < g.ndim; ++d) {
-      const double Bd = b[d] + bgv[(2 + d) * N + c];
-      double cmax = sqrt(0.5 * (cf2 + sqrt(cf2 * cf2 - 4.0 * cs2 * (Bd * Bd) / rt))) + fabs(m[d] / rt);
-      double r = cmax / dx[d * N + c];
-      best = (r != r) ? r : fmax(best, r);
-      if (r != r) break;
-    }
+    best = max_sticky(best, courant_cell<NDIR, S>(g, wp, bgv, dx, i0, i1, i2, gamma));
   }
   block_max_to(out, best, sh);
 }
