@@ -163,6 +163,22 @@ sac_status sac_profile(sac_ctx* c, int enable);
 sac_status sac_profile_read(sac_ctx* c, int kernel, double* total_ms, long* launches, int reset);
 long sac_kernel_launches(const sac_ctx* c);
 
+/* ---- getdt that allocates nothing (library extension; no reference counterpart) ----
+ * Same result and side effects as sac_getdt.  Its getdt_courant reduction runs as a
+ * deterministic two-pass block reduction whose scratch (8192 partial maxima and the
+ * result) is a file-scope device array of the library, not memory of the context,
+ * and the call makes no cudaMalloc/cudaFree or other allocating call.
+ *   - Limit: meshes of at most SAC_STATIC_MAX_CELLS cells; a larger mesh returns
+ *     SAC_ERR_UNSUPPORTED with the sizes in sac_last_error (use sac_getdt there).
+ *   - The scratch is one per device, shared by every context on it: calls that
+ *     overlap in time (other host threads, other streams) race on it.
+ *   - The first call on a device does the set-up (cudaGetSymbolAddress of the
+ *     scratch); make it before any stream capture.
+ *   - Nothing in the scratch has to start at zero: each slot that is read was
+ *     written earlier in the same call. */
+#define SAC_STATIC_MAX_CELLS 33554432L
+sac_status sac_getdt_static(sac_ctx* c, double* dt, int it);
+
 /* ---- many independent grids (library extension, no Fortran counterpart) ----
  * A batch advances ninst uneven 1D/2D problems together, each with its own dt,
  * with typeadvance='fourstep' (the RK4 step of src/vac.t:439-455) and the dt

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -316,6 +317,114 @@ template <typename S>
 __global__ void k_lin_threestep_b(S* w, const S* w2, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
     w[i] = w[i] / S(3) + w2[i] * S(2.0 / 3);
+}
+
+// ---------------------------------------------------------------------------
+// getdt_courant with file-scope scratch (sac_getdt_static): a two-pass,
+// deterministic block reduction.  Pass 1 writes one partial maximum per block
+// of kStaticCellsPerBlock mesh cells; pass 2 reduces the partials into the
+// slot after them.  Every slot read is written earlier in the same call, so
+// nothing has to start at zero.
+// ---------------------------------------------------------------------------
+constexpr int kStaticPartials = 8192;
+constexpr long kStaticCellsPerBlock = 256L * 16;
+constexpr long kStaticMaxCells = kStaticPartials * kStaticCellsPerBlock;  // 33,554,432 mesh cells
+static_assert(kStaticMaxCells == SAC_STATIC_MAX_CELLS, "the header states the limit");
+__device__ __align__(256) double g_courant_scratch[kStaticPartials + 1];  // partials, then the result
+
+// block max of non-negative values, NaN-sticky; valid in thread 0
+__device__ __forceinline__ double block_max_value(double v, double* sh) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const bool anynan = __syncthreads_or(v != v);
+  v = (v != v) ? 0.0 : v;
+  v = warp_max(v);
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double m = 0.0;
+  if (tid < 32) {
+    m = (tid < (int)(blockDim.x + 31) / 32) ? sh[tid] : 0.0;
+    m = warp_max(m);
+  }
+  return anynan ? __longlong_as_double(0x7ff8000000000000ll) : m;
+}
+
+template <int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_courant_partial(Geom g, const S* __restrict__ wp,
+                                                         const double* __restrict__ bgv,
+                                                         const double* __restrict__ dx, double* part,
+                                                         double gamma) {
+  __shared__ double sh[32];
+  const long nm0 = g.hi[0] - g.lo[0] + 1, nm1 = g.hi[1] - g.lo[1] + 1, nm2 = g.hi[2] - g.lo[2] + 1;
+  const long tot = nm0 * nm1 * nm2;
+  const long t0 = blockIdx.x * kStaticCellsPerBlock;
+  const long t1 = t0 + kStaticCellsPerBlock < tot ? t0 + kStaticCellsPerBlock : tot;
+  double best = 0.0;
+  for (long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+    const int i0 = g.lo[0] + (int)(t % nm0);
+    const int i1 = g.lo[1] + (int)((t / nm0) % nm1);
+    const int i2 = g.lo[2] + (int)(t / (nm0 * nm1));
+    best = max_sticky(best, courant_cell<NDIR, S>(g, wp, bgv, dx, i0, i1, i2, gamma));
+  }
+  best = block_max_value(best, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = best;
+}
+
+__global__ void __launch_bounds__(1024) k_courant_final(double* part, int n) {
+  __shared__ double sh[32];
+  double best = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) best = max_sticky(best, part[i]);
+  best = block_max_value(best, sh);
+  if (threadIdx.x == 0) part[kStaticPartials] = best;
+}
+
+// device address of g_courant_scratch per device ordinal, looked up once
+std::mutex g_static_mu;
+double* g_static_addr[64] = {};
+
+sac_status static_scratch(sac_ctx* c, double** out) {
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (c->dev < 0 || c->dev >= 64) return fail(c, SAC_ERR_ARG, "device ordinal out of range");
+  if (!g_static_addr[c->dev]) {
+    void* p = nullptr;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaGetSymbolAddress(&p, g_courant_scratch));
+    g_static_addr[c->dev] = (double*)p;
+  }
+  *out = g_static_addr[c->dev];
+  return SAC_OK;
+}
+
+// max over the mesh of cmax/dx into *cm, scratch in g_courant_scratch
+sac_status courant_max_static(sac_ctx* c, double* cm) {
+  const Geom& g = c->g;
+  const long nm = (long)(g.hi[0] - g.lo[0] + 1) * (g.hi[1] - g.lo[1] + 1) * (g.hi[2] - g.lo[2] + 1);
+  if (nm > kStaticMaxCells)
+    return fail(c, SAC_ERR_UNSUPPORTED,
+                "sac_getdt_static: the mesh has " + std::to_string(nm) + " cells, more than the " +
+                    std::to_string(kStaticMaxCells) + " its static scratch covers; use sac_getdt");
+  double* part = nullptr;
+  sac_status st = static_scratch(c, &part);
+  if (st != SAC_OK) return st;
+  const int nb = (int)((nm + kStaticCellsPerBlock - 1) / kStaticCellsPerBlock);
+  auto launch = [&](auto S0) {
+    using S = decltype(S0);
+    const S* wp = (const S*)c->P[0];
+    switch (g.ndir) {
+      case 1: k_courant_partial<1, S><<<nb, 256, 0, c->stream>>>(g, wp, c->BG, c->dx, part, c->par.gamma); break;
+      case 2: k_courant_partial<2, S><<<nb, 256, 0, c->stream>>>(g, wp, c->BG, c->dx, part, c->par.gamma); break;
+      default: k_courant_partial<3, S><<<nb, 256, 0, c->stream>>>(g, wp, c->BG, c->dx, part, c->par.gamma); break;
+    }
+  };
+  if (c->prec == SAC_PREC_FP32)
+    launch(0.0f);
+  else
+    launch(0.0);
+  k_courant_final<<<1, 1024, 0, c->stream>>>(part, nb);
+  c->kernel_launches += 2;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(cm, part + kStaticPartials, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SAC_OK;
 }
 
 }  // namespace
@@ -637,7 +746,7 @@ sac_status sac_getboundary(sac_ctx* c, double t) {
 }
 
 // the dt block of program vac, src/vac.t:61-70
-sac_status sac_getdt(sac_ctx* c, double* dt, int it) {
+static sac_status getdt_impl(sac_ctx* c, double* dt, int it, bool static_scratch_courant) {
   if (!c || !dt) return SAC_ERR_ARG;
   if (!c->state_set || !c->bc_set) return fail(c, SAC_ERR_STATE, "state and boundaries must be set");
   CK(cudaSetDevice(c->dev));
@@ -651,7 +760,14 @@ sac_status sac_getdt(sac_ctx* c, double* dt, int it) {
     d = c->par.dtpar;
   } else {
     d = bigdouble;
-    if (c->par.courantpar > 0.0) {  // getdt_courant, src/vac.t:641-699
+    if (c->par.courantpar > 0.0 && static_scratch_courant) {  // getdt_courant, src/vac.t:641-699
+      double courantmax = 0.0;
+      sac_status st = courant_max_static(c, &courantmax);
+      if (st != SAC_OK) return st;
+      if (!(courantmax == courantmax) || std::isinf(courantmax))
+        return fail(c, SAC_ERR_NONFINITE, "non-finite wave speed in getdt_courant");
+      if (courantmax > smalldouble) d = std::min(d, c->par.courantpar / courantmax);
+    } else if (c->par.courantpar > 0.0) {  // getdt_courant, src/vac.t:641-699
       CK(cudaMemsetAsync(c->red + 4, 0, sizeof(unsigned long long), c->stream));
       const long nm = (long)(g.hi[0] - g.lo[0] + 1) * (g.hi[1] - g.lo[1] + 1) * (g.hi[2] - g.lo[2] + 1);
       const int bs = 256;
@@ -713,6 +829,10 @@ sac_status sac_getdt(sac_ctx* c, double* dt, int it) {
   *dt = d;
   return SAC_OK;
 }
+
+sac_status sac_getdt(sac_ctx* c, double* dt, int it) { return getdt_impl(c, dt, it, false); }
+
+sac_status sac_getdt_static(sac_ctx* c, double* dt, int it) { return getdt_impl(c, dt, it, true); }
 
 sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmin, int idimmax, double dt, double t,
                       int it) {
