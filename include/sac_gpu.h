@@ -62,8 +62,8 @@ typedef int sac_status;
  *                      vacusr.viscosity.t without a driver)
  *   SAC_USR_STRAT      gravity + hyperdiffusion + a vertical-velocity driver near the
  *                      lower x1 boundary (stratified-atmosphere workload)
- *   SAC_USR_TUBE       gravity + hyperdiffusion + a horizontal-velocity driver near the
- *                      lower x2 boundary (2D flux-tube workload)              */
+ *   SAC_USR_TUBE       gravity + hyperdiffusion + a horizontal (x2) velocity driver near
+ *                      the lower x1 boundary (2D flux-tube workload)          */
 #define SAC_USR_NONE 0
 #define SAC_USR_VISCOSITY 1
 #define SAC_USR_SLOG 2
@@ -185,8 +185,9 @@ sac_status sac_getdt_static(sac_ctx* c, double* dt, int it);
  * block of src/vac.t:60-70 per instance.  Every instance is a separate program
  * vac run: the same parameters (sac_params, shared), its own mesh nx(ndim) with
  * two ghost layers per side, its own coordinates and state.  Boundary types that
- * store ghost values (fixed, fixed1, grad1) and the user drivers (slog, strat,
- * tube) are not available here (SAC_ERR_UNSUPPORTED).
+ * store ghost values (fixed, fixed1, grad1) and the Slog driver are not available
+ * here (SAC_ERR_UNSUPPORTED); the Gaussian drivers (strat, tube) take their
+ * amplitude and frequency per instance (sac_batch_set_driver).
  *
  * Host arrays are the instances' Fortran-order blocks one after another:
  *   x: instance i contributes x(ixG^T,ndim), w: instance i contributes w(ixG^T,nw),
@@ -217,6 +218,24 @@ void* sac_batch_get_stream(const sac_batch* b);
 /* time the update pass for each candidate tile shape on this batch and keep the
  * fastest; tile_xy[2] and ms (per update pass) receive the choice (may be NULL) */
 sac_status sac_batch_tune(sac_batch* b, int* tile_xy, double* ms);
+/* per-instance driver amplitude and angular frequency of the Gaussian velocity
+ * drivers (users SAC_USR_STRAT and SAC_USR_TUBE, tdep = sin(omega t)); the
+ * defaults are userpar[0] and userpar[1].  Either array may be NULL. */
+sac_status sac_batch_set_driver(sac_batch* b, const double* A, const double* omega);
+/* per-instance time and step counter (either may be NULL) */
+sac_status sac_batch_set_time(sac_batch* b, const double* t, const int* it);
+/* mesh cells over all instances (ghosts excluded) */
+long sac_batch_mesh_cells(const sac_batch* b);
+/* Packed mesh copies between the resident state and a DEVICE buffer, enqueued on
+ * the batch stream: instance i contributes np*mesh_i values, variable-major
+ * (rho, m.., e, b..), x1 fastest, ghosts excluded, in instance order.  dtype
+ * SAC_PACK_F32 | SAC_PACK_BF16 | SAC_PACK_F64.  After a scatter, call
+ * sac_batch_getboundary to refill the ghost cells. */
+#define SAC_PACK_F32 0
+#define SAC_PACK_BF16 1
+#define SAC_PACK_F64 2
+sac_status sac_batch_gather(sac_batch* b, void* dev, int dtype);
+sac_status sac_batch_scatter(sac_batch* b, const void* dev, int dtype);
 const char* sac_batch_last_error(const sac_batch* b);
 void sac_batch_destroy(sac_batch* b);
 

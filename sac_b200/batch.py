@@ -40,12 +40,19 @@ def _bind(lib):
     f("get_stream").argtypes = [P]
     f("get_stream").restype = ctypes.c_void_p
     f("tune").argtypes = [P, IP, DP]
+    f("set_driver").argtypes = [P, DP, DP]
+    f("set_time").argtypes = [P, DP, IP]
+    f("mesh_cells").argtypes = [P]
+    f("mesh_cells").restype = ctypes.c_long
+    f("gather").argtypes = [P, ctypes.c_void_p, ctypes.c_int]
+    f("scatter").argtypes = [P, ctypes.c_void_p, ctypes.c_int]
     f("last_error").argtypes = [P]
     f("last_error").restype = ctypes.c_char_p
     f("destroy").argtypes = [P]
     f("destroy").restype = None
     for n in ("create", "set_grid", "set_boundaries", "upload", "download", "upload_range", "download_range",
-              "getboundary", "advance", "state", "synchronize", "tune"):
+              "getboundary", "advance", "state", "synchronize", "tune", "set_driver", "set_time", "gather",
+              "scatter"):
         f(n).restype = ctypes.c_int
     lib._sac_batch_bound = True
     return lib
@@ -127,6 +134,34 @@ class Batch:
 
     def stream(self):
         return self.lib.sac_batch_get_stream(self.h)
+
+    def set_driver(self, A=None, omega=None):
+        """Per-instance amplitude and angular frequency of the Gaussian driver."""
+        a = None if A is None else np.ascontiguousarray(A, dtype=np.float64)
+        o = None if omega is None else np.ascontiguousarray(omega, dtype=np.float64)
+        self._call("set_driver", _dp(a) if a is not None else None, _dp(o) if o is not None else None)
+
+    def set_time(self, t=None, it=None):
+        ta = None if t is None else np.ascontiguousarray(t, dtype=np.float64)
+        ia = None if it is None else np.ascontiguousarray(it, dtype=np.int32)
+        self._call("set_time", _dp(ta) if ta is not None else None,
+                   ia.ctypes.data_as(IP) if ia is not None else None)
+
+    PACK = {"f32": 0, "bf16": 1, "f64": 2}
+
+    def gather(self, dev_ptr: int, dtype="f32"):
+        """Advanced variables on every instance's mesh into a packed device buffer
+        (np*mesh_i values per instance, variable-major, x1 fastest); asynchronous
+        on the batch stream."""
+        self._call("gather", ctypes.c_void_p(int(dev_ptr)), self.PACK[dtype])
+
+    def scatter(self, dev_ptr: int, dtype="f32"):
+        """The reverse of gather; refill the ghosts with getboundary() afterwards."""
+        self._call("scatter", ctypes.c_void_p(int(dev_ptr)), self.PACK[dtype])
+
+    @property
+    def packed_size(self):
+        return int(self.lib.sac_batch_mesh_cells(self.h)) * (2 * self.ndir + 2)
 
     def tune(self):
         tile = np.zeros(2, dtype=np.int32)

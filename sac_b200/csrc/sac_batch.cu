@@ -12,6 +12,7 @@
 //
 // Each instance follows exactly the single-grid path (sac_gpu.cu): the same cell
 // bodies, the same ghost resolve, the same dt rules of src/vac.t:61-70.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -53,11 +54,14 @@ struct sac_batch {
   void* P[4] = {nullptr, nullptr, nullptr, nullptr};
   double* BG = nullptr;
   double* dx = nullptr;
+  double* drv = nullptr;  // driver profiles [2][totX] (users strat and tube)
   double* stg = nullptr;
   InstDyn* d_dyn = nullptr;
   InstInfo* d_inst = nullptr;  // global table (courant pass, boundaries)
   Tile* d_cour = nullptr;
   int n_cour = 0;
+  long* d_meshoff = nullptr;  // per instance: first mesh cell in the packed mesh order
+  long mesh_total = 0;
   GhostChunk* d_gh_all = nullptr;
   int n_gh_all = 0;
   std::vector<Group> groups;
@@ -187,6 +191,38 @@ __global__ void kb_time(InstDyn* dyn, int n) {
   dyn[i].it += 1;
 }
 
+template <typename D>
+__device__ __forceinline__ D to_t(double v) { return (D)v; }
+template <>
+__device__ __forceinline__ __nv_bfloat16 to_t<__nv_bfloat16>(double v) { return __float2bfloat16((float)v); }
+__device__ __forceinline__ double to_d(double v) { return v; }
+__device__ __forceinline__ double to_d(float v) { return (double)v; }
+__device__ __forceinline__ double to_d(__nv_bfloat16 v) { return (double)__bfloat162float(v); }
+
+// packed mesh order: instance i owns np*mesh_i consecutive values, variable-major,
+// x1 fastest, ghosts excluded.  dir 0: state -> packed (gather), 1: packed -> state.
+template <typename S, typename D>
+__global__ void __launch_bounds__(256) kb_pack(const InstInfo* __restrict__ inst, const Tile* __restrict__ tiles,
+                                               int ntiles, const long* __restrict__ meshoff, S* P0, long sP, D* pk,
+                                               int np, int dir) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    const Geom& g = inst[tl.inst].g;
+    const int p0 = tl.p[0] + threadIdx.x, p1 = tl.p[1] + threadIdx.y;
+    if (p0 > g.hi[0] || p1 > g.hi[1]) continue;
+    const long nm0 = g.hi[0] - g.lo[0] + 1, nm = nm0 * (g.hi[1] - g.lo[1] + 1);
+    const long q = (p1 - g.lo[1]) * nm0 + (p0 - g.lo[0]);
+    const long c = inst[tl.inst].o.P + p0 + g.st[1] * p1;
+    D* dst = pk + meshoff[tl.inst] * np + q;
+    for (int iw = 0; iw < np; ++iw) {
+      if (dir == 0)
+        dst[(long)iw * nm] = to_t<D>(to_d(P0[(long)iw * sP + c]));
+      else
+        P0[(long)iw * sP + c] = (S)to_d(dst[(long)iw * nm]);
+    }
+  }
+}
+
 BcArgs bc_proto(sac_batch* b, void* A) {
   BcArgs a{};
   a.A = A;
@@ -231,6 +267,9 @@ Stage2Args stage_base(sac_batch* b) {
   a.grav_on = (b->par.sourceunsplit && grav_mod(b->par.user)) ? 1 : 0;
   a.visc_on = (b->par.sourceunsplit && visc_on_b(b)) ? 1 : 0;
   a.driver = DRV_NONE;
+  if (b->par.sourceunsplit && b->drv)
+    a.driver = b->par.user == SAC_USR_STRAT ? DRV_STRAT : DRV_TUBE;  // amplitude and omega per instance
+  a.drv = b->drv;
   return a;
 }
 
@@ -348,7 +387,7 @@ void free_all(sac_batch* b) {
     if (p) cudaFree((void*)p);
     p = nullptr;
   };
-  fr(b->BG), fr(b->dx), fr(b->stg), fr(b->d_dyn), fr(b->d_inst), fr(b->d_cour), fr(b->d_gh_all);
+  fr(b->BG), fr(b->dx), fr(b->drv), fr(b->stg), fr(b->d_dyn), fr(b->d_inst), fr(b->d_cour), fr(b->d_gh_all), fr(b->d_meshoff);
   fr(b->D), fr(b->F), fr(b->R), fr(b->d_type), fr(b->d_fixed), fr(b->d_fixB);
   for (Group& gr : b->groups) fr(gr.d_inst), fr(gr.d_face), fr(gr.d_nu), fr(gr.d_upd), fr(gr.d_gh);
 }
@@ -366,7 +405,7 @@ sac_status sac_batch_create(const sac_params* p, int ndim, int ndir, int ninst, 
   if (ndim < 1 || ndim > 2 || ndir < ndim || ndir > 3) return SAC_ERR_UNSUPPORTED;
   if (std::string(p->typeadvance) != "fourstep") return SAC_ERR_UNSUPPORTED;
   if (p->precision != SAC_PREC_FP64 && p->precision != SAC_PREC_FP32) return SAC_ERR_UNSUPPORTED;
-  if (p->user == SAC_USR_SLOG || p->user == SAC_USR_STRAT || p->user == SAC_USR_TUBE) return SAC_ERR_UNSUPPORTED;
+  if (p->user == SAC_USR_SLOG || (p->user == SAC_USR_TUBE && ndim < 2)) return SAC_ERR_UNSUPPORTED;
   sac_batch* b = new sac_batch();
   b->par = *p;
   b->dev = p->device;
@@ -449,6 +488,8 @@ sac_status sac_batch_set_grid(sac_batch* b, const double* x) {
   BK(cudaSetDevice(b->dev));
   const int ndim = b->ndim;
   std::vector<double> hdx((size_t)ndim * b->totX);
+  const bool gauss = b->par.user == SAC_USR_STRAT || b->par.user == SAC_USR_TUBE;
+  std::vector<double> hdrv(gauss ? (size_t)2 * b->totX : 0), prof;
   b->mindx2.assign((size_t)b->ninst * 3, 0.0);
   b->dtgrav.assign(b->ninst, kBig);
   long xoff = 0;
@@ -457,6 +498,13 @@ sac_status sac_batch_set_grid(sac_batch* b, const double* x) {
     std::vector<double> hx1, hdx1;
     gridsetup1(g.n, g.lo, g.hi, ndim, g.ncell, x + xoff, false, hx1, hdx1);
     xoff += (long)ndim * g.ncell;
+    if (gauss) {
+      prof.assign((size_t)2 * g.ncell, 0.0);
+      gauss_driver_profiles(b->par.user, ndim, g.ncell, hx1.data(), b->par.userpar, prof.data());
+      for (int k = 0; k < 2; ++k)
+        std::copy(prof.begin() + (long)k * g.ncell, prof.begin() + (long)(k + 1) * g.ncell,
+                  hdrv.begin() + (long)k * b->totX + b->h_inst[i].o.X);
+    }
     double mindx_all = kBig;
     for (int d = 0; d < ndim; ++d) {
       double m2 = kBig;
@@ -481,6 +529,10 @@ sac_status sac_batch_set_grid(sac_batch* b, const double* x) {
   BK(cudaMalloc(&b->BG, sizeof(double) * (b->nw - b->np) * b->totP));
   BK(cudaMalloc(&b->dx, sizeof(double) * ndim * b->totX));
   BK(cudaMemcpy(b->dx, hdx.data(), sizeof(double) * hdx.size(), cudaMemcpyHostToDevice));
+  if (gauss) {
+    BK(cudaMalloc(&b->drv, sizeof(double) * hdrv.size()));
+    BK(cudaMemcpy(b->drv, hdrv.data(), sizeof(double) * hdrv.size(), cudaMemcpyHostToDevice));
+  }
   BK(cudaMalloc(&b->D, es * (b->ndir + 3) * b->maxI));
   BK(cudaMalloc(&b->F, es * (size_t)ndim * b->np * b->maxI));
   BK(cudaMalloc(&b->R, es * (size_t)nr_pairs(ndim) * b->maxI));
@@ -498,11 +550,22 @@ sac_status sac_batch_set_grid(sac_batch* b, const double* x) {
     }
     if ((st = upload_vec(b, &gr.d_inst, t)) != SAC_OK) return st;
   }
+  std::vector<long> moff(b->ninst + 1, 0);
+  for (int i = 0; i < b->ninst; ++i) {
+    const Geom& g = b->h_inst[i].g;
+    long nm = 1;
+    for (int d = 0; d < ndim; ++d) nm *= g.hi[d] - g.lo[d] + 1;
+    moff[i + 1] = moff[i] + nm;
+  }
+  b->mesh_total = moff[b->ninst];
+  if ((st = upload_vec(b, &b->d_meshoff, moff)) != SAC_OK) return st;
   std::vector<InstDyn> dyn(b->ninst);
   for (int i = 0; i < b->ninst; ++i) {
     std::memset(&dyn[i], 0, sizeof(InstDyn));
     for (int d = 0; d < 3; ++d) dyn[i].mindx2[d] = b->mindx2[i * 3 + d];
     dyn[i].dtgrav = b->dtgrav[i];
+    dyn[i].drvA = b->par.userpar[0];
+    dyn[i].omega = b->par.userpar[1];
   }
   if ((st = upload_vec(b, &b->d_dyn, dyn)) != SAC_OK) return st;
   if ((st = build_lists(b)) != SAC_OK) return st;
@@ -751,5 +814,75 @@ sac_status sac_batch_tune(sac_batch* b, int* tile_out, double* ms_out) {
   if (ms_out) *ms_out = best;
   return SAC_OK;
 }
+
+
+// per-instance driver amplitude A and angular frequency omega (tdep = sin(omega t));
+// either array may be NULL to keep the current values
+sac_status sac_batch_set_driver(sac_batch* b, const double* A, const double* omega) {
+  if (!b) return SAC_ERR_ARG;
+  if (!b->grid_set) return bfail(b, SAC_ERR_STATE, "sac_batch_set_grid first");
+  BK(cudaSetDevice(b->dev));
+  std::vector<InstDyn> dyn(b->ninst);
+  BK(cudaMemcpyAsync(dyn.data(), b->d_dyn, sizeof(InstDyn) * b->ninst, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < b->ninst; ++i) {
+    if (A) dyn[i].drvA = A[i];
+    if (omega) dyn[i].omega = omega[i];
+  }
+  BK(cudaMemcpyAsync(b->d_dyn, dyn.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  return SAC_OK;
+}
+
+// per-instance time t and step count it (either may be NULL to keep them); a
+// step counter of 0 makes the next step the first one (no dtcantgrow bound)
+sac_status sac_batch_set_time(sac_batch* b, const double* t, const int* it) {
+  if (!b) return SAC_ERR_ARG;
+  if (!b->grid_set) return bfail(b, SAC_ERR_STATE, "sac_batch_set_grid first");
+  BK(cudaSetDevice(b->dev));
+  std::vector<InstDyn> dyn(b->ninst);
+  BK(cudaMemcpyAsync(dyn.data(), b->d_dyn, sizeof(InstDyn) * b->ninst, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < b->ninst; ++i) {
+    if (t) dyn[i].t = t[i];
+    if (it) dyn[i].it = it[i];
+  }
+  BK(cudaMemcpyAsync(b->d_dyn, dyn.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  return SAC_OK;
+}
+
+long sac_batch_mesh_cells(const sac_batch* b) { return b ? b->mesh_total : 0; }
+
+static sac_status pack(sac_batch* b, void* dev, int dtype, int dir) {
+  if (!b || !dev || dtype < 0 || dtype > 2) return SAC_ERR_ARG;
+  if (!b->state_set) return bfail(b, SAC_ERR_STATE, "no state on the device");
+  BK(cudaSetDevice(b->dev));
+  const unsigned grid = (unsigned)std::min<long>(b->n_cour, 148L * 8);
+  auto go = [&](auto S0) {
+    using S = decltype(S0);
+    S* P0 = (S*)b->P[0];
+    if (dtype == SAC_PACK_F32)
+      kb_pack<S, float><<<grid, dim3(32, 8), 0, b->stream>>>(b->d_inst, b->d_cour, b->n_cour, b->d_meshoff, P0,
+                                                               b->totP, (float*)dev, b->np, dir);
+    else if (dtype == SAC_PACK_BF16)
+      kb_pack<S, __nv_bfloat16><<<grid, dim3(32, 8), 0, b->stream>>>(
+          b->d_inst, b->d_cour, b->n_cour, b->d_meshoff, P0, b->totP, (__nv_bfloat16*)dev, b->np, dir);
+    else
+      kb_pack<S, double><<<grid, dim3(32, 8), 0, b->stream>>>(b->d_inst, b->d_cour, b->n_cour, b->d_meshoff, P0,
+                                                                b->totP, (double*)dev, b->np, dir);
+  };
+  if (b->prec == SAC_PREC_FP32)
+    go(0.0f);
+  else
+    go(0.0);
+  BK(cudaGetLastError());
+  return SAC_OK;
+}
+
+// the advanced variables on the mesh of every instance to / from a packed
+// device buffer (asynchronous on the batch stream)
+sac_status sac_batch_gather(sac_batch* b, void* dev, int dtype) { return pack(b, dev, dtype, 0); }
+sac_status sac_batch_scatter(sac_batch* b, const void* dev, int dtype) { return pack(b, (void*)dev, dtype, 1); }
 
 }  // extern "C"

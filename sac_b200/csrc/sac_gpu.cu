@@ -556,18 +556,11 @@ sac_status sac_set_grid(sac_ctx* c, int ndim, int ndir, const int ixGhi[3], cons
         hdrv[q] = (ux / std::sqrt(ux * ux + uy * uy)) * exyz;
         hdrv[N + q] = (uy / std::sqrt(ux * ux + uy * uy)) * exyz;
         c->drvA = 10.0;
-      } else if (u == SAC_USR_STRAT) {
-        const double xx = ndim > 1 ? x2 - up[2] : 0.0, yy = ndim > 2 ? x3 - up[3] : 0.0, zz = x1 - up[5];
-        hdrv[q] = std::exp(-(xx * xx + yy * yy) / (up[4] * up[4]));
-        hdrv[N + q] = std::exp(-(zz * zz) / (up[6] * up[6]));
-        c->drvA = up[0];
       } else {
-        const double zz = x1 - up[2], xx = x2 - up[4];
-        hdrv[q] = std::exp(-(zz * zz) / (up[3] * up[3]));
-        hdrv[N + q] = std::exp(-(xx * xx) / (up[5] * up[5]));
         c->drvA = up[0];
       }
     }
+    if (u == SAC_USR_STRAT || u == SAC_USR_TUBE) gauss_driver_profiles(u, ndim, N, hx.data(), up, hdrv.data());
   }
   const size_t bp = c->es * g.np * N;
   for (auto& p : c->P) CK(cudaMalloc(&p, bp));

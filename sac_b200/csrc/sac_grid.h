@@ -3,6 +3,7 @@
 // dx = (x(+1) - x(-1))/2 over the whole grid.  Shared by the single-grid and the
 // batched contexts so that both see the same cell widths as the reference.
 #pragma once
+#include <cmath>
 #include <cstdlib>
 #include <vector>
 
@@ -77,6 +78,28 @@ inline void gridsetup1(const int n[3], const int lo[3], const int hi[3], int ndi
           m[d] -= 1;
           hdx[d * ncell + gid(i, j, k)] = 0.5 * (qx[d * qc + qid(p[0], p[1], p[2])] - qx[d * qc + qid(m[0], m[1], m[2])]);
         }
+}
+
+// Spatial profiles of the Gaussian velocity drivers on the full grid, two
+// blocks of ncell: the stratified workload (user 4: horizontal Gaussian of width
+// up[4] about (up[2], up[3]) times a vertical one of width up[6] about x1=up[5])
+// and the flux tube (user 5: a Gaussian of width up[3] about x1=up[2] times one
+// of width up[5] about x2=up[4]).  The time factor A sin(omega t) is applied in
+// the stage update.
+inline void gauss_driver_profiles(int user, int ndim, long ncell, const double* hx, const double* up,
+                                  double* out) {
+  for (long q = 0; q < ncell; ++q) {
+    const double x1 = hx[q], x2 = ndim > 1 ? hx[ncell + q] : 0.0, x3 = ndim > 2 ? hx[2 * ncell + q] : 0.0;
+    if (user == 4) {
+      const double xx = ndim > 1 ? x2 - up[2] : 0.0, yy = ndim > 2 ? x3 - up[3] : 0.0, zz = x1 - up[5];
+      out[q] = std::exp(-(xx * xx + yy * yy) / (up[4] * up[4]));
+      out[ncell + q] = std::exp(-(zz * zz) / (up[6] * up[6]));
+    } else {
+      const double zz = x1 - up[2], xx = x2 - up[4];
+      out[q] = std::exp(-(zz * zz) / (up[3] * up[3]));
+      out[ncell + q] = std::exp(-(xx * xx) / (up[5] * up[5]));
+    }
+  }
 }
 
 }  // namespace sacgpu

@@ -52,6 +52,7 @@ struct InstDyn {
   double dt, t;
   double mindx2[3];  // min over the mesh of dx^2 per dimension (getdt_visc)
   double dtgrav;     // getdt_grav, fixed at the first step
+  double drvA, omega;  // velocity driver amplitude and angular frequency (tdep = sin(omega t))
   unsigned long long ctot[3], maxnu, courant;  // bits of non-negative maxima
   int it, bad;       // step counter; set when a reduction met NaN/Inf
 };

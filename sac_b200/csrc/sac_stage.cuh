@@ -194,7 +194,8 @@ __device__ __forceinline__ void nu_cell(const Stage2Args& a, const Geom& g, cons
 // k_update body at the mesh cell pos
 template <int NDIM, int NDIR, typename S>
 __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, const Offs& o, const int pos[3],
-                                            double qdt_d, double qdt2_d, double tdep, double& numax_out) {
+                                            double qdt_d, double qdt2_d, double tdep, double drvA,
+                                            double& numax_out) {
   using PR = Pairs<NDIM>;
   using T = S;
   constexpr int NP = 2 * NDIR + 2, E = NDIR + 1, B0 = NDIR + 1;
@@ -409,15 +410,15 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
       const T rtn = (T)((double)acc[0] + __ldg(BG(1) + c));
       if (a.driver == DRV_SLOG) {
         // src/vacusr.f:1355-1375 (x1 vertical; m2, m3 driven)
-        const T vvx = (T)(__ldg(a.drv + o.X + c) * tdep * a.drvA);
-        const T vvy = (T)(__ldg(a.drv + a.sX + o.X + c) * tdep * a.drvA);
+        const T vvx = (T)(__ldg(a.drv + o.X + c) * tdep * drvA);
+        const T vvy = (T)(__ldg(a.drv + a.sX + o.X + c) * tdep * drvA);
         if (NDIR >= 3) {
           acc[2] = acc[2] + rtn * vvx * q2;
           acc[3 % NP] = acc[3 % NP] + rtn * vvy * q2;
         }
         acc[E] = acc[E] + rtn * (vvx * vvx + vvy * vvy + T(0) * T(0)) * q2 / T(2);
       } else {
-        const T v = (T)(a.drvA * tdep * __ldg(a.drv + o.X + c) * __ldg(a.drv + a.sX + o.X + c));
+        const T v = (T)(drvA * tdep * __ldg(a.drv + o.X + c) * __ldg(a.drv + a.sX + o.X + c));
         const int comp = (a.driver == DRV_STRAT) ? 1 : 2;
         acc[comp] = acc[comp] + rtn * v * q2;
         acc[E] = acc[E] + rtn * (v * v) * q2 / T(2);
@@ -497,7 +498,7 @@ __global__ void __launch_bounds__(256, 2) k_update(const Stage2Args a) {
   pos[2] = g.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
   double numax = 0.0;
   if (pos[0] <= g.hi[0] && pos[1] <= g.hi[1] && pos[2] <= g.hi[2])
-    update_cell<NDIM, NDIR, S>(a, g, Offs{0, 0, 0, 0}, pos, a.qdt, a.qdt2, a.tdep, numax);
+    update_cell<NDIM, NDIR, S>(a, g, Offs{0, 0, 0, 0}, pos, a.qdt, a.qdt2, a.tdep, a.drvA, numax);
   if (a.visc_on) block_max_to(a.maxnu, numax, sh);
 }
 
@@ -566,11 +567,14 @@ __global__ void __launch_bounds__(256, 2) kb_update(const BatchStageArgs b) {
     int p[3];
     double numax = 0.0;
     if (tile_cell(tl, g, g.lo, g.hi, p)) {
-      // the RK4 stage steps of advect, src/vac.t:442-452
-      const double dt = b.dyn[tl.inst].dt;
+      // the RK4 stage steps of advect, src/vac.t:442-452; every stage sees the
+      // driver at the step's start time t (advect1 is called with t)
+      const InstDyn& D = b.dyn[tl.inst];
+      const double dt = D.dt;
       const double qdt = b.stage == 0 ? dt / 2 : b.stage == 1 ? dt / 2 : b.stage == 2 ? dt : dt / 6;
       const double qdt2 = qdt * ((double)(b.a.dmax - b.a.dmin) + 1.0) / (double)g.ndim;
-      update_cell<NDIM, NDIR, S>(b.a, g, I.o, p, qdt, qdt2, 0.0, numax);
+      const double tdep = b.a.driver != DRV_NONE ? sin(D.omega * D.t) : 0.0;
+      update_cell<NDIM, NDIR, S>(b.a, g, I.o, p, qdt, qdt2, tdep, D.drvA, numax);
     }
     if (b.a.visc_on) block_max_to(&b.dyn[tl.inst].maxnu, numax, sh);
   }

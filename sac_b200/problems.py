@@ -265,5 +265,50 @@ def orszag_tang(n=(64, 64), beta=1.0, gamma=5.0 / 3.0, B0=None, nu=1.0, typeadva
                    uniform_types(ndim, v["nw"], "periodic"))
 
 
-__all__ = ["Problem", "brio_wu", "stratified", "random_problem", "orszag_tang", "var_index",
+# ---------------------------------------------------------------------------
+# 2D magnetic flux tube in a stratified atmosphere (x1 vertical, x2 horizontal)
+# ---------------------------------------------------------------------------
+def flux_tube(n=(256, 256), height=2.0, half_width=1.0, H=0.3, B0=0.5, tube_w2=0.04, g=1.0, rho0=100.0,
+              gamma=5.0 / 3.0, A=1.0e-3, omega=None, z0=0.1, dz0=0.05, drv_w=0.1, nu=1.0,
+              courantpar=0.8, dtpar=-1.0, typeadvance="fourstep") -> Problem:
+    """Vertical flux tube B_b = (B_z(x), 0), B_z = B0 exp(-x^2/tube_w2), in an
+    atmosphere with rho_b = rho0 exp(-z/H) and gravity g along -x1, on z in [0, height]
+    (x1), x in [-half_width, half_width] (x2).
+
+    Magnetohydrostatic balance is exact: with straight vertical field lines the
+    Lorentz force is the horizontal magnetic-pressure gradient only, so
+    p_b = rho0 g H exp(-z/H) + (B0^2 - B_z(x)^2)/2 balances it in x (p_b + B_z^2/2
+    depends on z alone) and balances gravity in z (d p_b/dz = -rho_b g).  The
+    gas is isothermal (p_b/rho_b = g H) on the tube axis; away from it the
+    constant B0^2/2 added to the pressure heats the upper layers.  rho0 = 100
+    puts the plasma-beta = 1 layer of the tube axis inside the domain (beta 240
+    at the base, 0.3 at the top) and keeps the fastest wave speed near 1.6.  Zero
+    initial perturbation; a horizontal velocity driver
+    v_x = A sin(omega t) exp(-x^2/drv_w^2) exp(-(z-z0)^2/dz0^2) near the base
+    (omega defaults to the acoustic cut-off sqrt(gamma g H)/(2H)); open (cont)
+    x1 boundaries, periodic x2."""
+    ndim, ndir = 2, 2
+    x = make_grid(n, (0.0, -half_width), (height, half_width))
+    w = empty_state(n, ndir)
+    v = var_index(ndir)
+    z, xh = x[..., 0], x[..., 1]
+    rhob = rho0 * np.exp(-z / H)
+    bz = B0 * np.exp(-(xh * xh) / tube_w2)
+    pb = g * H * rhob + 0.5 * (B0 * B0 - bz * bz)
+    w[..., v["rhob"]] = rhob
+    w[..., v["bg0"] + 1] = bz
+    w[..., v["eb"]] = pb / (gamma - 1.0) + 0.5 * bz * bz
+    omega_ac = math.sqrt(gamma * g * H) / (2.0 * H)
+    if omega is None:
+        omega = omega_ac
+    up = [A, omega, z0, dz0, 0.0, drv_w]
+    prm = make_params(gamma=gamma, nu=nu, grav=[-g, 0.0, 0.0], courantpar=courantpar, dtpar=dtpar,
+                      typeadvance=typeadvance, user=USR_TUBE, userpar=up)
+    nw = v["nw"]
+    types = [["cont"] * nw, ["cont"] * nw, ["periodic"] * nw, ["periodic"] * nw]
+    return Problem(f"tube{n[0]}x{n[1]}", ndim, ndir, tuple(n), prm, x, w, types,
+                   meta=dict(omega_ac=omega_ac, A=A, omega=omega))
+
+
+__all__ = ["Problem", "brio_wu", "stratified", "random_problem", "orszag_tang", "flux_tube", "var_index",
            "USR_NONE", "USR_TUBE"]
