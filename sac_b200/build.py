@@ -1,7 +1,11 @@
-"""Build libsacgpu.so (sm_100a) in-tree with nvcc.
+"""Build the in-tree sm_100a libraries with nvcc.
 
-Floating-point contraction (FMA) is on; the parity bar against the CPU oracle
-(1e-12 relative L2 in FP64) leaves room for the one-rounding differences it makes.
+libsacgpu.so   the perturbation-MHD path (single grid and batch), csrc/
+libsacfno.so   the Fourier-neural-operator surrogate, csrc/fno/
+
+The solver's host unit and FP64 stage keep every rounding of the reference (no
+FMA contraction, IEEE division and square root); the FP32 stage may contract and
+approximate.  The surrogate computes in BF16 with FP32 accumulation.
 """
 from __future__ import annotations
 
@@ -14,7 +18,22 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libsacgpu.so")
+FNO_OUT = os.path.join(HERE, "libsacfno.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+# library -> (source dir, [(translation unit, flags)], public header)
+LIBS = {
+    OUT: (CSRC, [
+        ("sac_gpu.cu", ["--fmad=false"]),
+        ("stage_f64.cu", ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
+        ("stage_f32.cu", ["--fmad=true", "-prec-div=false", "-ftz=true"]),
+        ("sac_batch.cu", ["--fmad=false"]),
+    ], "sac_gpu.h"),
+    FNO_OUT: (os.path.join(CSRC, "fno"), [
+        ("fno_gemm.cu", []),
+    ], "sac_fno.h"),
+}
+UNITS = LIBS[OUT][1]
 
 
 def nvcc_path():
@@ -24,27 +43,17 @@ def nvcc_path():
     raise RuntimeError("nvcc not found")
 
 
-def sources():
-    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh", ".h"))]
+def _sources(d):
+    return [os.path.join(d, f) for f in sorted(os.listdir(d)) if f.endswith((".cu", ".cuh", ".h"))]
 
 
-def up_to_date():
-    if not os.path.exists(OUT):
+def up_to_date(out=OUT):
+    if not os.path.exists(out):
         return False
-    t = os.path.getmtime(OUT)
-    deps = sources() + [os.path.join(ROOT, "include", "sac_gpu.h"), __file__]
+    src, _, header = LIBS[out]
+    t = os.path.getmtime(out)
+    deps = _sources(src) + [os.path.join(ROOT, "include", header), __file__]
     return all(os.path.getmtime(s) <= t for s in deps)
-
-
-# translation units and their floating-point flags: the host file and the FP64
-# stage keep every rounding of the reference (no FMA contraction, IEEE division);
-# the FP32 stage may contract and approximate.
-UNITS = [
-    ("sac_gpu.cu", ["--fmad=false"]),
-    ("stage_f64.cu", ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
-    ("stage_f32.cu", ["--fmad=true", "-prec-div=false", "-ftz=true"]),
-    ("sac_batch.cu", ["--fmad=false"]),
-]
 
 
 def _run(cmd, verbose):
@@ -57,23 +66,38 @@ def _run(cmd, verbose):
         print(r.stderr, file=sys.stderr)
 
 
-def build(force=False, verbose=False, extra=()):
-    if not force and up_to_date():
-        return OUT
-    objdir = os.path.join(HERE, "_build")
+def _build_lib(out, force=False, verbose=False, extra=()):
+    if not force and up_to_date(out):
+        return out
+    src, units, _ = LIBS[out]
+    objdir = os.path.join(HERE, "_build", os.path.basename(out).replace(".so", ""))
     os.makedirs(objdir, exist_ok=True)
     objs = []
-    for src, flags in UNITS:
-        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+    for unit, flags in units:
+        obj = os.path.join(objdir, unit.replace(".cu", ".o"))
         _run([nvcc_path(), "-O3", "-std=c++17", *ARCH, "-lineinfo", *flags, "-Xcompiler", "-fPIC",
-              "-I", os.path.join(ROOT, "include"), "-c", "-o", obj, os.path.join(CSRC, src), *extra], verbose)
+              "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-c", "-o", obj, os.path.join(src, unit), *extra],
+             verbose)
         objs.append(obj)
-    _run([nvcc_path(), *ARCH, "-shared", "-o", OUT + ".tmp", *objs], verbose)
-    os.replace(OUT + ".tmp", OUT)
-    return OUT
+    _run([nvcc_path(), *ARCH, "-shared", "-o", out + ".tmp", *objs], verbose)
+    os.replace(out + ".tmp", out)
+    return out
+
+
+def build(force=False, verbose=False, extra=()):
+    """libsacgpu.so (the solver); returns its path."""
+    return _build_lib(OUT, force, verbose, extra)
+
+
+def build_fno(force=False, verbose=False, extra=()):
+    """libsacfno.so (the surrogate); returns its path."""
+    return _build_lib(FNO_OUT, force, verbose, extra)
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True,
-          extra=["-Xptxas", "-v"] if "--ptxas" in sys.argv else [])
-    print(OUT)
+    ex = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else []
+    f = "--force" in sys.argv
+    if "--fno" not in sys.argv or "--all" in sys.argv:
+        print(build(force=f, verbose=True, extra=ex))
+    if "--fno" in sys.argv or "--all" in sys.argv:
+        print(build_fno(force=f, verbose=True, extra=ex))

@@ -1,0 +1,114 @@
+"""The tcgen05 BF16 GEMM of libsacfno.so against a float64 product of the same
+BF16 inputs (FP32 accumulation: relative error a few 1e-6 of sum |a||b|)."""
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from sac_b200 import build, fno_abi  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib():
+    build.build_fno()
+    fno_abi.load()
+
+
+def _bf(shape, seed):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    return torch.randn(*shape, generator=g).to(torch.bfloat16).cuda()
+
+
+def _close(got, ref, scale):
+    err = (got.double() - ref).abs().max().item()
+    assert err <= 2e-5 * scale.max().item() + 1e-6, err
+
+
+def _ref(a, b):  # a: M x K, b: N x K
+    return a.double() @ b.double().T
+
+
+def _scale(a, b):
+    return a.double().abs() @ b.double().abs().T
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 16, 64), (256, 32, 128), (200, 48, 72), (384, 96, 256),
+                                   (130, 128, 40), (512, 256, 96), (64, 6 + 10, 16)])
+def test_k_major(M, N, K):
+    a, b = _bf((M, K), 1), _bf((N, K), 2)
+    c = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), c.data_ptr())
+    torch.cuda.synchronize()
+    _close(c, _ref(a, b), _scale(a, b))
+
+
+@pytest.mark.parametrize("amn,bmn", [(True, False), (False, True), (True, True)])
+def test_mn_major_operands(amn, bmn):
+    M, N, K = 256, 96, 136
+    a, b = _bf((M, K), 3), _bf((N, K), 4)
+    at, bt = a.T.contiguous(), b.T.contiguous()  # K x M, K x N storage
+    c = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    kw = {}
+    if amn:
+        kw.update(a_mn_major=True, a_m0=1, a_k=M)
+    if bmn:
+        kw.update(b_mn_major=True, b_n=1, b_k=N)
+    fno_abi.gemm(M, N, K, (at if amn else a).data_ptr(), (bt if bmn else b).data_ptr(), c.data_ptr(), **kw)
+    torch.cuda.synchronize()
+    _close(c, _ref(a, b), _scale(a, b))
+
+
+def test_split_rows_batches_and_transposed_store():
+    # A rows m = (g, s): A[g][k][s] (MN-major per group), C stored as C[g][n][s]
+    G, S, K, N, nb = 3, 64, 32, 48, 2
+    a = _bf((nb, G, K, S), 5)
+    b = _bf((nb, N, K), 6)
+    c = torch.zeros(nb, G, N, S, dtype=torch.float32, device="cuda")
+    fno_abi.gemm(G * S, N, K, a.data_ptr(), b.data_ptr(), c.data_ptr(), batch=nb,
+                 a_mn_major=True, a_m0=1, a_m1=K * S, a_k=S, a_b=G * K * S, a_msplit=S,
+                 b_n=K, b_b=N * K, c_m0=1, c_m1=N * S, c_n=S, c_b=G * N * S, c_msplit=S)
+    torch.cuda.synchronize()
+    for z in range(nb):
+        A = a[z].permute(0, 2, 1).reshape(G * S, K)
+        ref = _ref(A, b[z]).reshape(G, S, N).permute(0, 2, 1)
+        _close(c[z], ref, _scale(A, b[z]).reshape(G, S, N).permute(0, 2, 1))
+
+
+def test_epilogue_bias_add_gelu_and_grad():
+    M, N, K = 256, 32, 64
+    a, b = _bf((M, K), 7), _bf((N, K), 8)
+    bias = torch.randn(N, device="cuda")
+    add = torch.randn(M, N, device="cuda")
+    out = torch.zeros(M, N, dtype=torch.bfloat16, device="cuda")
+    pre = torch.zeros(M, N, dtype=torch.bfloat16, device="cuda")
+    fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), out.data_ptr(), c_bf16=True, bias_n=bias.data_ptr(),
+                 add=add.data_ptr(), act=1, pre=pre.data_ptr())
+    torch.cuda.synchronize()
+    z = _ref(a, b) + bias.double() + add.double()
+    torch.testing.assert_close(pre.double(), z, rtol=1e-2, atol=1e-2)
+    ref = torch.nn.functional.gelu(z)
+    torch.testing.assert_close(out.double(), ref, rtol=1e-2, atol=1e-2)
+    g = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), g.data_ptr(), act=2, pre=pre.data_ptr())
+    torch.cuda.synchronize()
+    x = pre.double().requires_grad_(True)
+    torch.nn.functional.gelu(x).sum().backward()
+    torch.testing.assert_close(g.double(), _ref(a, b) * x.grad, rtol=1e-4, atol=1e-3)
+
+
+def test_split_k_atomic_and_accumulate():
+    M, N, K = 128, 32, 4096
+    a, b = _bf((M, K), 9), _bf((N, K), 10)
+    c = torch.ones(M, N, dtype=torch.float32, device="cuda")
+    fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), c.data_ptr(), ksplit=16, c_mode=2)
+    fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), c.data_ptr(), c_mode=1, alpha=-0.5)
+    torch.cuda.synchronize()
+    _close(c, 1.0 + 0.5 * _ref(a, b), _scale(a, b))
+
+
+def test_bad_arguments_are_refused():
+    a = _bf((128, 12), 11)
+    c = torch.zeros(128, 16, device="cuda")
+    with pytest.raises(fno_abi.FnoError):
+        fno_abi.gemm(128, 16, 12, a.data_ptr(), a.data_ptr(), c.data_ptr())  # K % 8
