@@ -47,6 +47,61 @@ typedef struct sac_fno_gemm_desc {
 int sac_fno_gemm(const sac_fno_gemm_desc* d, void* cuda_stream);
 const char* sac_fno_last_error(void);
 
+/* ---- the network ----
+ * FNO on an S x F grid: lift cin -> width (1x1), `layers` Fourier layers
+ * z = W v + b + irfft2(R . rfft2(v)[24 x 24 corner modes]), GELU between layers,
+ * projection width -> hidden (GELU) -> cout.  BF16 weights and activations,
+ * FP32 accumulation and FP32 master weights.  Tensors are channel-first per
+ * sample: x[b][c][s][f], f fastest. */
+typedef struct sac_fno_config {
+  int S, F;              /* grid (multiples of 8, at least 50) */
+  int width, layers;     /* 32, 4 */
+  int modes1, modes2;    /* 24, 24 (built in) */
+  int hidden;            /* projection width, 128 */
+  int cin, cout;         /* input channels (multiple of 16), outputs (<= 16) */
+  int max_batch;         /* activations are held for this many samples (<= 64) */
+  int device;
+} sac_fno_config;
+typedef struct sac_fno sac_fno;
+
+void sac_fno_default_config(sac_fno_config* c);
+int sac_fno_create(const sac_fno_config* c, sac_fno** out);
+void sac_fno_destroy(sac_fno* n);
+const char* sac_fno_error(const sac_fno* n);
+void* sac_fno_stream(const sac_fno* n);   /* every call below is enqueued here */
+long sac_fno_num_params(const sac_fno* n);
+/* out[2*(6 + 4*layers)]: offset, count of each parameter group in the flat FP32
+ * vector: P, Pb, then per
+ * layer W, Wb, R.re, R.im (R[kx][ky][i][o], kx: 24 low then 24 high), then Q1, Q1b,
+ * Q2, Q2b (Q2 padded to cout rounded up to 8 rows) */
+int sac_fno_param_layout(const sac_fno* n, long* out);
+int sac_fno_init(sac_fno* n, unsigned long long seed);
+int sac_fno_set_params(sac_fno* n, const float* host);   /* synchronous */
+int sac_fno_get_params(sac_fno* n, float* host);         /* synchronous */
+int sac_fno_get_grads(sac_fno* n, float* host);          /* synchronous */
+int sac_fno_zero_grad(sac_fno* n);
+/* x: [B][cin][S][F] bf16, kept unchanged by the caller until sac_fno_backward;
+ * y: [B][cout][S][F] float */
+int sac_fno_forward(sac_fno* n, const void* x, float* y, int B);
+/* dy: [B][cout8][S][F] bf16, cout8 = cout rounded up to 8 (extra channels zero);
+ * accumulates the parameter gradients of the last forward pass */
+int sac_fno_backward(sac_fno* n, const void* dy);
+/* loss += mean over the cout channels of (y - target)^2 (device float);
+ * dy = its gradient (bf16, cout8 channels); target bf16 [B][cout][S][F] */
+int sac_fno_mse(sac_fno* n, const float* y, const void* target, void* dy, float* loss, int B);
+/* Adam with bias correction and decoupled weight decay; step counts from 1;
+ * clip > 0 rescales the gradient to that global L2 norm (synchronises) */
+int sac_fno_adam(sac_fno* n, float lr, float b1, float b2, float eps, float wd, int step, float clip);
+/* x[b][c] = state[b][c] * scale[b*nst + c] for c < nst (state float or bf16,
+ * [B][nst][S][F]); then nfeat constant planes feat[b*nfeat + k]; then the
+ * coordinates s/S - 1/2 and f/F; the remaining channels zero */
+int sac_fno_features(sac_fno* n, const void* state, int state_bf16, const float* scale, const float* feat,
+                     int nfeat, void* x, int B, int nst);
+/* state[b][c] += scale[b*nst + c] * y[b][c]  (float, [B][nst][S][F]) */
+int sac_fno_apply(sac_fno* n, float* state, const float* y, const float* scale, int B, int nst);
+/* synchronises; 7 when a tensor-core wait timed out since the last reset */
+int sac_fno_check(sac_fno* n, int reset);
+
 #ifdef __cplusplus
 }
 #endif

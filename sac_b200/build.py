@@ -31,6 +31,7 @@ LIBS = {
     ], "sac_gpu.h"),
     FNO_OUT: (os.path.join(CSRC, "fno"), [
         ("fno_gemm.cu", []),
+        ("fno_net.cu", []),
     ], "sac_fno.h"),
 }
 UNITS = LIBS[OUT][1]

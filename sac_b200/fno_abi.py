@@ -76,3 +76,137 @@ def gemm(M, N, K, a, b, c, *, batch=1, ksplit=1, a_m0=None, a_m1=0, a_k=1, a_b=0
     d.c_bf16, d.c_mode, d.alpha = int(bool(c_bf16)), c_mode, alpha
     d.bias_n, d.add, d.act, d.pre, d.err = bias_n or None, add or None, act, pre or None, err or None
     check(lib.sac_fno_gemm(ctypes.byref(d), VP(stream) if stream else None), lib)
+
+
+class FnoConfig(ctypes.Structure):
+    _fields_ = [("S", ctypes.c_int), ("F", ctypes.c_int), ("width", ctypes.c_int), ("layers", ctypes.c_int),
+                ("modes1", ctypes.c_int), ("modes2", ctypes.c_int), ("hidden", ctypes.c_int),
+                ("cin", ctypes.c_int), ("cout", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
+def _bind_net(lib):
+    if getattr(lib, "_net_bound", False):
+        return lib
+    lib.sac_fno_default_config.argtypes = [ctypes.POINTER(FnoConfig)]
+    lib.sac_fno_default_config.restype = None
+    lib.sac_fno_create.argtypes = [ctypes.POINTER(FnoConfig), ctypes.POINTER(VP)]
+    lib.sac_fno_destroy.argtypes = [VP]
+    lib.sac_fno_destroy.restype = None
+    lib.sac_fno_error.argtypes = [VP]
+    lib.sac_fno_error.restype = ctypes.c_char_p
+    lib.sac_fno_stream.argtypes = [VP]
+    lib.sac_fno_stream.restype = VP
+    lib.sac_fno_num_params.argtypes = [VP]
+    lib.sac_fno_num_params.restype = ctypes.c_long
+    lib.sac_fno_param_layout.argtypes = [VP, ctypes.POINTER(ctypes.c_long)]
+    lib.sac_fno_init.argtypes = [VP, ctypes.c_ulonglong]
+    lib.sac_fno_set_params.argtypes = [VP, FP]
+    lib.sac_fno_get_params.argtypes = [VP, FP]
+    lib.sac_fno_get_grads.argtypes = [VP, FP]
+    lib.sac_fno_zero_grad.argtypes = [VP]
+    lib.sac_fno_forward.argtypes = [VP, VP, VP, ctypes.c_int]
+    lib.sac_fno_backward.argtypes = [VP, VP]
+    lib.sac_fno_mse.argtypes = [VP, VP, VP, VP, VP, ctypes.c_int]
+    lib.sac_fno_adam.argtypes = [VP, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                 ctypes.c_float, ctypes.c_int, ctypes.c_float]
+    lib.sac_fno_features.argtypes = [VP, VP, ctypes.c_int, VP, VP, ctypes.c_int, VP, ctypes.c_int, ctypes.c_int]
+    lib.sac_fno_apply.argtypes = [VP, VP, VP, VP, ctypes.c_int, ctypes.c_int]
+    lib.sac_fno_check.argtypes = [VP, ctypes.c_int]
+    for f in ("sac_fno_create", "sac_fno_param_layout", "sac_fno_init", "sac_fno_set_params", "sac_fno_get_params",
+              "sac_fno_get_grads", "sac_fno_zero_grad", "sac_fno_forward", "sac_fno_backward", "sac_fno_mse",
+              "sac_fno_adam", "sac_fno_features", "sac_fno_apply", "sac_fno_check"):
+        getattr(lib, f).restype = ctypes.c_int
+    lib._net_bound = True
+    return lib
+
+
+class Net:
+    """The FNO of libsacfno.so.  Tensors are passed as integer device pointers
+    (e.g. torch's data_ptr()); every call is enqueued on the network's stream."""
+
+    def __init__(self, S=256, F=256, width=32, layers=4, hidden=128, cin=16, cout=6, max_batch=16, device=0,
+                 seed=0):
+        self.lib = _bind_net(load())
+        c = FnoConfig()
+        self.lib.sac_fno_default_config(ctypes.byref(c))
+        c.S, c.F, c.width, c.layers, c.hidden = S, F, width, layers, hidden
+        c.cin, c.cout, c.max_batch, c.device = cin, cout, max_batch, device
+        self.cfg = c
+        self.h = VP()
+        rc = self.lib.sac_fno_create(ctypes.byref(c), ctypes.byref(self.h))
+        if rc != 0:
+            raise FnoError(f"sac_fno_create: {self.lib.sac_fno_last_error().decode()}")
+        self.cpad = (cout + 7) // 8 * 8
+        self.nparam = int(self.lib.sac_fno_num_params(self.h))
+        if seed is not None:
+            self._c(self.lib.sac_fno_init(self.h, seed))
+
+    def _c(self, rc):
+        if rc != 0:
+            raise FnoError(f"status {rc}: {self.lib.sac_fno_error(self.h).decode(errors='replace')}")
+
+    @property
+    def stream(self):
+        return self.lib.sac_fno_stream(self.h)
+
+    def layout(self):
+        import numpy as np
+        n = 2 * (6 + 4 * self.cfg.layers)
+        out = np.zeros(n, dtype=np.int64)
+        self._c(self.lib.sac_fno_param_layout(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_long))))
+        return out.reshape(-1, 2)
+
+    def get_params(self):
+        import numpy as np
+        a = np.zeros(self.nparam, dtype=np.float32)
+        self._c(self.lib.sac_fno_get_params(self.h, a.ctypes.data_as(FP)))
+        return a
+
+    def set_params(self, a):
+        import numpy as np
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        assert a.size == self.nparam
+        self._c(self.lib.sac_fno_set_params(self.h, a.ctypes.data_as(FP)))
+
+    def get_grads(self):
+        import numpy as np
+        a = np.zeros(self.nparam, dtype=np.float32)
+        self._c(self.lib.sac_fno_get_grads(self.h, a.ctypes.data_as(FP)))
+        return a
+
+    def zero_grad(self):
+        self._c(self.lib.sac_fno_zero_grad(self.h))
+
+    def forward(self, x_ptr, y_ptr, B):
+        self._c(self.lib.sac_fno_forward(self.h, VP(x_ptr), VP(y_ptr), B))
+
+    def backward(self, dy_ptr):
+        self._c(self.lib.sac_fno_backward(self.h, VP(dy_ptr)))
+
+    def mse(self, y_ptr, t_ptr, dy_ptr, loss_ptr, B):
+        self._c(self.lib.sac_fno_mse(self.h, VP(y_ptr), VP(t_ptr), VP(dy_ptr), VP(loss_ptr), B))
+
+    def adam(self, lr, step, b1=0.9, b2=0.999, eps=1e-8, wd=1e-4, clip=0.0):
+        self._c(self.lib.sac_fno_adam(self.h, lr, b1, b2, eps, wd, step, clip))
+
+    def features(self, state_ptr, state_bf16, scale_ptr, feat_ptr, nfeat, x_ptr, B, nst):
+        self._c(self.lib.sac_fno_features(self.h, VP(state_ptr), int(bool(state_bf16)), VP(scale_ptr or None),
+                                          VP(feat_ptr or None), nfeat, VP(x_ptr), B, nst))
+
+    def apply(self, state_ptr, y_ptr, scale_ptr, B, nst):
+        self._c(self.lib.sac_fno_apply(self.h, VP(state_ptr), VP(y_ptr), VP(scale_ptr), B, nst))
+
+    def check(self, reset=True):
+        self._c(self.lib.sac_fno_check(self.h, int(bool(reset))))
+
+    def close(self):
+        if self.h:
+            self.lib.sac_fno_destroy(self.h)
+            self.h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
