@@ -224,6 +224,10 @@ sac_status sac_batch_tune(sac_batch* b, int* tile_xy, double* ms);
 sac_status sac_batch_set_driver(sac_batch* b, const double* A, const double* omega);
 /* per-instance time and step counter (either may be NULL) */
 sac_status sac_batch_set_time(sac_batch* b, const double* t, const int* it);
+/* per-instance end time, the reference's tmaxexact (src/vac.t:82): dt is clipped
+ * to tmax - t + smalldouble, and an instance that reached tmax takes dt = 0
+ * steps that leave its state and step counter untouched.  tmax <= 0: no limit. */
+sac_status sac_batch_set_tmax(sac_batch* b, const double* tmax);
 /* mesh cells over all instances (ghosts excluded) */
 long sac_batch_mesh_cells(const sac_batch* b);
 /* Packed mesh copies between the resident state and a DEVICE buffer, enqueued on

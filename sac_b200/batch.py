@@ -42,6 +42,7 @@ def _bind(lib):
     f("tune").argtypes = [P, IP, DP]
     f("set_driver").argtypes = [P, DP, DP]
     f("set_time").argtypes = [P, DP, IP]
+    f("set_tmax").argtypes = [P, DP]
     f("mesh_cells").argtypes = [P]
     f("mesh_cells").restype = ctypes.c_long
     f("gather").argtypes = [P, ctypes.c_void_p, ctypes.c_int]
@@ -51,7 +52,7 @@ def _bind(lib):
     f("destroy").argtypes = [P]
     f("destroy").restype = None
     for n in ("create", "set_grid", "set_boundaries", "upload", "download", "upload_range", "download_range",
-              "getboundary", "advance", "state", "synchronize", "tune", "set_driver", "set_time", "gather",
+              "getboundary", "advance", "state", "synchronize", "tune", "set_driver", "set_time", "set_tmax", "gather",
               "scatter"):
         f(n).restype = ctypes.c_int
     lib._sac_batch_bound = True
@@ -146,6 +147,26 @@ class Batch:
         ia = None if it is None else np.ascontiguousarray(it, dtype=np.int32)
         self._call("set_time", _dp(ta) if ta is not None else None,
                    ia.ctypes.data_as(IP) if ia is not None else None)
+
+    def set_tmax(self, tmax):
+        """Per-instance end time (tmaxexact); <= 0 removes the limit."""
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(tmax, dtype=np.float64), (self.ninst,)))
+        self._call("set_tmax", _dp(a))
+
+    def advance_to(self, tmax, chunk=8, max_steps=100000):
+        """Advance every instance with its own dt until it lands on tmax; returns
+        the largest step count an instance took."""
+        self.set_tmax(tmax)
+        t0, _, it0 = self.state()
+        target = np.broadcast_to(np.asarray(tmax, dtype=np.float64), (self.ninst,))
+        done = 0
+        while done < max_steps:
+            self.advance(chunk)
+            done += chunk
+            t, _, it = self.state()
+            if np.all(t >= target):
+                return int((it - it0).max())
+        raise RuntimeError("advance_to: tmax not reached")
 
     PACK = {"f32": 0, "bf16": 1, "f64": 2}
 

@@ -181,12 +181,14 @@ __global__ void kb_dt(InstDyn* dyn, int n, int ndim, double courantpar, double d
     if (grav) dt = fmin(dt, D.dtgrav);
     if (cantgrow && D.it > 0) dt = fmin(dt, D.dt);  // dtcantgrow, src/vac.t:68
   }
+  if (D.tmax > 0.0) dt = D.t >= D.tmax ? 0.0 : fmin(dt, D.tmax - D.t + kSmallD);  // tmaxexact, src/vac.t:82
   D.dt = dt;
 }
 
 __global__ void kb_time(InstDyn* dyn, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (dyn[i].dt == 0.0) return;  // finished at tmax
   dyn[i].t += dyn[i].dt;
   dyn[i].it += 1;
 }
@@ -237,12 +239,12 @@ BcArgs bc_proto(sac_batch* b, void* A) {
 }
 
 template <typename S>
-void launch_bound_b(sac_batch* b, BcArgs a, int nvar, const GhostChunk* chunks, int n) {
+void launch_bound_b(sac_batch* b, BcArgs a, int nvar, const GhostChunk* chunks, int n, const InstDyn* dyn) {
   if (!n) return;
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->dev);
   const unsigned grid = (unsigned)std::min<long>(n, (long)nsm * 8);
-  kb_bound<S><<<grid, 256, 0, b->stream>>>(a, b->d_inst, chunks, n, nvar);
+  kb_bound<S><<<grid, 256, 0, b->stream>>>(a, b->d_inst, chunks, n, nvar, dyn);
 }
 
 Stage2Args stage_base(sac_batch* b) {
@@ -329,7 +331,7 @@ void enqueue_step(sac_batch* b) {
         ba.mode = 2;
         ba.aux1 = w1;
       }
-      launch_bound_b<S>(b, ba, b->np, gr.d_gh, gr.n_gh);
+      launch_bound_b<S>(b, ba, b->np, gr.d_gh, gr.n_gh, b->d_dyn);
     }
   }
   kb_time<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst);
@@ -525,7 +527,10 @@ sac_status sac_batch_set_grid(sac_batch* b, const double* x) {
   free_all(b);
   b->grid_set = b->bc_set = b->state_set = b->bc_init = false;
   const size_t es = b->es;
-  for (auto& p : b->P) BK(cudaMalloc(&p, es * b->np * b->totP));
+  for (auto& p : b->P) {
+    BK(cudaMalloc(&p, es * b->np * b->totP));
+    BK(cudaMemset(p, 0, es * b->np * b->totP));  // scratch stages of finished instances stay finite
+  }
   BK(cudaMalloc(&b->BG, sizeof(double) * (b->nw - b->np) * b->totP));
   BK(cudaMalloc(&b->dx, sizeof(double) * ndim * b->totX));
   BK(cudaMemcpy(b->dx, hdx.data(), sizeof(double) * hdx.size(), cudaMemcpyHostToDevice));
@@ -695,9 +700,9 @@ sac_status sac_batch_getboundary(sac_batch* b) {
   BcArgs a = bc_proto(b, b->P[0]);
   a.init = 1;
   if (b->prec == SAC_PREC_FP32)
-    launch_bound_b<float>(b, a, b->nw, b->d_gh_all, b->n_gh_all);
+    launch_bound_b<float>(b, a, b->nw, b->d_gh_all, b->n_gh_all, nullptr);
   else
-    launch_bound_b<double>(b, a, b->nw, b->d_gh_all, b->n_gh_all);
+    launch_bound_b<double>(b, a, b->nw, b->d_gh_all, b->n_gh_all, nullptr);
   BK(cudaGetLastError());
   BK(cudaStreamSynchronize(b->stream));
   b->bc_init = true;
@@ -754,6 +759,14 @@ sac_status sac_batch_tune(sac_batch* b, int* tile_out, double* ms_out) {
   BK(cudaSetDevice(b->dev));
   const dim3 cands[] = {dim3(32, 4, 1), dim3(32, 8, 1), dim3(64, 4, 1), dim3(16, 16, 1), dim3(128, 2, 1),
                         dim3(256, 1, 1)};
+  // the update pass skips instances with dt = 0 (finished, or before the first
+  // step): time it with a tiny nonzero dt and restore the table afterwards
+  std::vector<InstDyn> saved(b->ninst), tmp;
+  BK(cudaMemcpy(saved.data(), b->d_dyn, sizeof(InstDyn) * b->ninst, cudaMemcpyDeviceToHost));
+  tmp = saved;
+  for (auto& d : tmp)
+    if (d.dt == 0.0) d.dt = 1e-300;
+  BK(cudaMemcpy(b->d_dyn, tmp.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice));
   cudaEvent_t e0, e1;
   BK(cudaEventCreate(&e0));
   BK(cudaEventCreate(&e1));
@@ -797,12 +810,8 @@ sac_status sac_batch_tune(sac_batch* b, int* tile_out, double* ms_out) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  // the timing runs wrote w1 and max nu; both are rewritten before use, but the
-  // running max nu feeds getdt_visc, so clear it
-  std::vector<InstDyn> dyn(b->ninst);
-  BK(cudaMemcpy(dyn.data(), b->d_dyn, sizeof(InstDyn) * b->ninst, cudaMemcpyDeviceToHost));
-  for (auto& d : dyn) d.maxnu = 0ull;
-  BK(cudaMemcpy(b->d_dyn, dyn.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice));
+  // the timing runs wrote w1 (scratch) and the running max nu: restore the table
+  BK(cudaMemcpy(b->d_dyn, saved.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice));
   b->upd_blk = bestb;
   sac_status st = build_lists(b);
   if (st != SAC_OK) return st;
@@ -847,6 +856,22 @@ sac_status sac_batch_set_time(sac_batch* b, const double* t, const int* it) {
     if (t) dyn[i].t = t[i];
     if (it) dyn[i].it = it[i];
   }
+  BK(cudaMemcpyAsync(b->d_dyn, dyn.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  return SAC_OK;
+}
+
+// per-instance end time (tmaxexact): dt is clipped so that the instance lands on
+// tmax exactly, after which it takes dt = 0 steps that leave it untouched; a
+// value <= 0 removes the limit
+sac_status sac_batch_set_tmax(sac_batch* b, const double* tmax) {
+  if (!b || !tmax) return SAC_ERR_ARG;
+  if (!b->grid_set) return bfail(b, SAC_ERR_STATE, "sac_batch_set_grid first");
+  BK(cudaSetDevice(b->dev));
+  std::vector<InstDyn> dyn(b->ninst);
+  BK(cudaMemcpyAsync(dyn.data(), b->d_dyn, sizeof(InstDyn) * b->ninst, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < b->ninst; ++i) dyn[i].tmax = tmax[i];
   BK(cudaMemcpyAsync(b->d_dyn, dyn.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice, b->stream));
   BK(cudaStreamSynchronize(b->stream));
   return SAC_OK;

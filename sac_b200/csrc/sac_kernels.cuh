@@ -53,6 +53,8 @@ struct InstDyn {
   double mindx2[3];  // min over the mesh of dx^2 per dimension (getdt_visc)
   double dtgrav;     // getdt_grav, fixed at the first step
   double drvA, omega;  // velocity driver amplitude and angular frequency (tdep = sin(omega t))
+  double tmax;         // > 0: the run ends at exactly this time (tmaxexact); the instance then
+                       // takes dt = 0 steps that leave its state untouched
   unsigned long long ctot[3], maxnu, courant;  // bits of non-negative maxima
   int it, bad;       // step counter; set when a reduction met NaN/Inf
 };
@@ -380,9 +382,11 @@ __global__ void k_bound(BcArgs a, long nslab0, long nslab1, long nslab2, int nva
 // batched: persistent CTAs of 256 threads walk the ghost chunks of all instances
 template <typename S>
 __global__ void __launch_bounds__(256) kb_bound(BcArgs proto, const InstInfo* __restrict__ inst,
-                                                const GhostChunk* __restrict__ chunks, int nchunks, int nvar) {
+                                                const GhostChunk* __restrict__ chunks, int nchunks, int nvar,
+                                                const InstDyn* __restrict__ dyn) {
   for (int t = blockIdx.x; t < nchunks; t += gridDim.x) {
     const GhostChunk ch = chunks[t];
+    if (dyn && dyn[ch.inst].dt == 0.0) continue;  // a finished instance keeps its state
     BcArgs a = proto;
     a.g = inst[ch.inst].g;
     a.oA = inst[ch.inst].o.P;

@@ -566,7 +566,7 @@ __global__ void __launch_bounds__(256, 2) kb_update(const BatchStageArgs b) {
     const Geom& g = I.g;
     int p[3];
     double numax = 0.0;
-    if (tile_cell(tl, g, g.lo, g.hi, p)) {
+    if (b.dyn[tl.inst].dt != 0.0 && tile_cell(tl, g, g.lo, g.hi, p)) {
       // the RK4 stage steps of advect, src/vac.t:442-452; every stage sees the
       // driver at the step's start time t (advect1 is called with t)
       const InstDyn& D = b.dyn[tl.inst];
