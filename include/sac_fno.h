@@ -17,9 +17,9 @@ extern "C" {
  *   C(m,n) = epilogue(alpha * sum_k A(m,k) * B(n,k))
  * Row index splits: addr(m, x) = base + batch*s_b + (m / msplit)*s_m1 + (m % msplit)*s_m0 + x*s_x.
  * A is K-major (a_k == 1) or MN-major (a_m0 == 1, a_mn_major = 1); B likewise with
- * b_k / b_n.  Requirements: K % 8 == 0; 16-byte aligned operands and 8-element
- * aligned strides across the contiguous chunks; M (resp. N) % 8 == 0 and
- * msplit % 8 == 0 for an MN-major A (resp. B).
+ * b_k / b_n and its own row split (b_nsplit, b_n1).  Requirements: K % 8 == 0;
+ * 16-byte aligned operands and 8-element aligned strides across the contiguous
+ * chunks; M (resp. N) % 8 == 0 and the split % 8 == 0 for an MN-major A (resp. B).
  * Epilogue: + bias_n[n], + add(m,n) (float, C addressing), then act: 1 = GELU
  * (the pre-activation is stored to pre when given), 2 = multiply by GELU'(pre).
  * c_mode: 0 store, 1 accumulate, 2 atomic add (float C; with ksplit > 1). */
@@ -40,6 +40,8 @@ typedef struct sac_fno_gemm_desc {
   int act;
   void* pre;
   int* err;
+  long b_n1;    /* B rows split like A's: (n / b_nsplit)*b_n1 + (n % b_nsplit)*b_n */
+  int b_nsplit;
 } sac_fno_gemm_desc;
 
 /* 0 on success; 1 on an argument that breaks the requirements (message in

@@ -55,26 +55,33 @@ int gemm(const GemmDesc& d, cudaStream_t st) {
     if (d.a_k != 1) return bad("K-major A needs a_k == 1");
     if (d.a_m0 % 8 || d.a_m1 % 8 || d.a_b % 8) return bad("K-major A alignment");
   }
+  if (d.b_nsplit <= 0) return bad("b_nsplit must be positive");
   if (d.b_mn_major) {
     if (d.b_n != 1) return bad("MN-major B needs b_n == 1");
-    if (d.N % 8 || d.b_k % 8 || d.b_b % 8) return bad("MN-major B alignment");
+    if (d.N % 8 || d.b_nsplit % 8 || d.b_k % 8 || d.b_n1 % 8 || d.b_b % 8) return bad("MN-major B alignment");
   } else {
     if (d.b_k != 1) return bad("K-major B needs b_k == 1");
-    if (d.b_n % 8 || d.b_b % 8) return bad("K-major B alignment");
+    if (d.b_n % 8 || d.b_n1 % 8 || d.b_b % 8) return bad("K-major B alignment");
   }
   if (d.c_mode == C_ATOMIC && d.c_bf16) return bad("atomic accumulation needs a float C");
   if (d.ksplit > 1 && d.c_mode != C_ATOMIC) return bad("ksplit > 1 needs c_mode atomic");
   if (d.act == ACT_GELU_GRAD && !d.pre) return bad("GELU' needs the pre-activation");
   if (d.c_mode == C_ATOMIC && (d.act != ACT_NONE || d.bias_n || d.add))
     return bad("atomic accumulation takes no bias, add or activation");
+  // widest tile that covers N, narrowed while the grid would leave SMs idle
+  int bn = d.N <= 16 ? 16 : d.N <= 32 ? 32 : d.N <= 48 ? 48 : d.N <= 64 ? 64 : d.N <= 96 ? 96 : d.N <= 128 ? 128 : 256;
+  const long mt = (d.M + kBM - 1) / kBM * (long)d.batch * d.ksplit;
+  while (bn > 64 && bn % 64 == 0 && mt * ((d.N + bn - 1) / bn) < 2L * 148) bn /= 2;
   cudaError_t e;
-  if (d.N <= 16) e = launch_bn<16>(d, st);
-  else if (d.N <= 32) e = launch_bn<32>(d, st);
-  else if (d.N <= 48) e = launch_bn<48>(d, st);
-  else if (d.N <= 64) e = launch_bn<64>(d, st);
-  else if (d.N <= 96) e = launch_bn<96>(d, st);
-  else if (d.N <= 128) e = launch_bn<128>(d, st);
-  else e = launch_bn<256>(d, st);
+  switch (bn) {
+    case 16: e = launch_bn<16>(d, st); break;
+    case 32: e = launch_bn<32>(d, st); break;
+    case 48: e = launch_bn<48>(d, st); break;
+    case 64: e = launch_bn<64>(d, st); break;
+    case 96: e = launch_bn<96>(d, st); break;
+    case 128: e = launch_bn<128>(d, st); break;
+    default: e = launch_bn<256>(d, st); break;
+  }
   if (e != cudaSuccess) {
     set_error(std::string("sac_fno_gemm: ") + cudaGetErrorString(e));
     return 3;

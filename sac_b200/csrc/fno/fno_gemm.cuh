@@ -52,6 +52,9 @@ struct GemmDesc {
   int act;              // EpiAct
   bf16* pre;            // ACT_GELU: stores the pre-activation; ACT_GELU_GRAD: reads it
   int* err;             // error word (bit 0: an mbarrier wait timed out)
+  // B rows split like A's: n = (n / b_nsplit, n % b_nsplit) -> (n / b_nsplit)*b_n1 + (n % b_nsplit)*b_n
+  long b_n1;
+  int b_nsplit;
 };
 
 constexpr int kBM = 128, kBK = 64, kThreads = 128;
@@ -210,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmDesc d) {
     uint8_t* sa = smem + s * STAGE;
     uint8_t* sb = sa + A_BYTES;
     load_tile<kBM>(ta, A, d.a_m0, d.a_m1, d.a_msplit, d.a_k, d.a_mn_major, m0, d.M, k0, kend);
-    load_tile<BN>(tb, B, d.b_n, 0, 1 << 30, d.b_k, d.b_mn_major, n0, d.N, k0, kend);
+    load_tile<BN>(tb, B, d.b_n, d.b_n1, d.b_nsplit, d.b_k, d.b_mn_major, n0, d.N, k0, kend);
     if (kt >= 2 && !mbar_wait(&bar[s], ((kt - 2) >> 1) & 1)) ok = false;  // stage s free again
     if (__syncthreads_or(!ok)) {
       ok = false;
@@ -260,32 +263,43 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmDesc d) {
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (m >= d.M) continue;
+      // all loads of the chunk first (independent, so they overlap), then the
+      // arithmetic, then the stores; columns past N are masked, not branched on
+      float x[16], ad[16], pr[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int n = n0 + cc + j;
-        if (n >= d.N) break;
-        float x = nk > 0 ? d.alpha * __uint_as_float(v[j]) : 0.0f;
+        const bool in = n < d.N;
         const long o = crow + (long)n * d.c_n;
-        if (d.bias_n) x += d.bias_n[n];
-        if (d.add) x += d.add[o];
+        x[j] = nk > 0 ? d.alpha * __uint_as_float(v[j]) : 0.0f;
+        ad[j] = (in && d.add) ? __ldg(d.add + o) : 0.0f;
+        pr[j] = (in && d.act == ACT_GELU_GRAD) ? __bfloat162float(d.pre[o]) : 0.0f;
+        if (in && d.bias_n) x[j] += __ldg(d.bias_n + n);
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int n = n0 + cc + j;
+        if (n >= d.N) continue;
+        const long o = crow + (long)n * d.c_n;
+        float y = x[j] + ad[j];
         if (d.act == ACT_GELU) {
-          if (d.pre) d.pre[o] = __float2bfloat16(x);
-          x = gelu_f(x);
+          if (d.pre) d.pre[o] = __float2bfloat16(y);
+          y = gelu_f(y);
         } else if (d.act == ACT_GELU_GRAD) {
-          x *= gelu_grad_f(__bfloat162float(d.pre[o]));
+          y *= gelu_grad_f(pr[j]);
         }
         if (d.c_bf16) {
           bf16* C = (bf16*)d.c;
-          if (d.c_mode == C_ACCUM) x += __bfloat162float(C[o]);
-          C[o] = __float2bfloat16(x);
+          if (d.c_mode == C_ACCUM) y += __bfloat162float(C[o]);
+          C[o] = __float2bfloat16(y);
         } else {
           float* C = (float*)d.c;
           if (d.c_mode == C_ATOMIC)
-            atomicAdd(C + o, x);
+            atomicAdd(C + o, y);
           else if (d.c_mode == C_ACCUM)
-            C[o] += x;
+            C[o] += y;
           else
-            C[o] = x;
+            C[o] = y;
         }
       }
     }

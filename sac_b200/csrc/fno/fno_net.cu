@@ -317,6 +317,7 @@ GemmDesc gd(int M, int N, int K, int batch = 1) {
   d.batch = batch;
   d.ksplit = 1;
   d.a_msplit = 1 << 30;
+  d.b_nsplit = 1 << 30;
   d.c_msplit = 1 << 30;
   d.alpha = 1.f;
   return d;
@@ -377,18 +378,18 @@ int forward(sac_fno* n, const bf16* x, float* y, int B) {
       d.err = n->errw;
       GK(d);
     }
-    // F2: Z[(b,c,j)][r] = sum_s T[(b,c,j)][s] Fx[r][s]
+    // F2: Z[(b,c,j)][r] = sum_s T[(b,c,j)][s] Fx[r][s]  (rows r, so that the store is coalesced)
     {
-      GemmDesc d = gd(B * W * kJ, kR, S);
-      d.a = n->tp;
+      GemmDesc d = gd(kR, B * W * kJ, S);
+      d.a = n->Fx;
       d.a_m0 = S;
       d.a_k = 1;
-      d.b = n->Fx;
+      d.b = n->tp;
       d.b_n = S;
       d.b_k = 1;
       d.c = n->zt[l];
-      d.c_m0 = kR;
-      d.c_n = 1;
+      d.c_m0 = 1;
+      d.c_n = kR;
       d.err = n->errw;
       GK(d);
     }
@@ -417,18 +418,18 @@ int forward(sac_fno* n, const bf16* x, float* y, int B) {
       d.err = n->errw;
       GK(d);
     }
-    // F5: spec[(b,o,s)][f] = sum_j' Y[(b,o,s)][j'] Hy[f][j']
+    // F5: spec[(b,o,s)][f] = sum_j' Y[(b,o,s)][j'] Hy[f][j']  (rows f)
     {
-      GemmDesc d = gd(B * W * S, F, kJ);
-      d.a = n->yb;
+      GemmDesc d = gd(F, B * W * S, kJ);
+      d.a = n->Hy;
       d.a_m0 = kJ;
       d.a_k = 1;
-      d.b = n->Hy;
+      d.b = n->yb;
       d.b_n = kJ;
       d.b_k = 1;
       d.c = n->spec;
-      d.c_m0 = F;
-      d.c_n = 1;
+      d.c_m0 = 1;
+      d.c_n = F;
       d.err = n->errw;
       GK(d);
     }
@@ -578,17 +579,17 @@ int backward(sac_fno* n, const bf16* dy) {
       d.err = n->errw;
       GK(d);
     }
-    {  // B4: dP[(b,o),j'][r] = sum_s dY[(b,o),j'][s] Fx[r][s]
-      GemmDesc d = gd(B * W * kJ, kR, S);
-      d.a = n->dyt;
+    {  // B4: dP[(b,o),j'][r] = sum_s dY[(b,o),j'][s] Fx[r][s]  (rows r)
+      GemmDesc d = gd(kR, B * W * kJ, S);
+      d.a = n->Fx;
       d.a_m0 = S;
       d.a_k = 1;
-      d.b = n->Fx;
+      d.b = n->dyt;
       d.b_n = S;
       d.b_k = 1;
       d.c = n->dpt;
-      d.c_m0 = kR;
-      d.c_n = 1;
+      d.c_m0 = 1;
+      d.c_n = kR;
       d.err = n->errw;
       GK(d);
     }
@@ -598,35 +599,36 @@ int backward(sac_fno* n, const bf16* dy) {
                                                n->dzt, gw + n->sRr[l].off, gw + n->sRi[l].off, B, W, n->m2);
       FK(cudaGetLastError());
     }
-    {  // B2: dT[(b,c),j][s] = sum_r dZ[(b,c),j][r] Fx[r][s]
-      GemmDesc d = gd(B * W * kJ, S, kR);
-      d.a = n->dzt;
+    {  // B2: dT[(b,c),j][s] = sum_r dZ[(b,c),j][r] Fx[r][s]  (rows s)
+      GemmDesc d = gd(S, B * W * kJ, kR);
+      d.a = n->Gx;
       d.a_m0 = kR;
       d.a_k = 1;
-      d.b = n->Gx;
+      d.b = n->dzt;
       d.b_n = kR;
       d.b_k = 1;
       d.c = n->dtp;
-      d.c_m0 = S;
-      d.c_n = 1;
+      d.c_m0 = 1;
+      d.c_n = S;
       d.c_bf16 = 1;
       d.err = n->errw;
       GK(d);
     }
-    {  // B1: dv[(b,c,s)][f] = dvacc + sum_j dT[(b,c)][j][s] Fy[j][f], then GELU' of the layer below
-      GemmDesc d = gd(B * W * S, F, kJ);
-      d.a = n->dtp;
-      d.a_mn_major = 1;
-      d.a_msplit = S;
-      d.a_m0 = 1;
-      d.a_m1 = (long)kJ * S;
-      d.a_k = S;
-      d.b = n->FyT;
-      d.b_n = kJ;
-      d.b_k = 1;
+    {  // B1: dv[(b,c,s)][f] = dvacc + sum_j dT[(b,c)][j][s] Fy[j][f], then GELU' of the layer
+       // below  (rows f; B rows n = (b,c,s) read MN-major from dT[(b,c)][j][s])
+      GemmDesc d = gd(F, B * W * S, kJ);
+      d.a = n->FyT;
+      d.a_m0 = kJ;
+      d.a_k = 1;
+      d.b = n->dtp;
+      d.b_mn_major = 1;
+      d.b_n = 1;
+      d.b_nsplit = S;
+      d.b_n1 = (long)kJ * S;
+      d.b_k = S;
       d.c = n->dz2;
-      d.c_m0 = F;
-      d.c_n = 1;
+      d.c_m0 = 1;
+      d.c_n = F;
       d.c_bf16 = 1;
       d.add = n->dvacc;
       if (l > 0) {

@@ -521,6 +521,7 @@ __global__ void __launch_bounds__(256) kb_face(const BatchStageArgs b, double ga
   __shared__ double sh[32];
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     const Tile tl = b.tiles[t];
+    if (b.dyn[tl.inst].dt == 0.0) continue;  // finished (tmax): nothing to compute
     const InstInfo& I = b.inst[tl.inst];
     const Geom& g = I.g;
     const int lo[3] = {0, 0, 0}, hi[3] = {g.n[0] - 1, g.n[1] - 1, g.n[2] - 1};
@@ -543,6 +544,7 @@ template <int NDIM, int NDIR, typename S>
 __global__ void __launch_bounds__(256) kb_nu(const BatchStageArgs b) {
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     const Tile tl = b.tiles[t];
+    if (b.dyn[tl.inst].dt == 0.0) continue;
     const InstInfo& I = b.inst[tl.inst];
     const Geom& g = I.g;
     int lo[3], hi[3], p[3];
@@ -587,6 +589,8 @@ __global__ void __launch_bounds__(256) kb_courant(const BatchStageArgs b, double
   constexpr int E = NDIR + 1;
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     const Tile tl = b.tiles[t];
+    const InstDyn& Dy = b.dyn[tl.inst];
+    if (Dy.tmax > 0.0 && Dy.t >= Dy.tmax) continue;  // finished: its dt will be 0
     const InstInfo& I = b.inst[tl.inst];
     const Geom& g = I.g;
     int p[3];

@@ -22,7 +22,7 @@ class GemmDesc(ctypes.Structure):
         ("c", VP), ("c_m0", ctypes.c_long), ("c_m1", ctypes.c_long), ("c_n", ctypes.c_long),
         ("c_b", ctypes.c_long), ("c_msplit", ctypes.c_int), ("c_bf16", ctypes.c_int), ("c_mode", ctypes.c_int),
         ("alpha", ctypes.c_float), ("bias_n", VP), ("add", VP), ("act", ctypes.c_int), ("pre", VP),
-        ("err", VP),
+        ("err", VP), ("b_n1", ctypes.c_long), ("b_nsplit", ctypes.c_int),
     ]
 
 
@@ -55,7 +55,8 @@ def check(rc, lib=None):
 
 
 def gemm(M, N, K, a, b, c, *, batch=1, ksplit=1, a_m0=None, a_m1=0, a_k=1, a_b=0, a_msplit=None,
-         a_mn_major=False, b_n=None, b_k=1, b_b=0, b_mn_major=False, c_m0=None, c_m1=0, c_n=1, c_b=0,
+         a_mn_major=False, b_n=None, b_k=1, b_b=0, b_mn_major=False, b_n1=0, b_nsplit=None,
+         c_m0=None, c_m1=0, c_n=1, c_b=0,
          c_msplit=None, c_bf16=False, c_mode=0, alpha=1.0, bias_n=0, add=0, act=0, pre=0, err=0, stream=0):
     """Thin call of sac_fno_gemm with integer device pointers (0 = none)."""
     lib = load()
@@ -69,6 +70,8 @@ def gemm(M, N, K, a, b, c, *, batch=1, ksplit=1, a_m0=None, a_m1=0, a_k=1, a_b=0
     d.b = b
     d.b_n = (K if not b_mn_major else 1) if b_n is None else b_n
     d.b_k, d.b_b, d.b_mn_major = b_k, b_b, int(bool(b_mn_major))
+    d.b_n1 = b_n1
+    d.b_nsplit = (1 << 30) if b_nsplit is None else b_nsplit
     d.c = c
     d.c_m0 = N if c_m0 is None else c_m0
     d.c_m1, d.c_n, d.c_b = c_m1, c_n, c_b

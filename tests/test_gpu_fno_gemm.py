@@ -112,3 +112,17 @@ def test_bad_arguments_are_refused():
     c = torch.zeros(128, 16, device="cuda")
     with pytest.raises(fno_abi.FnoError):
         fno_abi.gemm(128, 16, 12, a.data_ptr(), a.data_ptr(), c.data_ptr())  # K % 8
+
+
+def test_b_rows_split_mn_major():
+    # B(n = (g, s), k) = b[g][k][s] (MN-major within each group), C stored C[g][s][m]
+    G, S, K, M = 3, 64, 48, 256
+    a = _bf((M, K), 12)
+    b = _bf((G, K, S), 13)
+    c = torch.zeros(G, S, M, dtype=torch.float32, device="cuda")
+    fno_abi.gemm(M, G * S, K, a.data_ptr(), b.data_ptr(), c.data_ptr(), b_mn_major=True, b_n=1, b_k=S,
+                 b_n1=K * S, b_nsplit=S, c_m0=1, c_n=M)
+    torch.cuda.synchronize()
+    Bm = b.permute(0, 2, 1).reshape(G * S, K)
+    ref = _ref(a, Bm).T.reshape(G, S, M)
+    _close(c, ref, _scale(a, Bm).T.reshape(G, S, M))
