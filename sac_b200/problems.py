@@ -156,29 +156,54 @@ def stratified(n=(128, 128, 128), height=1.5, H=0.3, B0=0.3, gamma=5.0 / 3.0, am
 def add_modes(w, x, ndim, ndir, amp, nmodes=64, kmax=16, seed=0, rho_scale=None):
     """Seeded random-phase Fourier modes (|k|<=kmax) added to rho', v and b'
     (divergence-free b' by projecting each mode's amplitude orthogonal to k).
-    Momentum is set as (rho_b+rho') v."""
+    Momentum is set as (rho_b+rho') v.
+
+    The grid is a tensor product of 1D axes, so each mode is a product of 1D
+    complex exponentials; the sum over modes runs as one complex matrix product
+    (planes of the first ndim-1 axes times the last axis), which keeps 512^3
+    states within seconds."""
     rng = np.random.default_rng(seed)
     v = var_index(ndir)
     L = [x[..., d].max() - x[..., d].min() for d in range(ndim)]
     L = [l * (1 + 1.0 / (x.shape[d] - 1)) for d, l in enumerate(L)]
-    drho = np.zeros(x.shape[:-1])
-    dv = np.zeros(x.shape[:-1] + (ndir,))
-    db = np.zeros(x.shape[:-1] + (ndir,))
+    axes = []
+    for d in range(ndim):
+        idx = [0] * ndim
+        idx[d] = slice(None)
+        axes.append(x[tuple(idx) + (d,)])
+    ks, phs, avs, abs_ = [], [], [], []
     for _ in range(nmodes):
         while True:
             k = rng.integers(-kmax, kmax + 1, size=ndim)
             if 0 < np.linalg.norm(k) <= kmax:
                 break
-        phase = sum(2 * math.pi * k[d] * x[..., d] / L[d] for d in range(ndim))
         ph = rng.uniform(0, 2 * math.pi, size=3)
-        drho += np.sin(phase + ph[0])
         av = rng.normal(size=ndir)
-        dv += np.sin(phase + ph[1])[..., None] * av
         ab = rng.normal(size=ndir)
         kk = np.zeros(ndir)
         kk[:ndim] = k / np.asarray(L)
         ab = ab - kk * (ab @ kk) / (kk @ kk)
-        db += np.sin(phase + ph[2])[..., None] * ab
+        ks.append(k)
+        phs.append(ph)
+        avs.append(av)
+        abs_.append(ab)
+    ks = np.array(ks)
+    phs = np.array(phs)
+    shape = x.shape[:-1]
+    # E_d[m, i] = exp(i 2 pi k_d x_d / L_d)
+    E = [np.exp(1j * 2 * math.pi * ks[:, d, None] * axes[d][None, :] / L[d]) for d in range(ndim)]
+    lead = np.ones((nmodes, 1), dtype=complex)
+    for d in range(ndim - 1):
+        lead = (lead[:, :, None] * E[d][:, None, :]).reshape(nmodes, -1)
+    last = E[ndim - 1]                                      # [m][n_last]
+
+    def field(coef):  # sum_m Im(coef_m * e^{i phase_m}) on the grid
+        out = (lead.T * coef[None, :]) @ last                # [(lead)][last]
+        return np.imag(out).reshape(shape[:-1] + shape[-1:]) if ndim > 1 else np.imag(out).reshape(shape)
+
+    drho = field(np.exp(1j * phs[:, 0]))
+    dv = np.stack([field(np.exp(1j * phs[:, 1]) * np.array([a[c] for a in avs])) for c in range(ndir)], axis=-1)
+    db = np.stack([field(np.exp(1j * phs[:, 2]) * np.array([a[c] for a in abs_])) for c in range(ndir)], axis=-1)
     norm = lambda a: a / max(np.abs(a).max(), 1e-300)  # noqa: E731
     drho = amp * norm(drho)
     dv = amp * norm(dv)
