@@ -316,67 +316,78 @@ def ours(args, rank, world, local_rank):
 
     sbuild.build()
     torch.cuda.set_device(local_rank)
+    legs = set(args.legs.split(","))
     P = workload(args.n)
     cells = P.ncells
-    ctx, lib = make_ctx(P, local_rank, "fp64")
-    r64 = timed_steps(args, P, ctx, lib, local_rank, world)
-    value = job_rate(cells, args.steps, world, r64["ms"] / 1e3)
-
-    # end to end through the C-ABI with host buffers: per step upload(w),
-    # getdt, advect, download(w) from/to pinned host memory
     nbytes = P.nw * int(np.prod(P.ixGhi)) * 8
-    pin = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
-    hw = pin.numpy().reshape(P.ixGhi + (P.nw,), order="F")
-    hw[...] = ctx.download()
-    t, it = r64["t"], r64["it"]
-    e2e_steps = max(3, min(args.steps, 10))
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        ctx.upload(hw)
-        dt = ctx.getdt(it)
-        ctx.advect(dt, t, it)
-        t += dt
-        it += 1
-        ctx.download(hw)
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world, device=f"cuda:{local_rank}")
-    e2e = job_rate(cells, e2e_steps, world, e2e_s)
-    ctx.close()
+    r64 = r32 = None
+    value = e2e = v32 = None
+    if legs & {"fp64", "e2e"}:
+        ctx, lib = make_ctx(P, local_rank, "fp64")
+        r64 = timed_steps(args, P, ctx, lib, local_rank, world)
+        value = job_rate(cells, args.steps, world, r64["ms"] / 1e3)
+        if "e2e" in legs:
+            # end to end through the C-ABI with host buffers: per step upload(w),
+            # getdt, advect, download(w) from/to pinned host memory
+            pin = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+            hw = pin.numpy().reshape(P.ixGhi + (P.nw,), order="F")
+            hw[...] = ctx.download()
+            t, it = r64["t"], r64["it"]
+            e2e_steps = max(3, min(args.steps, 10))
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(e2e_steps):
+                ctx.upload(hw)
+                dt = ctx.getdt(it)
+                ctx.advect(dt, t, it)
+                t += dt
+                it += 1
+                ctx.download(hw)
+            e2e_s = max_over_ranks(time.perf_counter() - t0, world, device=f"cuda:{local_rank}")
+            e2e = job_rate(cells, e2e_steps, world, e2e_s)
+        ctx.close()
 
-    # the FP32-perturbation path on the same workload
-    P32 = workload(args.n)
-    ctx32, lib32 = make_ctx(P32, local_rank, "fp32")
-    r32 = timed_steps(args, P32, ctx32, lib32, local_rank, world, clocks=False)
-    ctx32.close()
-    v32 = job_rate(cells, args.steps, world, r32["ms"] / 1e3)
+    if "fp32" in legs:
+        # the FP32-perturbation path on the same workload
+        P32 = workload(args.n)
+        ctx32, lib32 = make_ctx(P32, local_rank, "fp32")
+        r32 = timed_steps(args, P32, ctx32, lib32, local_rank, world, clocks=r64 is None)
+        ctx32.close()
+        v32 = job_rate(cells, args.steps, world, r32["ms"] / 1e3)
 
     if rank != 0:
         return 0
     peak, peak_kind = load_peaks()
+    lead = r64 or r32
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": r64["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "stratified atmosphere 128^3, FP64, RK4, hyperdiffusion, gravity, driver",
+        "metric": METRIC, "value": value if value is not None else v32, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": lead["ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if r64 else "f32", "data": "synthetic",
+        "config": {"workload": f"stratified atmosphere {args.n}^3, FP64, RK4, hyperdiffusion, gravity, driver",
                    "cells_per_step": cells, "parallelism": f"replicas{world}",
-                   "l2": "no flush: resident state ~1.6 GB per replica, larger than L2",
+                   "l2": "no flush: resident state ~1.6 GB per replica at 128^3, larger than L2",
                    "step": "getdt + advect (4 RK stages + boundary fills)"},
-        "roofline": roofline(BYTES_PER_CELL_UPDATE["fp64"], cells, r64["kern"], peak, peak_kind,
-                             "update_fp64_traffic.json", "k_update<3,3,double>"),
-        "kernels_ms_per_step": {k: v[0] / args.steps for k, v in r64["kern"].items()},
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                "path": "sac_upload + sac_getdt + sac_advect + sac_download per step, pinned host w"},
-        "gpu_launches": r64["launches"],
-        "clocks": r64["clocks"],
-        "fp32": {"value": v32, "ms_per_step": r32["ms"] / args.steps, "speedup_vs_fp64": v32 / value,
-                 "gpu_launches": r32["launches"],
-                 "kernels_ms_per_step": {k: v[0] / args.steps for k, v in r32["kern"].items()},
-                 "roofline": roofline(BYTES_PER_CELL_UPDATE["fp32"], cells, r32["kern"], peak, peak_kind,
-                                      "update_fp32_traffic.json", "k_update<3,3,float>")},
+        "gpu_launches": lead["launches"],
+        "clocks": lead["clocks"],
     }
-    if world == 1 and not args.no_cpu:
+    if r64:
+        line["roofline"] = roofline(BYTES_PER_CELL_UPDATE["fp64"], cells, r64["kern"], peak, peak_kind,
+                                    "update_fp64_traffic.json", "k_update<3,3,double>")
+        line["kernels_ms_per_step"] = {k: v[0] / args.steps for k, v in r64["kern"].items()}
+    if e2e is not None:
+        line["e2e"] = {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                       "path": "sac_upload + sac_getdt + sac_advect + sac_download per step, pinned host w"}
+    if r32:
+        line["fp32"] = {"value": v32, "ms_per_step": r32["ms"] / args.steps,
+                        "speedup_vs_fp64": (v32 / value) if value else None,
+                        "gpu_launches": r32["launches"],
+                        "kernels_ms_per_step": {k: v[0] / args.steps for k, v in r32["kern"].items()},
+                        "roofline": roofline(BYTES_PER_CELL_UPDATE["fp32"], cells, r32["kern"], peak, peak_kind,
+                                             "update_fp32_traffic.json", "k_update<3,3,float>")}
+    if world == 1 and not args.no_cpu and "cpu" in legs:
         v, n, el, cores = cpu_sample()
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"{n} RK4 steps in {el:.1f} s on a {REF_SAMPLE[0]}x{REF_SAMPLE[1]}x"
@@ -393,6 +404,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128, help="mesh cells per dimension (default 128)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--legs", default="fp64,e2e,fp32,cpu",
+                    help="comma list of fp64, e2e, fp32, cpu (profiling runs select one kernel family)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
