@@ -122,7 +122,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # the CPU legs (oracle = C++ restatement of the reference)
 # ---------------------------------------------------------------------------
-def cpu_sample(seconds=10.0, max_steps=8):
+def cpu_sample(seconds=12.0, max_steps=64):
     """Cell-updates/s of the oracle on the host cores: one untimed RK4 step, then
     timed steps until `seconds` elapse, on a REF_SAMPLE slab of the workload."""
     from oracle import oracle
