@@ -451,8 +451,25 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
 // ---------------------------------------------------------------------------
 // single-grid kernels
 // ---------------------------------------------------------------------------
+// resident blocks per SM of the face and setnu passes (measured at 128^3, like
+// the update's below: face 1.11 -> 0.82 ms in FP64 at 4 blocks, nu 1.04 -> 0.98
+// ms in FP64 at 6; FP32 setnu is fastest without a bound)
+#ifndef SAC_FACE_MINB_F64
+#define SAC_FACE_MINB_F64 4
+#endif
+#ifndef SAC_FACE_MINB_F32
+#define SAC_FACE_MINB_F32 4
+#endif
+#ifndef SAC_NU_MINB_F64
+#define SAC_NU_MINB_F64 6
+#endif
+#ifndef SAC_NU_MINB_F32
+#define SAC_NU_MINB_F32 1
+#endif
+
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256) k_face(const Stage2Args a, int do_ctot) {
+__global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_FACE_MINB_F64 : SAC_FACE_MINB_F32)
+    k_face(const Stage2Args a, int do_ctot) {
   __shared__ double sh[32];
   const Geom& g = a.g;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -472,7 +489,8 @@ __global__ void __launch_bounds__(256) k_face(const Stage2Args a, int do_ctot) {
 }
 
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256) k_nu(const Stage2Args a) {
+__global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_NU_MINB_F64 : SAC_NU_MINB_F32)
+    k_nu(const Stage2Args a) {
   const Geom& g = a.g;
   int ext[3], p[3];
 #pragma unroll
@@ -530,7 +548,8 @@ __device__ __forceinline__ bool tile_cell(const Tile& tl, const Geom& g, const i
 }
 
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256) kb_face(const BatchStageArgs b, double gamma) {
+__global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_FACE_MINB_F64 : SAC_FACE_MINB_F32)
+    kb_face(const BatchStageArgs b, double gamma) {
   __shared__ double sh[32];
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     const Tile tl = b.tiles[t];
@@ -554,7 +573,8 @@ __global__ void __launch_bounds__(256) kb_face(const BatchStageArgs b, double ga
 }
 
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256) kb_nu(const BatchStageArgs b) {
+__global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_NU_MINB_F64 : SAC_NU_MINB_F32)
+    kb_nu(const BatchStageArgs b) {
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     const Tile tl = b.tiles[t];
     if (b.dyn[tl.inst].dt == 0.0) continue;
