@@ -164,10 +164,14 @@ sac_status sac_profile_read(sac_ctx* c, int kernel, double* total_ms, long* laun
 long sac_kernel_launches(const sac_ctx* c);
 
 /* ---- getdt that allocates nothing (library extension; no reference counterpart) ----
- * Same result and side effects as sac_getdt.  Its getdt_courant reduction runs as a
- * deterministic two-pass block reduction whose scratch (8192 partial maxima and the
- * result) is a file-scope device array of the library, not memory of the context,
- * and the call makes no cudaMalloc/cudaFree or other allocating call.
+ * For callers that cannot allocate device memory where they need dt: a host that
+ * gives the whole device to its own pre-sized pool, or code running inside a stream
+ * capture or a host callback, where cudaMalloc is not allowed or synchronises the
+ * device.  Same result and side effects as sac_getdt.  Its getdt_courant reduction
+ * runs as a deterministic two-pass block reduction whose scratch (8192 partial
+ * maxima and the result, 64 KB) is a file-scope device array of the library, held by
+ * every GPU that loads the library until the process exits; the call makes no
+ * cudaMalloc/cudaFree or other allocating call.
  *   - Limit: meshes of at most SAC_STATIC_MAX_CELLS cells; a larger mesh returns
  *     SAC_ERR_UNSUPPORTED with the sizes in sac_last_error (use sac_getdt there).
  *   - The scratch is one per device, shared by every context on it: calls that
