@@ -85,6 +85,8 @@ int sac_fno_zero_grad(sac_fno* n);
 /* x: [B][cin][S][F] bf16, kept unchanged by the caller until sac_fno_backward;
  * y: [B][cout][S][F] float */
 int sac_fno_forward(sac_fno* n, const void* x, float* y, int B);
+/* the same output without storing what the backward pass needs (inference) */
+int sac_fno_infer(sac_fno* n, const void* x, float* y, int B);
 /* dy: [B][cout8][S][F] bf16, cout8 = cout rounded up to 8 (extra channels zero);
  * accumulates the parameter gradients of the last forward pass */
 int sac_fno_backward(sac_fno* n, const void* dy);

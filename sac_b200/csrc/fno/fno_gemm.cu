@@ -21,18 +21,50 @@ namespace {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
-template <int BN>
-cudaError_t launch_bn(const GemmDesc& d, cudaStream_t st) {
+template <int BN, int EPI>
+cudaError_t launch_kind(const GemmDesc& d, cudaStream_t st) {
   constexpr int smem = gemm_smem_bytes<BN>();
   static bool attr = false;  // per process; the attribute is per device function
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(k_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
   dim3 grid((unsigned)((d.M + kBM - 1) / kBM), (unsigned)((d.N + BN - 1) / BN), (unsigned)(d.batch * d.ksplit));
-  k_gemm<BN><<<grid, kThreads, smem, st>>>(d);
+  k_gemm<BN, EPI><<<grid, kThreads, smem, st>>>(d);
   return cudaGetLastError();
+}
+
+// the compiled epilogue form that matches the descriptor (EPI_GENERIC otherwise)
+int epi_kind(const GemmDesc& d) {
+  const bool bias = d.bias_n != nullptr, add = d.add != nullptr;
+  if (d.c_mode == C_ATOMIC)
+    return (!d.c_bf16 && !bias && !add && d.act == ACT_NONE) ? EPI_F32_ATOMIC : EPI_GENERIC;
+  if (d.c_mode != C_STORE) return EPI_GENERIC;
+  for (int k = 1; k < EPI_KINDS; ++k) {
+    const EpiForm f = epi_form(k);
+    if (f.atomic) continue;
+    if (f.bias == bias && f.add == add && f.bf16 == (d.c_bf16 != 0) && f.act == d.act) return k;
+  }
+  return EPI_GENERIC;
+}
+
+template <int BN>
+cudaError_t launch_bn(const GemmDesc& d, cudaStream_t st) {
+  switch (epi_kind(d)) {
+    case EPI_F32: return launch_kind<BN, EPI_F32>(d, st);
+    case EPI_BF16: return launch_kind<BN, EPI_BF16>(d, st);
+    case EPI_BF16_BIAS: return launch_kind<BN, EPI_BF16_BIAS>(d, st);
+    case EPI_F32_BIAS: return launch_kind<BN, EPI_F32_BIAS>(d, st);
+    case EPI_BF16_BIAS_GELU: return launch_kind<BN, EPI_BF16_BIAS_GELU>(d, st);
+    case EPI_BF16_BIAS_ADD: return launch_kind<BN, EPI_BF16_BIAS_ADD>(d, st);
+    case EPI_BF16_BIAS_ADD_GELU: return launch_kind<BN, EPI_BF16_BIAS_ADD_GELU>(d, st);
+    case EPI_BF16_ADD: return launch_kind<BN, EPI_BF16_ADD>(d, st);
+    case EPI_BF16_ADD_GRAD: return launch_kind<BN, EPI_BF16_ADD_GRAD>(d, st);
+    case EPI_BF16_GRAD: return launch_kind<BN, EPI_BF16_GRAD>(d, st);
+    case EPI_F32_ATOMIC: return launch_kind<BN, EPI_F32_ATOMIC>(d, st);
+    default: return launch_kind<BN, EPI_GENERIC>(d, st);
+  }
 }
 
 }  // namespace

@@ -59,6 +59,42 @@ struct GemmDesc {
 
 constexpr int kBM = 128, kBK = 64, kThreads = 128;
 
+// Epilogue forms compiled as separate kernels, so that the per-element work
+// carries no test of runtime flags; EPI_GENERIC reads every flag at run time.
+struct EpiForm {
+  bool generic, bias, add, bf16, atomic;
+  int act;
+};
+enum EpiKind : int {
+  EPI_GENERIC = 0,
+  EPI_F32,             // store float
+  EPI_BF16,            // store bf16
+  EPI_BF16_BIAS,       // + bias, bf16
+  EPI_F32_BIAS,        // + bias, float
+  EPI_BF16_BIAS_GELU,  // + bias, GELU (pre stored), bf16
+  EPI_BF16_BIAS_ADD,   // + bias + add, bf16
+  EPI_BF16_BIAS_ADD_GELU,
+  EPI_BF16_ADD,        // + add, bf16
+  EPI_BF16_ADD_GRAD,   // (acc + add) * GELU'(pre), bf16
+  EPI_BF16_GRAD,       // acc * GELU'(pre), bf16
+  EPI_F32_ATOMIC,      // atomic add, float
+  EPI_KINDS
+};
+__host__ __device__ constexpr EpiForm epi_form(int k) {
+  return k == EPI_F32                  ? EpiForm{false, false, false, false, false, ACT_NONE}
+         : k == EPI_BF16               ? EpiForm{false, false, false, true, false, ACT_NONE}
+         : k == EPI_BF16_BIAS          ? EpiForm{false, true, false, true, false, ACT_NONE}
+         : k == EPI_F32_BIAS           ? EpiForm{false, true, false, false, false, ACT_NONE}
+         : k == EPI_BF16_BIAS_GELU     ? EpiForm{false, true, false, true, false, ACT_GELU}
+         : k == EPI_BF16_BIAS_ADD      ? EpiForm{false, true, true, true, false, ACT_NONE}
+         : k == EPI_BF16_BIAS_ADD_GELU ? EpiForm{false, true, true, true, false, ACT_GELU}
+         : k == EPI_BF16_ADD           ? EpiForm{false, false, true, true, false, ACT_NONE}
+         : k == EPI_BF16_ADD_GRAD      ? EpiForm{false, false, true, true, false, ACT_GELU_GRAD}
+         : k == EPI_BF16_GRAD          ? EpiForm{false, false, false, true, false, ACT_GELU_GRAD}
+         : k == EPI_F32_ATOMIC         ? EpiForm{false, false, false, false, true, ACT_NONE}
+                                       : EpiForm{true, false, false, false, false, ACT_NONE};
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 // UMMA shared-memory descriptor, no swizzle: start, leading and stride byte
@@ -171,8 +207,8 @@ __device__ __forceinline__ uint64_t tile_desc(uint32_t saddr, int mn_major, int 
   return umma_sdesc(saddr + kstep * 2 * ROWS * 16, ROWS * 16, 128);
 }
 
-template <int BN>
-__global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmDesc d) {
+template <int BN, int EPI>
+__global__ void __launch_bounds__(kThreads, BN <= 64 ? 4 : BN <= 128 ? 3 : 1) k_gemm(const GemmDesc d) {
   constexpr int A_BYTES = kBM * kBK * 2, B_BYTES = BN * kBK * 2, STAGE = A_BYTES + B_BYTES;
   constexpr int TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -265,6 +301,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmDesc d) {
       if (m >= d.M) continue;
       // all loads of the chunk first (independent, so they overlap), then the
       // arithmetic, then the stores; columns past N are masked, not branched on
+      constexpr EpiForm E = epi_form(EPI);
+      const bool has_bias = E.generic ? d.bias_n != nullptr : E.bias;
+      const bool has_add = E.generic ? d.add != nullptr : E.add;
+      const int act = E.generic ? d.act : E.act;
+      const bool out_bf16 = E.generic ? d.c_bf16 != 0 : E.bf16;
+      const int mode = E.generic ? d.c_mode : (E.atomic ? C_ATOMIC : C_STORE);
+      const bool store_pre = d.pre != nullptr;  // uniform: inference passes no pre buffer
       float x[16], ad[16], pr[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
@@ -272,9 +315,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmDesc d) {
         const bool in = n < d.N;
         const long o = crow + (long)n * d.c_n;
         x[j] = nk > 0 ? d.alpha * __uint_as_float(v[j]) : 0.0f;
-        ad[j] = (in && d.add) ? __ldg(d.add + o) : 0.0f;
-        pr[j] = (in && d.act == ACT_GELU_GRAD) ? __bfloat162float(d.pre[o]) : 0.0f;
-        if (in && d.bias_n) x[j] += __ldg(d.bias_n + n);
+        ad[j] = (in && has_add) ? __ldg(d.add + o) : 0.0f;
+        pr[j] = (in && act == ACT_GELU_GRAD) ? __bfloat162float(d.pre[o]) : 0.0f;
+        if (in && has_bias) x[j] += __ldg(d.bias_n + n);
       }
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
@@ -282,21 +325,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmDesc d) {
         if (n >= d.N) continue;
         const long o = crow + (long)n * d.c_n;
         float y = x[j] + ad[j];
-        if (d.act == ACT_GELU) {
-          if (d.pre) d.pre[o] = __float2bfloat16(y);
+        if (act == ACT_GELU) {
+          if (store_pre) d.pre[o] = __float2bfloat16(y);
           y = gelu_f(y);
-        } else if (d.act == ACT_GELU_GRAD) {
+        } else if (act == ACT_GELU_GRAD) {
           y *= gelu_grad_f(pr[j]);
         }
-        if (d.c_bf16) {
+        if (out_bf16) {
           bf16* C = (bf16*)d.c;
-          if (d.c_mode == C_ACCUM) y += __bfloat162float(C[o]);
+          if (mode == C_ACCUM) y += __bfloat162float(C[o]);
           C[o] = __float2bfloat16(y);
         } else {
           float* C = (float*)d.c;
-          if (d.c_mode == C_ATOMIC)
+          if (mode == C_ATOMIC)
             atomicAdd(C + o, y);
-          else if (d.c_mode == C_ACCUM)
+          else if (mode == C_ACCUM)
             C[o] += y;
           else
             C[o] = y;

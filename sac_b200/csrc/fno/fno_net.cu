@@ -341,10 +341,11 @@ void c_chanfirst(GemmDesc& d, void* c, int N, long P, int bf) {
 }
 
 // ---------------------------------------------------------------------------
-int forward(sac_fno* n, const bf16* x, float* y, int B) {
+// train: keep what the backward pass needs (pre-activations, the input pointer)
+int forward(sac_fno* n, const bf16* x, float* y, int B, bool train) {
   const int S = n->S, F = n->F, W = n->W, H = n->H;
   const long P = n->P;
-  n->xin = x;
+  n->xin = train ? x : nullptr;
   n->Blast = B;
   // lift: v0[b][o][p] = sum_c Pw[o][c] x[b][c][p] + pb[o]
   {
@@ -445,7 +446,7 @@ int forward(sac_fno* n, const bf16* x, float* y, int B) {
       d.bias_n = n->w + n->sWb[l].off;
       if (l < n->L - 1) {
         d.act = ACT_GELU;
-        d.pre = n->pre[l];
+        d.pre = train ? n->pre[l] : nullptr;
       }
       d.err = n->errw;
       GK(d);
@@ -461,7 +462,7 @@ int forward(sac_fno* n, const bf16* x, float* y, int B) {
     c_chanfirst(d, n->h, H, P, 1);
     d.bias_n = n->w + n->sQ1b.off;
     d.act = ACT_GELU;
-    d.pre = n->hpre;
+    d.pre = train ? n->hpre : nullptr;
     d.err = n->errw;
     GK(d);
   }
@@ -936,7 +937,16 @@ int sac_fno_forward(sac_fno* n, const void* x, float* y, int B) {
   if (!n || !x || !y) return fail(n, "sac_fno_forward: null argument");
   if (B < 1 || B > n->Bmax) return fail(n, "sac_fno_forward: batch outside 1..max_batch");
   FK(cudaSetDevice(n->cfg.device));
-  return forward(n, (const bf16*)x, y, B);
+  return forward(n, (const bf16*)x, y, B, true);
+}
+
+// the forward pass without what training needs (no pre-activation stores); a
+// backward pass cannot follow it
+int sac_fno_infer(sac_fno* n, const void* x, float* y, int B) {
+  if (!n || !x || !y) return fail(n, "sac_fno_infer: null argument");
+  if (B < 1 || B > n->Bmax) return fail(n, "sac_fno_infer: batch outside 1..max_batch");
+  FK(cudaSetDevice(n->cfg.device));
+  return forward(n, (const bf16*)x, y, B, false);
 }
 
 // dy: [B][cpad][S][F] bf16 with cpad = cout rounded up to 8 (padding channels zero)

@@ -109,6 +109,7 @@ def _bind_net(lib):
     lib.sac_fno_get_grads.argtypes = [VP, FP]
     lib.sac_fno_zero_grad.argtypes = [VP]
     lib.sac_fno_forward.argtypes = [VP, VP, VP, ctypes.c_int]
+    lib.sac_fno_infer.argtypes = [VP, VP, VP, ctypes.c_int]
     lib.sac_fno_backward.argtypes = [VP, VP]
     lib.sac_fno_mse.argtypes = [VP, VP, VP, VP, VP, ctypes.c_int]
     lib.sac_fno_adam.argtypes = [VP, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -117,7 +118,7 @@ def _bind_net(lib):
     lib.sac_fno_apply.argtypes = [VP, VP, VP, VP, ctypes.c_int, ctypes.c_int]
     lib.sac_fno_check.argtypes = [VP, ctypes.c_int]
     for f in ("sac_fno_create", "sac_fno_param_layout", "sac_fno_init", "sac_fno_set_params", "sac_fno_get_params",
-              "sac_fno_get_grads", "sac_fno_zero_grad", "sac_fno_forward", "sac_fno_backward", "sac_fno_mse",
+              "sac_fno_get_grads", "sac_fno_zero_grad", "sac_fno_forward", "sac_fno_infer", "sac_fno_backward", "sac_fno_mse",
               "sac_fno_adam", "sac_fno_features", "sac_fno_apply", "sac_fno_check"):
         getattr(lib, f).restype = ctypes.c_int
     lib._net_bound = True
@@ -183,6 +184,10 @@ class Net:
 
     def forward(self, x_ptr, y_ptr, B):
         self._c(self.lib.sac_fno_forward(self.h, VP(x_ptr), VP(y_ptr), B))
+
+    def infer(self, x_ptr, y_ptr, B):
+        """forward() without the stores the backward pass needs."""
+        self._c(self.lib.sac_fno_infer(self.h, VP(x_ptr), VP(y_ptr), B))
 
     def backward(self, dy_ptr):
         self._c(self.lib.sac_fno_backward(self.h, VP(dy_ptr)))

@@ -61,7 +61,7 @@ def main(argv=None):
     torch.cuda.synchronize()
 
     def fwd():
-        net.forward(x.data_ptr(), y.data_ptr(), B)
+        net.infer(x.data_ptr(), y.data_ptr(), B)
 
     step = [0]
 
@@ -86,7 +86,7 @@ def main(argv=None):
     net.check()
     ms = e0.elapsed_time(e1) / a.iters
     fl = flops_per_sample() * (3 if a.train else 1)
-    out = {"mode": "train step" if a.train else "forward", "batch": B, "ms_per_call": ms,
+    out = {"mode": "train step" if a.train else "inference forward", "batch": B, "ms_per_call": ms,
            "samples_per_s": B / (ms / 1e3), "flops_per_sample": fl, "tflops": fl * B / (ms / 1e3) / 1e12,
            "forward_bytes_per_sample": bytes_per_sample(),
            "forward_gbs": (bytes_per_sample() * B / (ms / 1e3) / 1e9) if not a.train else None}

@@ -273,7 +273,7 @@ class Surrogate:
                 blk = state[sl]
             self.net.features(blk.data_ptr(), False, self.scale.data_ptr(), self.feat.data_ptr(), NFEAT,
                               self.x.data_ptr(), B, NST)
-            self.net.forward(self.x.data_ptr(), self.y.data_ptr(), B)
+            self.net.infer(self.x.data_ptr(), self.y.data_ptr(), B)
             with torch.cuda.stream(self.stream):
                 self.scale[:B * NST] = torch.as_tensor(sc_out[i0 * NST:(i0 + B) * NST], dtype=torch.float32,
                                                        device="cuda")

@@ -124,3 +124,19 @@ def test_adam_training_reduces_the_loss():
         net.check()
         losses.append(loss.item())
     assert losses[-1] < 0.2 * losses[0], losses[::10]
+
+
+def test_inference_pass_equals_training_forward():
+    B = 2
+    net = _net(B)
+    xd = _inputs(B, 4).cuda()
+    y1 = torch.zeros(B, CFG["cout"], CFG["S"], CFG["F"], device="cuda")
+    y2 = torch.zeros_like(y1)
+    dy = torch.zeros(B, net.cpad, CFG["S"], CFG["F"], dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    net.forward(xd.data_ptr(), y1.data_ptr(), B)
+    net.infer(xd.data_ptr(), y2.data_ptr(), B)
+    net.check()
+    assert torch.equal(y1, y2)
+    with pytest.raises(fno_abi.FnoError):
+        net.backward(dy.data_ptr())  # nothing recorded for a backward pass
