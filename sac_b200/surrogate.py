@@ -316,9 +316,11 @@ def rel_l2(a, b):
 
 
 def rollout(sur: Surrogate, A, om, dt, window, nwin, M=16, tol=1e-3, divb_tol=1e-3, energy_tol=1e-3,
-            n=(256, 256), log=print):
+            n=(256, 256), solver_windows=0, log=print):
     """Judged surrogate roll-out and the plain solver's own run on the same
-    drivers; returns errors and device times (CUDA events)."""
+    drivers; returns errors and device times (CUDA events).  The first
+    `solver_windows` windows (growth from rest, where the surrogate's relative
+    error is largest) are taken by the plain solver, inside the timed region."""
     torch = _torch()
     S, F = n[1], n[0]
     ninst = len(A)
@@ -365,7 +367,13 @@ def rollout(sur: Surrogate, A, om, dt, window, nwin, M=16, tol=1e-3, divb_tol=1e
     s0 = torch.cuda.Event(enable_timing=True)
     s1 = torch.cuda.Event(enable_timing=True)
     s0.record()
-    for k in range(nwin):
+    if solver_windows > 0:
+        judge.advance(window * solver_windows)
+        judge.gather(state.data_ptr(), "f32")
+        judge.synchronize()
+        ckpt.copy_(state)
+        t_ck = solver_windows * window * dt
+    for k in range(solver_windows, nwin):
         t, t_next = k * window * dt, (k + 1) * window * dt
         judged_now = (k + 1) % M == 0
         if judged_now:
@@ -416,7 +424,7 @@ def rollout(sur: Surrogate, A, om, dt, window, nwin, M=16, tol=1e-3, divb_tol=1e
            "speedup": solver_ms / sur_ms, "final_rel_l2_mean": float(final.mean()),
            "final_rel_l2_max": float(final.max()), "final_rel_l2_median": float(np.median(final)),
            "judged": judged, "rejected": rejected, "worst_judged_rel_l2": worst,
-           "judge_solver_steps": judge_steps}
+           "judge_solver_steps": judge_steps, "solver_windows": solver_windows}
     log(json.dumps(out))
     return out
 
@@ -449,6 +457,8 @@ def main(argv=None):
     ap.add_argument("--out", default=None)
     ap.add_argument("--weights", default=None, help="skip data and training; load these weights")
     ap.add_argument("--dt", type=float, default=None, help="the fixed dt of the trajectories")
+    ap.add_argument("--solver-windows", type=int, default=2,
+                    help="windows from rest taken by the plain solver in the second set of roll-outs")
     a = ap.parse_args(argv)
     torch = _torch()
     torch.cuda.init()
@@ -483,8 +493,9 @@ def main(argv=None):
         torch.cuda.empty_cache()
     At, omt = drivers(a.ntest, a.seed + 1000, omega_ac)
     runs = []
-    for M, tol in ((a.M, 1e-3), (a.M, 2e-2), (10 ** 9, 1e-3)):
-        r = rollout(sur, At, omt, dt, a.window, nwin, M=M, tol=tol, n=n, log=log)
+    for M, tol, sw in ((a.M, 1e-3, 0), (a.M, 2e-2, 0), (10 ** 9, 1e-3, 0), (a.M, 1e-3, a.solver_windows),
+                       (a.M, 2e-2, a.solver_windows), (10 ** 9, 1e-3, a.solver_windows)):
+        r = rollout(sur, At, omt, dt, a.window, nwin, M=M, tol=tol, n=n, solver_windows=sw, log=log)
         runs.append(r)
     res = {"rollouts": runs, "train": val, "generate_s": gen_s, "dt": dt, "ntrain": a.ntrain,
            "train_steps": sur.step}
