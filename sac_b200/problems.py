@@ -110,8 +110,11 @@ def brio_wu(nx=800, courantpar=0.8, tmax=0.1, typeadvance="fourstep", nu=1.0) ->
     w[m, v["e"]] = p / (gamma - 1.0) + 0.5 * (b1 * b1 + b2 * b2)
     w[m, v["b0"] + 1] = b1
     w[m, v["b0"] + 2] = b2
+    # hyperdiffusion with the viscous dt limit (gravity module, zero gravity):
+    # at Courant 0.8 the Courant limit alone lets the shock blow up
+    from .params import USR_GRAVVISC
     prm = make_params(gamma=gamma, nu=nu, courantpar=courantpar, typeadvance=typeadvance,
-                      user=USR_VISCOSITY)
+                      user=USR_GRAVVISC, grav=(0.0, 0.0, 0.0))
     return Problem("briowu", ndim, ndir, (nx,), prm, x, w, uniform_types(ndim, v["nw"], "cont"), tmax=tmax)
 
 
