@@ -388,9 +388,10 @@ __global__ void __launch_bounds__(256) kb_bound(BcArgs proto, const InstInfo* __
     const GhostChunk ch = chunks[t];
     if (dyn && dyn[ch.inst].dt == 0.0) continue;  // a finished instance keeps its state
     BcArgs a = proto;
-    a.g = inst[ch.inst].g;
-    a.oA = inst[ch.inst].o.P;
-    a.oB = inst[ch.inst].o.B;
+    const InstInfo I = inst[ch.inst];
+    a.g = I.g;
+    a.oA = I.o.P;
+    a.oB = I.o.B;
     for (int d = 0; d < 3; ++d) {  // periodic sources one mesh extent away (src/vacgrid.t:109-120)
       const int nm = d < a.g.ndim ? a.g.hi[d] - a.g.lo[d] + 1 : 0;
       a.pairshift[d][0] = nm;

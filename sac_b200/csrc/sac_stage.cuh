@@ -563,7 +563,7 @@ __global__ void __launch_bounds__(256) kb_face(const BatchStageArgs b, double ga
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     const Tile tl = b.tiles[t];
     if (b.dyn[tl.inst].dt == 0.0) continue;  // finished (tmax): nothing to compute
-    const InstInfo& I = b.inst[tl.inst];
+    const InstInfo I = b.inst[tl.inst];  // a register copy: stores cannot alias it
     const Geom& g = I.g;
     const int lo[3] = {0, 0, 0}, hi[3] = {g.n[0] - 1, g.n[1] - 1, g.n[2] - 1};
     int p[3];
@@ -586,7 +586,7 @@ __global__ void __launch_bounds__(256) kb_nu(const BatchStageArgs b) {
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     const Tile tl = b.tiles[t];
     if (b.dyn[tl.inst].dt == 0.0) continue;
-    const InstInfo& I = b.inst[tl.inst];
+    const InstInfo I = b.inst[tl.inst];  // a register copy: stores cannot alias it
     const Geom& g = I.g;
     int lo[3], hi[3], p[3];
     for (int d = 0; d < 3; ++d) {
@@ -606,7 +606,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_BATCH_UPDATE_MINB_F6
   __shared__ double sh[32];
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
     const Tile tl = b.tiles[t];
-    const InstInfo& I = b.inst[tl.inst];
+    const InstInfo I = b.inst[tl.inst];  // a register copy: stores cannot alias it
     const Geom& g = I.g;
     int p[3];
     double numax = 0.0;
@@ -614,11 +614,11 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_BATCH_UPDATE_MINB_F6
       // the RK4 stage steps of advect, src/vac.t:442-452; every stage sees the
       // driver at the step's start time t (advect1 is called with t)
       const InstDyn& D = b.dyn[tl.inst];
-      const double dt = D.dt;
+      const double dt = D.dt, drvA = D.drvA, omega = D.omega, tnow = D.t;
       const double qdt = b.stage == 0 ? dt / 2 : b.stage == 1 ? dt / 2 : b.stage == 2 ? dt : dt / 6;
       const double qdt2 = qdt * ((double)(b.a.dmax - b.a.dmin) + 1.0) / (double)g.ndim;
-      const double tdep = b.a.driver != DRV_NONE ? sin(D.omega * D.t) : 0.0;
-      update_cell<NDIM, NDIR, S>(b.a, g, I.o, p, qdt, qdt2, tdep, D.drvA, numax);
+      const double tdep = b.a.driver != DRV_NONE ? sin(omega * tnow) : 0.0;
+      update_cell<NDIM, NDIR, S>(b.a, g, I.o, p, qdt, qdt2, tdep, drvA, numax);
     }
     if (b.a.visc_on) block_max_to(&b.dyn[tl.inst].maxnu, numax, sh);
   }
@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(256) kb_courant(const BatchStageArgs b, double
     const Tile tl = b.tiles[t];
     const InstDyn& Dy = b.dyn[tl.inst];
     if (Dy.tmax > 0.0 && Dy.t >= Dy.tmax) continue;  // finished: its dt will be 0
-    const InstInfo& I = b.inst[tl.inst];
+    const InstInfo I = b.inst[tl.inst];  // a register copy: stores cannot alias it
     const Geom& g = I.g;
     int p[3];
     double best = 0.0;
