@@ -68,7 +68,10 @@ def eqpar_map(eqpar, names, ndim):
 
 
 class Run:
-    def __init__(self, par_text: str, user: str = "gravvisc", default_text: str = DEFAULT_PAR, device=0):
+    def __init__(self, par_text: str, user: str = "gravvisc", default_text: str = DEFAULT_PAR, device=0,
+                 context=None):
+        """context: the class behind the C-ABI calls (abi.Context, the device
+        library, by default)."""
         pf = params.read_par(default_text, par_text)
         self.pf = pf
         g = lambda grp, k, d=None: pf.get(grp, k, d)  # noqa: E731
@@ -160,7 +163,7 @@ class Run:
         self.isaveout = 0
         self.itmin = self.it
         self.dt = 0.0
-        self.ctx = abi.Context(self.params)
+        self.ctx = (context or abi.Context)(self.params)
         self.ctx.set_grid(ndim, ndir, self.ixGhi, self.ixM, self.x, self.fullgridini)
         self.ctx.set_boundaries(params.pack_typeB(self.types), 2 * ndim)
         self.ctx.upload(self.w)
