@@ -688,10 +688,136 @@ void specialsource(Oracle& o, double qdt, const std::vector<int>& iws, double qt
   if (u == SAC_USR_STRAT || u == SAC_USR_TUBE) driver_gauss(o, qdt, qt, w);
 }
 
-// addsource2, src/vac.t:552-582 (addsource: resistivity and Powell divB are off)
+// addsource_divb, src/vacphys.mhd0.t:263-297.  ensurebound(1,...) keeps ixO=ixM
+// and ixI=ixG (the mesh has two ghost layers), so no boundary refill.  getdivb
+// (:106-144) sums gradient4 of b+bg over every dimension; gradient4 zeroes the
+// two edge layers, so the layer of b+bg it reads beyond ixO+1 never reaches the
+// result and computing b+bg on the whole grid is equivalent.
+void addsource_divb(Oracle& o, double qdt, const std::vector<int>& iws, const Arr& w, Arr& wnew, Work& wk) {
+  wk.init(o.ncell);
+  Arr &tmp = wk.f, &g = wk.tmp, &divb = wk.fb;
+  forR(o, o.ixM, [&](long c) { divb[c] = 0.0; });
+  for (int d = 0; d < o.ndim; ++d) {
+    const double *b = o.V(w, o.b0_ + 1 + d), *bg = o.V(w, o.bg0_ + 1 + d);
+    forR(o, o.ixG, [&](long c) { tmp[c] = b[c] + bg[c]; });
+    gradient4(o, tmp, o.ixM, d, g);
+    forR(o, o.ixM, [&](long c) { divb[c] = divb[c] + g[c]; });
+  }
+  forR(o, o.ixM, [&](long c) { divb[c] = qdt * divb[c]; });
+  const double *r = o.V(w, o.rho_), *rb = o.V(w, o.rhob_);
+  for (int iw : iws) {
+    double* wn = o.V(wnew, iw);
+    if (iw > o.m0_ && iw <= o.m0_ + o.ndir) {
+      const int C = iw - o.m0_;
+      const double *b = o.V(w, o.b0_ + C), *bg = o.V(w, o.bg0_ + C);
+      forR(o, o.ixM, [&](long c) { wn[c] = wn[c] - (b[c] + bg[c]) * divb[c]; });
+    } else if (iw > o.b0_ && iw <= o.b0_ + o.ndir) {
+      const double* m = o.V(w, o.m0_ + (iw - o.b0_));
+      forR(o, o.ixM, [&](long c) { wn[c] = wn[c] - m[c] / (r[c] + rb[c]) * divb[c]; });
+    } else if (iw == o.e_) {
+      forR(o, o.ixM, [&](long c) {
+        double s = o.V(w, o.m0_ + 1)[c] * (o.V(w, o.b0_ + 1)[c] + o.V(w, o.bg0_ + 1)[c]);
+        for (int C = 2; C <= o.ndir; ++C)
+          s = s + o.V(w, o.m0_ + C)[c] * (o.V(w, o.b0_ + C)[c] + o.V(w, o.bg0_ + C)[c]);
+        wn[c] = wn[c] - s / (r[c] + rb[c]) * divb[c];
+      });
+    }
+  }
+}
+
+// Levi-Civita symbol lvc(i,j,k) of 0-based indices (src/vacdef.t:91)
+int lvc(int i, int j, int k) {
+  if (i == j || j == k || i == k) return 0;
+  return ((i + 1) % 3 == j) ? 1 : -1;
+}
+
+// gradient of the resistive module, src/vacphys.mhdres.t:304-317: note the sign,
+// -(q(+1)-q(-1))/dx/2; it enters every resistive term twice, or squared
+void gradient_res(const Oracle& o, const Arr& q, const Rg& ix, int d, Arr& g) {
+  const long s = o.st[d];
+  const double* dxd = o.dx.data() + (long)d * o.ncell;
+  forR(o, ix, [&](long c) { g[c] = -(q[c + s] - q[c - s]) / dxd[c] / 2.0; });
+}
+
+// getcurrent, src/vacphys.mhdres.t:48-95: J_i = sum eps_ijk gradient_j(b_k+bg_k)
+// on ix for i >= idirmin0 = 7-2*ndir (1-based); returns idirmin (0-based, 3 when
+// no component exists)
+int getcurrent(const Oracle& o, const Arr& w, const Rg& ix, Arr J[3], Arr& tmp, Arr& g) {
+  const int k0 = 6 - 2 * o.ndir;
+  int idirmin = 3;
+  for (int i = std::max(k0, 0); i < 3; ++i) forR(o, ix, [&](long c) { J[i][c] = 0.0; });
+  for (int i = std::max(k0, 0); i < 3; ++i)
+    for (int j = 0; j < o.ndim; ++j)
+      for (int k = 0; k < o.ndir; ++k) {
+        const int l = lvc(i, j, k);
+        if (l == 0) continue;
+        const double *b = o.V(w, o.b0_ + 1 + k), *bg = o.V(w, o.bg0_ + 1 + k);
+        forR(o, grow(o, ix, 1), [&](long c) { tmp[c] = b[c] + bg[c]; });
+        gradient_res(o, tmp, ix, j, g);
+        if (l == 1)
+          forR(o, ix, [&](long c) { J[i][c] = J[i][c] + g[c]; });
+        else
+          forR(o, ix, [&](long c) { J[i][c] = J[i][c] - g[c]; });
+        idirmin = std::min(idirmin, i);
+      }
+  return idirmin;
+}
+
+// addsource_res2, src/vacphys.mhdres.t:231-301, for a constant eta =
+// eqpar(eta_) > 0 (eta < 0 needs a user specialeta and is rejected).
+// ensurebound(2,...) keeps ixO=ixM, and ix=ixM+1.
+void addsource_res2(Oracle& o, double qdt, const std::vector<int>& iws, const Arr& w, Arr& wnew, Work& wk) {
+  wk.init(o.ncell);
+  const long n = o.ncell;
+  Arr J[3];
+  for (Arr& a : J) a.assign(n, 0.0);
+  const Rg ixO = o.ixM, ix = grow(o, ixO, 1);
+  const int idirmin = getcurrent(o, w, ix, J, wk.f, wk.tmp);
+  const double eta = o.par.eta;
+  Arr &tmp = wk.f, &tmp2 = wk.tmp;
+  for (int iw : iws) {
+    if (iw > o.b0_ && iw <= o.b0_ + o.ndir) {
+      const int i = iw - o.b0_ - 1;
+      double* wn = o.V(wnew, iw);
+      for (int j = 0; j < o.ndim; ++j)
+        for (int k = idirmin; k < 3; ++k) {
+          const int l = lvc(i, j, k);
+          if (l == 0) continue;
+          forR(o, ix, [&](long c) { tmp[c] = J[k][c] * eta * qdt; });
+          gradient_res(o, tmp, ixO, j, tmp2);
+          if (l == 1)
+            forR(o, ixO, [&](long c) { wn[c] = wn[c] - tmp2[c]; });
+          else
+            forR(o, ixO, [&](long c) { wn[c] = wn[c] + tmp2[c]; });
+        }
+    } else if (iw == o.e_) {
+      double* wn = o.V(wnew, iw);
+      for (int i = 0; i < o.ndim; ++i)
+        for (int j = 0; j < o.ndir; ++j)
+          for (int k = idirmin; k < 3; ++k) {
+            const int l = lvc(i, j, k);
+            if (l == 0) continue;
+            const double *b = o.V(w, o.b0_ + 1 + j), *bg = o.V(w, o.bg0_ + 1 + j);
+            forR(o, ix, [&](long c) { tmp[c] = (b[c] + bg[c]) * J[k][c] * eta * qdt; });
+            gradient_res(o, tmp, ixO, i, tmp2);
+            if (l == 1)
+              forR(o, ixO, [&](long c) { wn[c] = wn[c] + tmp2[c]; });
+            else
+              forR(o, ixO, [&](long c) { wn[c] = wn[c] - tmp2[c]; });
+          }
+    }
+  }
+}
+
+// addsource2, src/vac.t:552-582: specialsource, then addsource
+// (src/vacphys.mhd0.t:225-258): the resistive term when |eta| > smalldouble
+// (compactres=F, par/DEFAULT:57, selects addsource_res2), then the Powell term
+// when divbfix is set and ndim > 1 ({^NOONED}).
 void addsource2(Oracle& o, double qdt, const std::vector<int>& iws, double qtC, const Arr& wCT,
                 double qt, Arr& w, Work& wk) {
   specialsource(o, qdt, iws, qtC, wCT, qt, w, wk);
+  if (std::fabs(o.par.eta) > smalldouble) addsource_res2(o, qdt, iws, wCT, w, wk);
+  if (o.par.divbfix && o.ndim > 1) addsource_divb(o, qdt, iws, wCT, w, wk);
 }
 
 // centdiff4, src/vaccd.t:7-78.  The flux divergence is applied on the mesh ixO=ixM.
@@ -1204,9 +1330,17 @@ int oracle_getdt(oracle_ctx* cx, double* dt, int it) {
   } else {
     d = bigdouble;
     if (o.par.courantpar > 0.0) getdt_courant(o, o.w, d);
-    if (o.par.eta != 0.0) {
-      o.err = "Resistive MHD module is OFF";
+    if (o.par.eta < 0.0) {
+      o.err = "eta < 0 needs a user specialeta";
       return SAC_ERR_UNSUPPORTED;
+    }
+    if (o.par.eta > 0.0) {
+      // getdt_res, src/vacphys.mhdres.t:5-45: dtdiffpar*minval(dx(ixM,1:ndim))**2/eta,
+      // with dtdiffpar as getdt_visc may have overwritten it at an earlier call
+      double mn = bigdouble;
+      for (int dd = 0; dd < o.ndim; ++dd)
+        forR(o, o.ixM, [&](long c) { mn = std::min(mn, o.dx[(long)dd * o.ncell + c]); });
+      d = std::min(d, o.par.dtdiffpar * (mn * mn) / o.par.eta);
     }
     const int u = o.par.user;
     if (u == SAC_USR_SLOG || u == SAC_USR_GRAVVISC || u == SAC_USR_STRAT || u == SAC_USR_TUBE) {
@@ -1236,6 +1370,10 @@ int oracle_advect(oracle_ctx* cx, const char* method, const int* iws, int idimmi
   while (!m.empty() && m.back() == ' ') m.pop_back();
   if (m != "cd4" && m != "source" && m != "nul") return SAC_ERR_UNSUPPORTED;
   if (idimmin < 1 || idimmax > o.ndim || idimmin > idimmax) return SAC_ERR_ARG;
+  if (o.par.eta < -smalldouble) {
+    o.err = "eta < 0 needs a user specialeta";
+    return SAC_ERR_UNSUPPORTED;
+  }
   return advect(o, m, v, idimmin - 1, idimmax - 1, dt, t, cx->wk);
 }
 

@@ -1,0 +1,213 @@
+"""The oracle's optional source terms against direct numpy restatements (CPU).
+
+Powell's div B source (addsource_divb, src/vacphys.mhd0.t:263-297) and the
+resistive source (addsource_res2, src/vacphys.mhdres.t:231-301, constant eta)
+are checked on one 'source' step of typeadvance='onestep' with no user module,
+where the mesh update is exactly w_new = w + qdt S(w).  The Powell term is also
+checked to be compiled out of 1D runs ({^NOONED}, src/vacphys.mhd0.t:255), and
+the resistive dt limit (getdt_res, src/vacphys.mhdres.t:5-45) by its formula."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from sac_b200 import params, problems
+
+import _util
+
+
+def _view(P, a, d=None, k=0):
+    """a (full grid, first ndim axes) on the mesh shifted by k cells along d."""
+    sl = []
+    for e in range(P.ndim):
+        lo = 2 + (k if e == d else 0)
+        sl.append(slice(lo, lo + P.nx[e]))
+    return a[tuple(sl)]
+
+
+def _dx(P, d):
+    x = P.x[..., d]
+    return 0.5 * (_view(P, x, d, 1) - _view(P, x, d, -1))
+
+
+def _gradient4(P, q, d):
+    """gradient4 on the mesh, its two edge layers zeroed (src/vacgrid.t:665-712)."""
+    g = -(_view(P, q, d, 2) - 8.0 * (_view(P, q, d, 1) - _view(P, q, d, -1)) - _view(P, q, d, -2)) / _dx(P, d) / 12.0
+    idx = [slice(None)] * P.ndim
+    for layer in (0, 1, -1, -2):
+        idx[d] = layer
+        g[tuple(idx)] = 0.0
+    return g
+
+
+def _powell_step(P, w, qdt):
+    v = problems.var_index(P.ndir)
+    B = [w[..., v["b0"] + 1 + c] + w[..., v["bg0"] + 1 + c] for c in range(P.ndir)]
+    divb = np.zeros(P.nx)
+    for d in range(P.ndim):
+        divb = divb + _gradient4(P, B[d], d)
+    divb = qdt * divb
+    rt = _view(P, w[..., v["rho"]] + w[..., v["rhob"]])
+    new = _view(P, w).copy()
+    s = 0.0
+    for c in range(P.ndir):
+        Bc = _view(P, B[c])
+        mc = _view(P, w[..., v["m0"] + 1 + c])
+        new[..., v["m0"] + 1 + c] = new[..., v["m0"] + 1 + c] - Bc * divb
+        new[..., v["b0"] + 1 + c] = new[..., v["b0"] + 1 + c] - mc / rt * divb
+        s = mc * Bc if c == 0 else s + mc * Bc
+    new[..., v["e"]] = new[..., v["e"]] - s / rt * divb
+    return new
+
+
+@pytest.mark.parametrize("nx,ndir", [((14, 12), 2), ((14, 12), 3), ((10, 9, 8), 3)])
+def test_powell_source_step_matches_numpy(nx, ndir):
+    types = ["cont", "fixed", "periodic", "periodic", "cont", "symm"][: 2 * len(nx)]
+    P = problems.random_problem(nx, ndir=ndir, seed=31, types=types, user=params.USR_NONE,
+                                typeadvance="onestep")
+    P.params.divbfix = 1
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    qdt = 0.013
+    o.advect(qdt, 0.0, 0, method="source")
+    got = _util.mesh(P, o.download())
+    want = _powell_step(P, w0, qdt)
+    nadv = 2 * P.ndir + 2
+    assert np.abs(got[..., :nadv] - _util.mesh(P, w0)[..., :nadv]).max() > 1e-6  # the source acts
+    np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
+
+
+def test_powell_source_is_off_in_1d():
+    P = problems.random_problem((40,), ndir=3, seed=32)
+    a = _util.start(Oracle, P)
+    _util.run(a, 10)
+    P.params.divbfix = 1
+    b = _util.start(Oracle, P)
+    _util.run(b, 10)
+    np.testing.assert_array_equal(a.download(), b.download())
+
+
+def test_powell_source_changes_a_2d_run():
+    P = problems.random_problem((14, 12), seed=33, types=["cont", "cont", "periodic", "periodic"])
+    a = _util.start(Oracle, P)
+    _util.run(a, 5)
+    P.params.divbfix = 1
+    b = _util.start(Oracle, P)
+    _util.run(b, 5)
+    assert np.abs(a.download() - b.download()).max() > 1e-8
+
+
+# ---------------------------------------------------------------------------
+# resistivity
+# ---------------------------------------------------------------------------
+def _lvc(i, j, k):
+    if i == j or j == k or i == k:
+        return 0
+    return 1 if (i + 1) % 3 == j else -1
+
+
+def _region(P, a, g, d=None, k=0):
+    """a on the mesh grown by g layers, shifted by k cells along d."""
+    sl = []
+    for e in range(P.ndim):
+        lo = 2 - g + (k if e == d else 0)
+        sl.append(slice(lo, lo + P.nx[e] + 2 * g))
+    return a[tuple(sl)]
+
+
+def _inner(P, T, d=None, k=0):
+    """T given on the mesh grown by one layer: its mesh part shifted by k along d."""
+    sl = []
+    for e in range(P.ndim):
+        lo = 1 + (k if e == d else 0)
+        sl.append(slice(lo, lo + P.nx[e]))
+    return T[tuple(sl)]
+
+
+def _resist_step(P, w, qdt, eta):
+    v = problems.var_index(P.ndir)
+    B = [w[..., v["b0"] + 1 + c] + w[..., v["bg0"] + 1 + c] for c in range(P.ndir)]
+    x = P.x
+
+    def dx(d, g):
+        return 0.5 * (_region(P, x[..., d], g, d, 1) - _region(P, x[..., d], g, d, -1))
+
+    # J = curl B by the resistive module's gradient -(q(+1)-q(-1))/dx/2
+    k0 = 6 - 2 * P.ndir
+    J, idirmin = {}, 3
+    for i in range(max(k0, 0), 3):
+        J[i] = np.zeros([n + 2 for n in P.nx])
+        for j in range(P.ndim):
+            for k in range(P.ndir):
+                sgn = _lvc(i, j, k)
+                if sgn:
+                    gr = -(_region(P, B[k], 1, j, 1) - _region(P, B[k], 1, j, -1)) / dx(j, 1) / 2.0
+                    J[i] = J[i] + gr if sgn == 1 else J[i] - gr
+                    idirmin = min(idirmin, i)
+    new = _view(P, w).copy()
+
+    def grad_mesh(T, d):
+        return -(_inner(P, T, d, 1) - _inner(P, T, d, -1)) / dx(d, 0) / 2.0
+
+    for i in range(P.ndir):
+        iw = v["b0"] + 1 + i
+        for j in range(P.ndim):
+            for k in range(idirmin, 3):
+                sgn = _lvc(i, j, k)
+                if sgn:
+                    t2 = grad_mesh(J[k] * eta * qdt, j)
+                    new[..., iw] = new[..., iw] - t2 if sgn == 1 else new[..., iw] + t2
+    for i in range(P.ndim):
+        for j in range(P.ndir):
+            for k in range(idirmin, 3):
+                sgn = _lvc(i, j, k)
+                if sgn:
+                    t2 = grad_mesh(_region(P, B[j], 1) * J[k] * eta * qdt, i)
+                    new[..., v["e"]] = new[..., v["e"]] + t2 if sgn == 1 else new[..., v["e"]] - t2
+    return new
+
+
+@pytest.mark.parametrize("nx,ndir", [((30,), 2), ((30,), 3), ((14, 12), 2), ((14, 12), 3), ((10, 9, 8), 3)])
+def test_resistive_source_step_matches_numpy(nx, ndir):
+    types = ["cont", "fixed", "periodic", "periodic", "cont", "symm"][: 2 * len(nx)]
+    P = problems.random_problem(nx, ndir=ndir, seed=34, types=types, user=params.USR_NONE,
+                                typeadvance="onestep")
+    eta = 0.02
+    P.params.eta = eta
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    qdt = 0.011
+    o.advect(qdt, 0.0, 0, method="source")
+    got = _util.mesh(P, o.download()) - _util.mesh(P, w0)
+    want = _resist_step(P, w0, qdt, eta) - _util.mesh(P, w0)
+    nadv = 2 * P.ndir + 2
+    scale = np.abs(want[..., :nadv]).max()
+    assert scale > 1e-6  # the source acts
+    # the ghost-layer cell widths come from the oracle's own extrapolation of x
+    # (gridsetup1), equal to the generator's to rounding
+    np.testing.assert_allclose(got[..., :nadv], want[..., :nadv], rtol=0, atol=1e-12 * scale)
+
+
+def test_resistive_dt_limit():
+    P = problems.random_problem((14, 12), seed=35, types=["cont", "cont", "periodic", "periodic"],
+                                user=params.USR_NONE)
+    o = _util.start(Oracle, P)
+    dt0 = o.getdt(0)
+    P.params.eta = 0.5
+    o = _util.start(Oracle, P)
+    dt1 = o.getdt(0)
+    x = P.x
+    mn = min(float((0.5 * (_view(P, x[..., d], d, 1) - _view(P, x[..., d], d, -1))).min()) for d in range(P.ndim))
+    want = min(dt0, P.params.dtdiffpar * mn * mn / 0.5)
+    assert want < dt0  # the diffusion limit decides
+    np.testing.assert_allclose(dt1, want, rtol=1e-14)
+
+
+def test_negative_eta_is_rejected():
+    from sac_b200 import abi
+    P = problems.random_problem((14, 12), seed=36, types=["cont", "cont", "periodic", "periodic"])
+    P.params.eta = -0.1
+    o = _util.start(Oracle, P)
+    with pytest.raises(abi.SacError):
+        o.getdt(0)
+    with pytest.raises(abi.SacError):
+        o.advect(0.01, 0.0, 0)
