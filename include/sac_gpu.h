@@ -75,7 +75,9 @@ typedef struct sac_params {
   /* equation parameters eqpar(1:neqpar+nspecialpar), src/vacpar.t.mhd:26,
    * src/vacusrpar.f:3-6 */
   double gamma;   /* eqpar(gamma_) */
-  double eta;     /* eqpar(eta_): must be 0 (resistive module off, -off=resist) */
+  double eta;     /* eqpar(eta_): 0, or a constant resistivity > 0 (addsource_res2 with
+                   * compactres=F and getdt_res, src/vacphys.mhdres.t); eta < 0 (a user
+                   * specialeta) is SAC_ERR_UNSUPPORTED */
   double grav[3]; /* eqpar(grav1_..grav3_) */
   double nu;      /* eqpar(nu_): hyperdiffusion on when |nu|>smalldouble */
   /* &paramlist, src/vacio.t:47 */
@@ -87,7 +89,9 @@ typedef struct sac_params {
   char typeadvance[SAC_LENTYPE + 1]; /* onestep|twostep|threestep|fourstep|sterck|jameson */
   char typepred[SAC_LENTYPE + 1];    /* predictor of 'twostep': 'nul' or 'cd4' */
   int sourceunsplit;                 /* sources added inside centdiff4 (par/DEFAULT:44) */
-  int divbfix;                       /* Powell source; only 0 is implemented */
+  int divbfix;                       /* Powell div B source (addsource_divb, src/vacphys.mhd0.t:263-297),
+                                      * added when ndim > 1 and sourceunsplit.  par/DEFAULT:46 sets T;
+                                      * sac_default_params leaves 0, as the reference's 3D pars do */
   /* plug-in */
   int user;            /* SAC_USR_* */
   /* driver parameters.  SAC_USR_STRAT: [0]=amplitude A, [1]=omega, [2],[3]=driver
@@ -190,7 +194,8 @@ sac_status sac_getdt_static(sac_ctx* c, double* dt, int it);
  * vac run: the same parameters (sac_params, shared), its own mesh nx(ndim) with
  * two ghost layers per side, its own coordinates and state.  Boundary types that
  * store ghost values (fixed, fixed1, grad1) and the Slog driver are not available
- * here (SAC_ERR_UNSUPPORTED); the Gaussian drivers (strat, tube) take their
+ * here (SAC_ERR_UNSUPPORTED), nor is resistivity (eta != 0); the Powell source
+ * (divbfix) is, for ndim = 2.  The Gaussian drivers (strat, tube) take their
  * amplitude and frequency per instance (sac_batch_set_driver).
  *
  * Host arrays are the instances' Fortran-order blocks one after another:

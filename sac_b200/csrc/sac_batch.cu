@@ -268,6 +268,7 @@ Stage2Args stage_base(sac_batch* b) {
     for (int s = 0; s < 2; ++s) a.zero1[d][s] = b->zero1[d][s];
   a.grav_on = (b->par.sourceunsplit && grav_mod(b->par.user)) ? 1 : 0;
   a.visc_on = (b->par.sourceunsplit && visc_on_b(b)) ? 1 : 0;
+  a.divb_on = (b->par.sourceunsplit && b->par.divbfix && b->ndim > 1) ? 1 : 0;  // src/vacphys.mhd0.t:255
   a.driver = DRV_NONE;
   if (b->par.sourceunsplit && b->drv)
     a.driver = b->par.user == SAC_USR_STRAT ? DRV_STRAT : DRV_TUBE;  // amplitude and omega per instance
@@ -408,6 +409,7 @@ sac_status sac_batch_create(const sac_params* p, int ndim, int ndir, int ninst, 
   if (std::string(p->typeadvance) != "fourstep") return SAC_ERR_UNSUPPORTED;
   if (p->precision != SAC_PREC_FP64 && p->precision != SAC_PREC_FP32) return SAC_ERR_UNSUPPORTED;
   if (p->user == SAC_USR_SLOG || (p->user == SAC_USR_TUBE && ndim < 2)) return SAC_ERR_UNSUPPORTED;
+  if (p->eta != 0.0) return SAC_ERR_UNSUPPORTED;  // resistivity runs on the single-grid path only
   sac_batch* b = new sac_batch();
   b->par = *p;
   b->dev = p->device;

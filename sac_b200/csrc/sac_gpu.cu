@@ -258,6 +258,11 @@ sac_status advect1_t(sac_ctx* c, const std::string& method, double qdt, int dmin
       for (int s2 = 0; s2 < 2; ++s2) a.zero1[d][s2] = c->zero1[d][s2];
     a.grav_on = (c->par.sourceunsplit && grav_module(u)) ? 1 : 0;
     a.visc_on = visc ? 1 : 0;
+    // addsource (src/vacphys.mhd0.t:225-258): resistivity when |eta| > smalldouble,
+    // Powell's term when divbfix is set, compiled out of 1D builds ({^NOONED}, :255)
+    a.res_on = (c->par.sourceunsplit && std::fabs(c->par.eta) > smalldouble) ? 1 : 0;
+    a.eta = c->par.eta;
+    a.divb_on = (c->par.sourceunsplit && c->par.divbfix && g.ndim > 1) ? 1 : 0;
     a.driver = DRV_NONE;
     if (c->par.sourceunsplit && c->drv) {
       if (u == SAC_USR_SLOG && g.ndim == 3) {
@@ -790,7 +795,10 @@ static sac_status getdt_impl(sac_ctx* c, double* dt, int it, bool static_scratch
         return fail(c, SAC_ERR_NONFINITE, "non-finite wave speed in getdt_courant");
       if (courantmax > smalldouble) d = std::min(d, c->par.courantpar / courantmax);
     }
-    if (c->par.eta != 0.0) return fail(c, SAC_ERR_UNSUPPORTED, "Resistive MHD module is OFF (eta must be 0)");
+    if (c->par.eta < 0.0) return fail(c, SAC_ERR_UNSUPPORTED, "eta < 0 needs a user specialeta");
+    // getdt_res, src/vacphys.mhdres.t:5-45: dtdiffpar*minval(dx(ixM,1:ndim))**2/eta,
+    // with dtdiffpar as getdt_visc may have overwritten it at an earlier call
+    if (c->par.eta > 0.0) d = std::min(d, c->par.dtdiffpar * (c->mindx_all * c->mindx_all) / c->par.eta);
     const int u = c->par.user;
     if (grav_module(u)) {  // getdt_special of the Slog/gravity user files
       if (visc_on(c)) {    // getdt_visc, src/vacusr.viscosity.t:509-542
@@ -839,6 +847,7 @@ sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmi
   while (!m.empty() && (m.back() == ' ' || m.back() == '\0')) m.pop_back();
   if (m != "cd4" && m != "source" && m != "nul") return fail(c, SAC_ERR_UNSUPPORTED, "method " + m);
   if (idimmin < 1 || idimmax > g.ndim || idimmin > idimmax) return fail(c, SAC_ERR_ARG, "idim range");
+  if (c->par.eta < -smalldouble) return fail(c, SAC_ERR_UNSUPPORTED, "eta < 0 needs a user specialeta");
   unsigned mask = 0;
   if (iws) {
     const int n = iws[g.nw];

@@ -191,8 +191,27 @@ __device__ __forceinline__ void nu_cell(const Stage2Args& a, const Geom& g, cons
   }
 }
 
+// optional source terms of the update, compiled in per instantiation so that the
+// default stage carries none of their registers
+enum StageOpt { OPT_DIVB = 1, OPT_RES = 2 };
+
+// Levi-Civita symbol of 0-based indices (lvc, src/vacdef.t:91)
+__host__ __device__ constexpr int lvc3(int i, int j, int k) {
+  return (i == j || j == k || i == k) ? 0 : ((i + 1) % 3 == j ? 1 : -1);
+}
+// getcurrent's idirmin (0-based): the lowest current component with a term
+// eps_ijk d_j B_k, j < ndim, k < ndir (3: none, as for ndir = 1)
+__host__ __device__ constexpr int res_idirmin(int ndim, int ndir) {
+  int m = 3;
+  for (int i = 2; i >= (6 - 2 * ndir > 0 ? 6 - 2 * ndir : 0); --i)
+    for (int j = 0; j < ndim; ++j)
+      for (int k = 0; k < ndir; ++k)
+        if (lvc3(i, j, k) != 0) m = i;
+  return m;
+}
+
 // k_update body at the mesh cell pos
-template <int NDIM, int NDIR, typename S>
+template <int NDIM, int NDIR, typename S, int OPT>
 __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, const Offs& o, const int pos[3],
                                             double qdt_d, double qdt2_d, double tdep, double drvA,
                                             double& numax_out) {
@@ -425,6 +444,101 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
       }
     }
 
+    // --- addsource (src/vacphys.mhd0.t:225-258) after specialsource, as addsource2
+    // orders them (src/vac.t:569-571): the resistive term, then Powell's; both
+    // read wCT only
+    // b + bg at cell n, summed in FP64
+    auto Bat = [&](int C, int n) { return (T)((double)ld(W(B0 + 1 + C), n) + __ldg(BG(2 + C) + n)); };
+
+    // --- resistivity, addsource_res2 (src/vacphys.mhdres.t:231-301), constant eta ------
+    // J = curl(b+bg) by getcurrent (:48-95) at the 2*ndim face neighbours, with the
+    // module's gradient -(q(+1)-q(-1))/dx/2 (:304-317); each term is that gradient of
+    // J eta qdt (b) or of B J eta qdt (e) on the mesh.  Walking the neighbour
+    // direction d outermost keeps the reference's order of additions: d is jdir of
+    // the b loop and idir of the e loop.
+    if constexpr ((OPT & OPT_RES) != 0) {
+      constexpr int IDM = res_idirmin(NDIM, NDIR);
+      if constexpr (IDM < 3) {
+        const T eta = (T)a.eta;
+        auto curr = [&](int n, T J[3]) {
+#pragma unroll
+          for (int i = IDM; i < 3; ++i) {
+            J[i] = T(0);
+#pragma unroll
+            for (int j = 0; j < NDIM; ++j)
+#pragma unroll
+              for (int k = 0; k < NDIR; ++k) {
+                const int l = lvc3(i, j, k);
+                if (l == 0) continue;
+                const int sj = st[j];
+                const T dxn = (T)__ldg(a.fDX[j] + o.X + n);
+                const T gr = -(Bat(k, n + sj) - Bat(k, n - sj)) / dxn / T(2);
+                J[i] = (l == 1) ? J[i] + gr : J[i] - gr;
+              }
+          }
+        };
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+          const int s = st[d];
+          T Jp[3], Jm[3];
+          curr(c + s, Jp);
+          curr(c - s, Jm);
+          const T dxd = dxv[d];
+#pragma unroll
+          for (int i = 0; i < NDIR; ++i) {
+            if (!((a.iwmask >> (B0 + 1 + i)) & 1u)) continue;
+#pragma unroll
+            for (int k = IDM; k < 3; ++k) {
+              const int l = lvc3(i, d, k);
+              if (l == 0) continue;
+              const T gr = -(Jp[k] * eta * q2 - Jm[k] * eta * q2) / dxd / T(2);
+              acc[B0 + 1 + i] = (l == 1) ? acc[B0 + 1 + i] - gr : acc[B0 + 1 + i] + gr;
+            }
+          }
+          if ((a.iwmask >> E) & 1u) {
+#pragma unroll
+            for (int j = 0; j < NDIR; ++j) {
+#pragma unroll
+              for (int k = IDM; k < 3; ++k) {
+                const int l = lvc3(d, j, k);
+                if (l == 0) continue;
+                const T up = Bat(j, c + s) * Jp[k] * eta * q2, um = Bat(j, c - s) * Jm[k] * eta * q2;
+                const T gr = -(up - um) / dxd / T(2);
+                acc[E] = (l == 1) ? acc[E] + gr : acc[E] - gr;
+              }
+            }
+          }
+        }
+      }
+    }
+
+    // --- Powell div B source, addsource_divb (src/vacphys.mhd0.t:263-297) ----------------
+    // div B is getdivb's sum over every dimension of gradient4(b+bg) (:106-144)
+    if constexpr (NDIM > 1 && (OPT & OPT_DIVB) != 0) {
+      T divb = T(0);
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) {
+        T gd = T(0);
+        if (!z4[d]) {
+          const int s = st[d];
+          gd = -(Bat(d, c + 2 * s) - T(8) * (Bat(d, c + s) - Bat(d, c - s)) - Bat(d, c - 2 * s)) / dxv[d] / T(12);
+        }
+        divb = divb + gd;
+      }
+      divb = q2 * divb;
+      const T rt = ld(Df(0), c);
+      T sm = T(0);
+#pragma unroll
+      for (int C = 0; C < NDIR; ++C) {
+        const T mC = ld(W(1 + C), c);
+        const T BC = Bat(C, c);
+        if ((a.iwmask >> (1 + C)) & 1u) acc[1 + C] = acc[1 + C] - BC * divb;
+        if ((a.iwmask >> (B0 + 1 + C)) & 1u) acc[B0 + 1 + C] = acc[B0 + 1 + C] - mC / rt * divb;
+        sm = (C == 0) ? mC * BC : sm + mC * BC;
+      }
+      if ((a.iwmask >> E) & 1u) acc[E] = acc[E] - sm / rt * divb;
+    }
+
     // --- store with the Runge-Kutta epilogue (src/vac.t:450,454) ---------------------
     S* out = (S*)a.out + o.P;
     if (a.epi == EPI_PLAIN) {
@@ -518,7 +632,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_NU_MINB_F64 : SAC_NU
 #define SAC_UPDATE_MINB_F32 8
 #endif
 
-template <int NDIM, int NDIR, typename S>
+template <int NDIM, int NDIR, typename S, int OPT>
 __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_UPDATE_MINB_F64 : SAC_UPDATE_MINB_F32)
     k_update(const Stage2Args a) {
   __shared__ double sh[32];
@@ -529,7 +643,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_UPDATE_MINB_F64 : SA
   pos[2] = g.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
   double numax = 0.0;
   if (pos[0] <= g.hi[0] && pos[1] <= g.hi[1] && pos[2] <= g.hi[2])
-    update_cell<NDIM, NDIR, S>(a, g, Offs{0, 0, 0, 0}, pos, a.qdt, a.qdt2, a.tdep, a.drvA, numax);
+    update_cell<NDIM, NDIR, S, OPT>(a, g, Offs{0, 0, 0, 0}, pos, a.qdt, a.qdt2, a.tdep, a.drvA, numax);
   if (a.visc_on) block_max_to(a.maxnu, numax, sh);
 }
 
@@ -600,7 +714,7 @@ __global__ void __launch_bounds__(256) kb_nu(const BatchStageArgs b) {
   }
 }
 
-template <int NDIM, int NDIR, typename S>
+template <int NDIM, int NDIR, typename S, int OPT>
 __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_BATCH_UPDATE_MINB_F64 : SAC_BATCH_UPDATE_MINB_F32)
     kb_update(const BatchStageArgs b) {
   __shared__ double sh[32];
@@ -618,7 +732,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_BATCH_UPDATE_MINB_F6
       const double qdt = b.stage == 0 ? dt / 2 : b.stage == 1 ? dt / 2 : b.stage == 2 ? dt : dt / 6;
       const double qdt2 = qdt * ((double)(b.a.dmax - b.a.dmin) + 1.0) / (double)g.ndim;
       const double tdep = b.a.driver != DRV_NONE ? sin(omega * tnow) : 0.0;
-      update_cell<NDIM, NDIR, S>(b.a, g, I.o, p, qdt, qdt2, tdep, drvA, numax);
+      update_cell<NDIM, NDIR, S, OPT>(b.a, g, I.o, p, qdt, qdt2, tdep, drvA, numax);
     }
     if (b.a.visc_on) block_max_to(&b.dyn[tl.inst].maxnu, numax, sh);
   }
@@ -719,7 +833,27 @@ void launch_update(const Stage2Args& a0, cudaStream_t st) {
     dim3 blk = NDIM == 1 ? dim3(256, 1, 1) : (NDIM == 2 ? dim3(32, 8, 1) : dim3(32, 4, 2));
     const int n0 = g.hi[0] - g.lo[0] + 1, n1 = g.hi[1] - g.lo[1] + 1, n2 = g.hi[2] - g.lo[2] + 1;
     dim3 grd((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, (n2 + blk.z - 1) / blk.z);
-    k_update<NDIM, decltype(NR)::value, S><<<grd, blk, 0, st>>>(a);
+    constexpr int NDIR = decltype(NR)::value;
+    // the optional sources present for this shape: Powell's needs ndim > 1, the
+    // resistive one a current component (ndir > 1)
+    const int opt = ((NDIM > 1 && a.divb_on) ? OPT_DIVB : 0) | ((NDIR > 1 && a.res_on) ? OPT_RES : 0);
+    if constexpr (NDIM > 1) {
+      if (opt == OPT_DIVB) {
+        k_update<NDIM, NDIR, S, OPT_DIVB><<<grd, blk, 0, st>>>(a);
+        return;
+      }
+      if (opt == (OPT_DIVB | OPT_RES)) {
+        k_update<NDIM, NDIR, S, OPT_DIVB | OPT_RES><<<grd, blk, 0, st>>>(a);
+        return;
+      }
+    }
+    if constexpr (NDIR > 1) {
+      if (opt == OPT_RES) {
+        k_update<NDIM, NDIR, S, OPT_RES><<<grd, blk, 0, st>>>(a);
+        return;
+      }
+    }
+    k_update<NDIM, NDIR, S, 0><<<grd, blk, 0, st>>>(a);
   });
 }
 
@@ -759,7 +893,16 @@ void launch_batch_update(const BatchStageArgs& b0, dim3 blk, cudaStream_t st) {
   fill_field_ptrs(b.a, sizeof(S));
   if (!b.ntiles) return;
   dispatch_nd(b.a.g, [&](auto ND, auto NR) {
-    kb_update<decltype(ND)::value, decltype(NR)::value, S><<<persistent_grid(b.ntiles, 2), blk, 0, st>>>(b);
+    // the batch has no resistivity (rejected at creation); Powell's term for ndim > 1
+    constexpr int NDIM = decltype(ND)::value;
+    const unsigned grid = persistent_grid(b.ntiles, 2);
+    if constexpr (NDIM > 1) {
+      if (b.a.divb_on) {
+        kb_update<NDIM, decltype(NR)::value, S, OPT_DIVB><<<grid, blk, 0, st>>>(b);
+        return;
+      }
+    }
+    kb_update<NDIM, decltype(NR)::value, S, 0><<<grid, blk, 0, st>>>(b);
   });
 }
 

@@ -47,6 +47,9 @@ struct Stage2Args {
   unsigned iwmask;
   int zero1[3][2];
   int grav_on, visc_on, driver, epi;
+  int divb_on;            // Powell div B source (divbfix, ndim > 1)
+  int res_on;             // resistive source with the constant eta below
+  double eta;
   // per-field base pointers (filled by fill_field_ptrs), so that a load is one
   // pointer from parameter space plus the cell offset
   const void* fF[3][8];   // F[d][iw]

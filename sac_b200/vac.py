@@ -27,7 +27,7 @@ DEFAULT_PAR = """
  &savelist /
  &stoplist itmax=1000000 tmax=1.D99 tmaxexact=F dtmin=1.D-99 residmin=0.D0 residmax=1.D99 /
  &methodlist typeadvance='twostep' dimsplit=T typedimsplit='default' sourcesplit=F sourceunsplit=T
-    typesourcesplit='default' divbfix=T smallfix=F /
+    typesourcesplit='default' divbfix=T smallfix=F compactres=F /
  &boundlist extraB=F /
  &paramlist courantpar=0.8D0 dtcantgrow=F dtdiffpar=0.5D0 dtpar=-1.D0 slowsteps=0 /
 """
@@ -144,13 +144,21 @@ class Run:
         self.dimsplit = tds != "unsplit"
         if bool(g("methodlist", "sourcesplit", False)):
             raise NotImplementedError("sourcesplit=T is outside the implemented path")
+        # the Powell source is on by default (par/DEFAULT:46) and needs unsplit
+        # sources here, since split sources are not built (src/vacio.t:357-359)
+        divbfix = bool(g("methodlist", "divbfix", True))
+        sourceunsplit = bool(g("methodlist", "sourceunsplit", True))
+        if divbfix and not sourceunsplit:
+            raise ValueError("divbfix=T requires unsplitsource=T or splitsource=T !")
+        if bool(g("methodlist", "compactres", False)):
+            raise NotImplementedError("compactres=T (addsource_res1) is outside the implemented path")
         ep = eqpar_map(snap.eqpar, snap.varnames.split(), ndim)
         self.params = params.make_params(
             gamma=ep["gamma"], eta=ep["eta"], grav=ep["grav"], nu=ep["nu"],
             courantpar=float(g("paramlist", "courantpar", 0.8)), dtpar=float(g("paramlist", "dtpar", -1.0)),
             dtdiffpar=float(g("paramlist", "dtdiffpar", 0.5)), dtcantgrow=int(bool(g("paramlist", "dtcantgrow", False))),
-            typeadvance=typeadvance, typepred=pred, sourceunsplit=int(bool(g("methodlist", "sourceunsplit", True))),
-            divbfix=0, user=USER[user], device=device)
+            typeadvance=typeadvance, typepred=pred, sourceunsplit=int(sourceunsplit),
+            divbfix=int(divbfix), user=USER[user], device=device)
         self.slowsteps = int(g("paramlist", "slowsteps", 0))
         self.types = params.typeB_from_par(pf, nw, 2 * ndim)
         self.wnames = g("methodlist", "wnames", snap.varnames)

@@ -94,6 +94,31 @@ def test_gravity_viscosity_mixed_bounds_2d():
     _check(Ps, b, 12, RTOL)
 
 
+def _divb_problems(dtpar=None):
+    types = ["cont", "cont1", "periodic", "periodic"]
+    Ps = [problems.random_problem(n, seed=s, types=types) for n, s in (((14, 12), 4), ((20, 10), 5))]
+    prm = Ps[0].params
+    prm.divbfix = 1
+    if dtpar is not None:
+        prm.dtpar = dtpar
+    for P in Ps:
+        P.params = prm
+    return Ps, prm
+
+
+def test_divbfix_2d_fp64():
+    Ps, prm = _divb_problems()
+    _check(Ps, _batch_of(Ps, prm), 12, RTOL)
+
+
+def test_divbfix_2d_fp32():
+    Ps, prm = _divb_problems(dtpar=2.0e-3)
+    prm.precision = params.PREC_FP32
+    b = _batch_of(Ps, prm)  # the batch keeps its own copy of the parameters
+    prm.precision = params.PREC_FP64
+    _check(Ps, b, 10, FP32_RTOL)
+
+
 def test_1d_instances():
     Ps = [problems.random_problem((n,), ndir=2, seed=n, types=["cont", "symm"]) for n in (40, 64, 33)]
     prm = Ps[0].params
@@ -148,6 +173,10 @@ def test_unsupported_options_are_errors():
     from sac_b200 import abi
     prm = batch.ot_params()
     prm.typeadvance = b"twostep"
+    with pytest.raises(abi.SacError):
+        batch.Batch(prm, 2, 2, [(16, 16)])
+    prm = batch.ot_params()
+    prm.eta = 0.01  # resistivity runs on the single-grid path only
     with pytest.raises(abi.SacError):
         batch.Batch(prm, 2, 2, [(16, 16)])
     prm = batch.ot_params()

@@ -127,6 +127,75 @@ def test_source_method_only():
     _compare(P, o, g)
 
 
+# Powell's div B source (divbfix), src/vacphys.mhd0.t:263-297
+@pytest.mark.parametrize("ndir", [2, 3])
+def test_divbfix_random_2d(ndir):
+    P = problems.random_problem((20, 16), ndir=ndir, seed=41, types=["cont", "fixed", "periodic", "periodic"])
+    P.params.divbfix = 1
+    _steps(P, 100)
+
+
+def test_divbfix_random_3d():
+    P = problems.random_problem((12, 10, 8), seed=42, types=["fixed", "cont", "periodic", "periodic", "cont", "symm"])
+    P.params.divbfix = 1
+    _steps(P, 100)
+
+
+def test_divbfix_stratified_driver():
+    P = problems.stratified(n=(16, 12, 12), amp=0.05)
+    P.params.divbfix = 1
+    _steps(P, 50)
+
+
+def test_divbfix_source_method_and_splitting():
+    P = problems.random_problem((16, 12), seed=43, types=["cont", "cont", "periodic", "periodic"])
+    P.params.divbfix = 1
+    o, g = _pair(P)
+    for k in range(3):
+        o.advect(0.01, 0.01 * k, k, method="source")
+        g.advect(0.01, 0.01 * k, k, method="source")
+    _compare(P, o, g)
+    _util.run(o, 10, t0=0.03, it0=3, idim=[1, 2])
+    _util.run(g, 10, t0=0.03, it0=3, idim=[1, 2])
+    _compare(P, o, g)
+
+
+# constant resistivity (addsource_res2 and getdt_res, src/vacphys.mhdres.t)
+@pytest.mark.parametrize("nx,ndir", [((40,), 2), ((40,), 3), ((20, 16), 2), ((20, 16), 3), ((12, 10, 8), 3)])
+def test_resistive_random(nx, ndir):
+    types = ["cont", "fixed", "periodic", "periodic", "cont", "symm"][: 2 * len(nx)]
+    P = problems.random_problem(nx, ndir=ndir, seed=44, types=types)
+    P.params.eta = 0.01
+    _steps(P, 100)
+
+
+def test_resistive_with_divbfix_3d():
+    P = problems.random_problem((12, 10, 8), seed=45, types=["cont", "cont", "periodic", "periodic", "fixed", "cont"])
+    P.params.eta = 0.01
+    P.params.divbfix = 1
+    _steps(P, 100)
+
+
+def test_resistive_source_method():
+    P = problems.random_problem((16, 12), ndir=3, seed=46, types=["cont", "cont", "periodic", "periodic"])
+    P.params.eta = 0.05
+    o, g = _pair(P)
+    for k in range(3):
+        o.advect(0.01, 0.01 * k, k, method="source")
+        g.advect(0.01, 0.01 * k, k, method="source")
+    _compare(P, o, g)
+
+
+def test_negative_eta_is_an_error():
+    P = problems.random_problem((12, 10), seed=47, types=["cont", "cont", "periodic", "periodic"])
+    P.params.eta = -0.01
+    g = _util.start(abi.Context, P)
+    with pytest.raises(abi.SacError):
+        g.getdt(0)
+    with pytest.raises(abi.SacError):
+        g.advect(0.01, 0.0, 0)
+
+
 def test_diag_matches_oracle():
     P = problems.random_problem((12, 10, 8), seed=6, types=["cont", "cont", "periodic", "periodic", "cont", "cont"])
     o, g = _pair(P)
@@ -167,6 +236,19 @@ def test_fp32_stratified_3d():
 
 def test_fp32_random_2d():
     _fp32_steps(problems.random_problem((20, 16), seed=5, types=["cont", "fixed", "periodic", "periodic"]), 100)
+
+
+def test_fp32_divbfix_2d():
+    P = problems.random_problem((20, 16), seed=41, types=["cont", "fixed", "periodic", "periodic"])
+    P.params.divbfix = 1
+    _fp32_steps(P, 100)
+
+
+def test_fp32_resistive_3d():
+    P = problems.random_problem((12, 10, 8), seed=45, types=["cont", "cont", "periodic", "periodic", "fixed", "cont"])
+    P.params.eta = 0.01
+    P.params.divbfix = 1
+    _fp32_steps(P, 100)
 
 
 def test_fp32_zero_perturbation_stays_zero():
