@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 INI = os.path.join(HERE, "golden", "briowu-test12_np01_000.ini")
 
 
-def _par(tmp, tag, itmax=20):
+def _par(tmp, tag, itmax=20, method=""):
     return f"""
  &filelist filenameini='{INI}'
     filename='{tmp}/{tag}.log', '{tmp}/{tag}.out'
@@ -23,7 +23,7 @@ def _par(tmp, tag, itmax=20):
  &savelist itsave(1,2)=0 ditsave=5,5 /
  &stoplist itmax={itmax} /
  &methodlist wnames='rhop m1 m2 Ep b1p b2p rhob Eb b1b b2b'
-    typefull=6*'cd4',4*'nul' typeadvance='fourstep' /
+    typefull=6*'cd4',4*'nul' typeadvance='fourstep' {method} /
  &boundlist typeB=40*'cont' /
  &paramlist courantpar=0.8 /
 """
@@ -40,6 +40,18 @@ def test_driver_on_the_oracle_writes_the_schedule(tmp_path):
     assert [s.it for s in snaps] == [0, 5, 10, 15, 20]
     log = open(tmp_path / "o.log").read().splitlines()
     assert len(log) >= 5 and np.isfinite(snaps[-1].w).all()
+
+
+def test_source_switches_follow_the_par(tmp_path):
+    # divbfix defaults to T (par/DEFAULT:46) and needs unsplit sources
+    # (src/vacio.t:357-359); compactres=T selects addsource_res1, not built
+    assert vac.Run(_par(tmp_path, "a"), context=Oracle).params.divbfix == 1
+    assert vac.Run(_par(tmp_path, "b", method="divbfix=F"), context=Oracle).params.divbfix == 0
+    with pytest.raises(ValueError):
+        vac.Run(_par(tmp_path, "c", method="sourceunsplit=F"), context=Oracle)
+    assert vac.Run(_par(tmp_path, "d", method="sourceunsplit=F divbfix=F"), context=Oracle).params.sourceunsplit == 0
+    with pytest.raises(NotImplementedError):
+        vac.Run(_par(tmp_path, "e", method="compactres=T"), context=Oracle)
 
 
 @pytest.mark.gpu
