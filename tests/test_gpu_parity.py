@@ -186,6 +186,15 @@ def test_resistive_source_method():
     _compare(P, o, g)
 
 
+@pytest.mark.parametrize("kind", ["zero", "special"])
+def test_unbuilt_boundary_types_are_errors(kind):
+    P = problems.random_problem((12, 10), seed=48, types=[kind, "cont", "periodic", "periodic"])
+    g = abi.Context(P.params)
+    g.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
+    with pytest.raises(abi.SacError):
+        g.set_boundaries(P.typeB_packed, P.nB)
+
+
 def test_negative_eta_is_an_error():
     P = problems.random_problem((12, 10), seed=47, types=["cont", "cont", "periodic", "periodic"])
     P.params.eta = -0.01
