@@ -632,6 +632,19 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_NU_MINB_F64 : SAC_NU
 #define SAC_UPDATE_MINB_F32 8
 #endif
 
+// the 3D update's block shape per storage type (256 threads; x along the
+// contiguous dimension)
+#ifndef SAC_UPDATE_BLK3_F64_X
+#define SAC_UPDATE_BLK3_F64_X 8
+#define SAC_UPDATE_BLK3_F64_Y 8
+#define SAC_UPDATE_BLK3_F64_Z 4
+#endif
+#ifndef SAC_UPDATE_BLK3_F32_X
+#define SAC_UPDATE_BLK3_F32_X 32
+#define SAC_UPDATE_BLK3_F32_Y 4
+#define SAC_UPDATE_BLK3_F32_Z 2
+#endif
+
 template <int NDIM, int NDIR, typename S, int OPT>
 __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_UPDATE_MINB_F64 : SAC_UPDATE_MINB_F32)
     k_update(const Stage2Args a) {
@@ -830,7 +843,10 @@ void launch_update(const Stage2Args& a0, cudaStream_t st) {
   const Geom& g = a.g;
   dispatch_nd(g, [&](auto ND, auto NR) {
     constexpr int NDIM = decltype(ND)::value;
-    dim3 blk = NDIM == 1 ? dim3(256, 1, 1) : (NDIM == 2 ? dim3(32, 8, 1) : dim3(32, 4, 2));
+    dim3 blk = NDIM == 1 ? dim3(256, 1, 1)
+                         : (NDIM == 2 ? dim3(32, 8, 1)
+                                      : (sizeof(S) == 8 ? dim3(SAC_UPDATE_BLK3_F64_X, SAC_UPDATE_BLK3_F64_Y, SAC_UPDATE_BLK3_F64_Z)
+                                                        : dim3(SAC_UPDATE_BLK3_F32_X, SAC_UPDATE_BLK3_F32_Y, SAC_UPDATE_BLK3_F32_Z)));
     const int n0 = g.hi[0] - g.lo[0] + 1, n1 = g.hi[1] - g.lo[1] + 1, n2 = g.hi[2] - g.lo[2] + 1;
     dim3 grd((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, (n2 + blk.z - 1) / blk.z);
     constexpr int NDIR = decltype(NR)::value;
