@@ -156,7 +156,9 @@ __device__ __forceinline__ double courant_cell(const Geom& g, const S* __restric
   }
   const double cf2 = Bt2 / rt + cs2;
   double best = 0.0;
-  for (int d = 0; d < g.ndim; ++d) {
+#pragma unroll
+  for (int d = 0; d < NDIR; ++d) {  // ndim <= ndir: unrolled, m and b stay in registers
+    if (d >= g.ndim) break;
     const double Bd = b[d] + bgv[(2 + d) * N + c];
     double cmax = sqrt(0.5 * (cf2 + sqrt(cf2 * cf2 - 4.0 * cs2 * (Bd * Bd) / rt))) + fabs(m[d] / rt);
     double r = cmax / dx[d * N + c];
@@ -173,16 +175,18 @@ __device__ __forceinline__ double max_sticky(double best, double r) {
 
 // k_courant: max over the mesh of courant_cell, one atomic per block
 template <int NDIR, typename S>
-__global__ void k_courant(Geom g, const S* __restrict__ wp, const double* __restrict__ bgv,
+__global__ void k_courant(const __grid_constant__ Geom g, const S* __restrict__ wp, const double* __restrict__ bgv,
                           const double* __restrict__ dx, unsigned long long* out, double gamma) {
   __shared__ double sh[32];
   double best = 0.0;
-  const long nm0 = g.hi[0] - g.lo[0] + 1, nm1 = g.hi[1] - g.lo[1] + 1, nm2 = g.hi[2] - g.lo[2] + 1;
-  const long tot = nm0 * nm1 * nm2;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
-    const int i0 = g.lo[0] + (int)(t % nm0);
-    const int i1 = g.lo[1] + (int)((t / nm0) % nm1);
-    const int i2 = g.lo[2] + (int)(t / (nm0 * nm1));
+  // 32-bit decode: sac_set_grid keeps the grid's cell offsets below 2^31
+  const unsigned nm0 = g.hi[0] - g.lo[0] + 1, nm1 = g.hi[1] - g.lo[1] + 1, nm2 = g.hi[2] - g.lo[2] + 1;
+  const unsigned tot = nm0 * nm1 * nm2;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+    const unsigned q = t / nm0;
+    const int i0 = g.lo[0] + (int)(t - q * nm0);
+    const int i1 = g.lo[1] + (int)(q % nm1);
+    const int i2 = g.lo[2] + (int)(q / nm1);
     best = max_sticky(best, courant_cell<NDIR, S>(g, wp, bgv, dx, i0, i1, i2, gamma));
   }
   block_max_to(out, best, sh);
@@ -218,13 +222,13 @@ struct BcArgs {
   const void* basep;                // w (mode 1)
 };
 
-__device__ __forceinline__ long fix_index(const Geom& g, int d, bool up, const int p[3]) {
-  int q[3] = {p[0], p[1], p[2]};
-  int ext[3];
-  for (int e = 0; e < 3; ++e) ext[e] = (e < g.ndim) ? g.n[e] : 1;
-  ext[d] = g.lo[d];
-  q[d] = up ? p[d] - (g.hi[d] + 1) : p[d];
-  return q[0] + (long)ext[0] * (q[1] + (long)ext[1] * q[2]);
+__device__ __forceinline__ long fix_index(const Geom& g, int d, bool up, int p0, int p1, int p2) {
+  const int e0 = g.ndim > 0 ? g.n[0] : 1, e1 = g.ndim > 1 ? g.n[1] : 1;
+  const int x0 = d == 0 ? g.lo[0] : e0, x1 = d == 1 ? g.lo[1] : e1;  // the slab's extent
+  const int pd = d == 0 ? p0 : (d == 1 ? p1 : p2);
+  const int qd = up ? pd - (g.hi[d] + 1) : pd;
+  const int q0 = d == 0 ? qd : p0, q1 = d == 1 ? qd : p1, q2 = d == 2 ? qd : p2;
+  return q0 + (long)x0 * (q1 + (long)x1 * q2);
 }
 
 template <typename S>
@@ -233,30 +237,33 @@ __device__ __forceinline__ double bc_read(const BcArgs& a, int iw, long c) {
   return iw < np ? (double)((const S*)a.A)[(long)iw * a.sA + a.oA + c] : a.bgA[(long)(iw - np) * a.sB + a.oB + c];
 }
 
-// Value of variable iw at cell p (mesh or ghost).  fixed_leaf/leaf report a chain
-// that ended in a stored fixB value (needed by the RK4 final combination).
+// Value of variable iw at cell (p0,p1,p2) (mesh or ghost).  fixed_leaf/leaf
+// report a chain that ended in a stored fixB value (needed by the RK4 final
+// combination).  The coordinates are scalars, so that replacing the one along
+// the ghost dimension is a select rather than a store to a local array.
 template <int DEPTH, typename S>
-__device__ double bc_resolve(const BcArgs& a, int iw, const int p[3], bool& fixed_leaf, long& leaf) {
-  const long c = p[0] + a.g.st[1] * p[1] + a.g.st[2] * p[2];
+__device__ double bc_resolve(const BcArgs& a, int iw, int p0, int p1, int p2, bool& fixed_leaf, long& leaf) {
+  const long c = p0 + a.g.st[1] * p1 + a.g.st[2] * p2;
   int d = -1;
-  for (int e = 0; e < a.g.ndim; ++e)
-    if (p[e] < a.g.lo[e] || p[e] > a.g.hi[e]) d = e;
+  if (a.g.ndim > 0 && (p0 < a.g.lo[0] || p0 > a.g.hi[0])) d = 0;
+  if (a.g.ndim > 1 && (p1 < a.g.lo[1] || p1 > a.g.hi[1])) d = 1;
+  if (a.g.ndim > 2 && (p2 < a.g.lo[2] || p2 > a.g.hi[2])) d = 2;
   if constexpr (DEPTH == 0) {
     return bc_read<S>(a, iw, c);
   } else {
     if (d < 0) return bc_read<S>(a, iw, c);
-    const bool up = p[d] > a.g.hi[d];
+    const int pd = d == 0 ? p0 : (d == 1 ? p1 : p2);
+    const int lo = a.g.lo[d], hi = a.g.hi[d];
+    const bool up = pd > hi;
     const int iB = 2 * d + (up ? 1 : 0);
     const int nB = 2 * a.g.ndim;
     const int t = a.type[iw * nB + iB];
-    const int edge = up ? a.g.hi[d] : a.g.lo[d];
+    const int edge = up ? hi : lo;
     auto at = [&](int q) {
-      int r[3] = {p[0], p[1], p[2]};
-      r[d] = q;
-      return bc_resolve<DEPTH - 1, S>(a, iw, r, fixed_leaf, leaf);
+      return bc_resolve<DEPTH - 1, S>(a, iw, d == 0 ? q : p0, d == 1 ? q : p1, d == 2 ? q : p2, fixed_leaf, leaf);
     };
     const bool isfixed = a.fixed[iw * nB + iB] != 0;
-    auto fbv = [&]() { return a.fixB[a.fixoff[iB] + (long)iw * a.slab[iB] + fix_index(a.g, d, up, p)]; };
+    auto fbv = [&]() { return a.fixB[a.fixoff[iB] + (long)iw * a.slab[iB] + fix_index(a.g, d, up, p0, p1, p2)]; };
     switch (t) {
       case BT_CONT:
         return at(edge);
@@ -269,15 +276,15 @@ __device__ double bc_resolve(const BcArgs& a, int iw, const int p[3], bool& fixe
         if (a.init && a.fullgridini) return bc_read<S>(a, iw, c);
         return at(edge);
       case BT_PERIODIC:
-        return at(p[d] + a.pairshift[d][up ? 1 : 0]);
+        return at(pd + a.pairshift[d][up ? 1 : 0]);
       case BT_SYMM:
       case BT_SYMM0:
-        return at(up ? 2 * a.g.hi[d] + 1 - p[d] : 2 * a.g.lo[d] - 1 - p[d]);
+        return at(up ? 2 * hi + 1 - pd : 2 * lo - 1 - pd);
       case BT_ASYMM:
-        return -at(up ? 2 * a.g.hi[d] + 1 - p[d] : 2 * a.g.lo[d] - 1 - p[d]);
+        return -at(up ? 2 * hi + 1 - pd : 2 * lo - 1 - pd);
       case BT_CONTCD4: {  // reflection about the edge cell, src/vacgrid.t:261-293
-        const int n = up ? p[d] - a.g.hi[d] : a.g.lo[d] - p[d];
-        return at(up ? a.g.hi[d] - n : a.g.lo[d] + n);
+        const int n = up ? pd - hi : lo - pd;
+        return at(up ? hi - n : lo + n);
       }
       default: {  // cont1, fixed1, grad1, src/vacgrid.t:373-409
         if (isfixed) {
@@ -288,7 +295,7 @@ __device__ double bc_resolve(const BcArgs& a, int iw, const int p[3], bool& fixe
         }
         if (t != BT_CONT1 && a.init && a.fullgridini) return bc_read<S>(a, iw, c);
         const int f = up ? edge - 1 : edge + 1;
-        const int n = abs(p[d] - edge);
+        const int n = abs(pd - edge);
         const double ve = at(edge), vf = at(f);
         return sub_rn(mul_rn((double)(n + 1), ve), mul_rn((double)n, vf));
       }
@@ -313,7 +320,7 @@ __host__ __device__ inline void ghost_slabs(const Geom& g, long ns[3]) {
 // Ghost cells enumerated slab by slab: slab d holds the cells whose highest ghost
 // dimension is d (all coordinates for dims < d, mesh coordinates for dims > d).
 template <typename S>
-__device__ void bound_cell(const BcArgs& a, long t, const long ns[3], int nvar) {
+__device__ void bound_cell(const BcArgs& a, long t, const long ns[3], int iw0, int iw1) {
   const Geom& g = a.g;
   int d;
   long r;
@@ -343,17 +350,21 @@ __device__ void bound_cell(const BcArgs& a, long t, const long ns[3], int nvar) 
       off[e] = 0;
     }
   }
+  // 32-bit decode: a slab holds fewer cells than the grid, whose cell offsets
+  // sac_set_grid keeps below 2^31
+  const unsigned ur = (unsigned)r, e0 = (unsigned)ext[0], e1 = (unsigned)ext[1];
+  const unsigned q0 = ur / e0;
   int p[3];
-  p[0] = (int)(r % ext[0]);
-  p[1] = (int)((r / ext[0]) % ext[1]);
-  p[2] = (int)(r / ((long)ext[0] * ext[1]));
+  p[0] = (int)(ur - q0 * e0);
+  p[1] = (int)(q0 % e1);
+  p[2] = (int)(q0 / e1);
   for (int e = 0; e < 3; ++e) p[e] += off[e];
   if (p[d] >= g.lo[d]) p[d] = g.hi[d] + 1 + (p[d] - g.lo[d]);  // upper layers
   const long c = p[0] + g.st[1] * p[1] + g.st[2] * p[2];
-  for (int iw = 0; iw < nvar; ++iw) {
+  for (int iw = iw0; iw < iw1; ++iw) {
     bool fl = false;
     long leaf = 0;
-    double v = bc_resolve<3, S>(a, iw, p, fl, leaf);
+    double v = bc_resolve<3, S>(a, iw, p[0], p[1], p[2], fl, leaf);
     const bool pert = iw < g.np;
     S* A = (S*)a.A;
     S* w1 = (S*)a.aux1;
@@ -371,12 +382,14 @@ __device__ void bound_cell(const BcArgs& a, long t, const long ns[3], int nvar) 
   }
 }
 
+// __grid_constant__: the resolver takes the parameters by reference, which
+// would otherwise copy the whole struct to each thread's stack
 template <typename S>
-__global__ void k_bound(BcArgs a, long nslab0, long nslab1, long nslab2, int nvar) {
+__global__ void k_bound(const __grid_constant__ BcArgs a, long nslab0, long nslab1, long nslab2, int nvar) {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long ns[3] = {nslab0, nslab1, nslab2};
   if (t >= nslab0 + nslab1 + nslab2) return;
-  bound_cell<S>(a, t, ns, nvar);
+  bound_cell<S>(a, t, ns, 0, nvar);
 }
 
 // batched: persistent CTAs of 256 threads walk the ghost chunks of all instances
@@ -400,7 +413,7 @@ __global__ void __launch_bounds__(256) kb_bound(BcArgs proto, const InstInfo* __
     long ns[3];
     ghost_slabs(a.g, ns);
     const long k = (long)ch.start + threadIdx.x;
-    if (k < ns[0] + ns[1] + ns[2]) bound_cell<S>(a, k, ns, nvar);
+    if (k < ns[0] + ns[1] + ns[2]) bound_cell<S>(a, k, ns, 0, nvar);
   }
 }
 
