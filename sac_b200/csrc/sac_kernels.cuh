@@ -392,24 +392,31 @@ __global__ void k_bound(const __grid_constant__ BcArgs a, long nslab0, long nsla
   bound_cell<S>(a, t, ns, 0, nvar);
 }
 
-// batched: persistent CTAs of 256 threads walk the ghost chunks of all instances
+// batched: persistent CTAs of 256 threads walk the ghost chunks of all instances.
+// The instance's arguments live in shared memory, written once per chunk by one
+// thread: a per-thread copy would put the whole struct on every thread's stack.
 template <typename S>
-__global__ void __launch_bounds__(256) kb_bound(BcArgs proto, const InstInfo* __restrict__ inst,
+__global__ void __launch_bounds__(256) kb_bound(const __grid_constant__ BcArgs proto, const InstInfo* __restrict__ inst,
                                                 const GhostChunk* __restrict__ chunks, int nchunks, int nvar,
                                                 const InstDyn* __restrict__ dyn) {
+  __shared__ BcArgs a;
   for (int t = blockIdx.x; t < nchunks; t += gridDim.x) {
     const GhostChunk ch = chunks[t];
-    if (dyn && dyn[ch.inst].dt == 0.0) continue;  // a finished instance keeps its state
-    BcArgs a = proto;
-    const InstInfo I = inst[ch.inst];
-    a.g = I.g;
-    a.oA = I.o.P;
-    a.oB = I.o.B;
-    for (int d = 0; d < 3; ++d) {  // periodic sources one mesh extent away (src/vacgrid.t:109-120)
-      const int nm = d < a.g.ndim ? a.g.hi[d] - a.g.lo[d] + 1 : 0;
-      a.pairshift[d][0] = nm;
-      a.pairshift[d][1] = -nm;
+    if (dyn && dyn[ch.inst].dt == 0.0) continue;  // a finished instance keeps its state (uniform per block)
+    __syncthreads();  // the previous chunk's readers are done with a
+    if (threadIdx.x == 0) {
+      a = proto;
+      const InstInfo& I = inst[ch.inst];
+      a.g = I.g;
+      a.oA = I.o.P;
+      a.oB = I.o.B;
+      for (int d = 0; d < 3; ++d) {  // periodic sources one mesh extent away (src/vacgrid.t:109-120)
+        const int nm = d < a.g.ndim ? a.g.hi[d] - a.g.lo[d] + 1 : 0;
+        a.pairshift[d][0] = nm;
+        a.pairshift[d][1] = -nm;
+      }
     }
+    __syncthreads();
     long ns[3];
     ghost_slabs(a.g, ns);
     const long k = (long)ch.start + threadIdx.x;
