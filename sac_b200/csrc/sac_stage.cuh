@@ -111,9 +111,11 @@ __device__ __forceinline__ void face_cell(const Stage2Args& a, const Offs& o, in
       }
       const C_ fe = (md * (ptC + C_(0)) - bd * s1 - bgd * s2) / rtC + ebC * md / rtC - bd * s2 / rtC;
       Fw(d, E)[c] = (S)(fe + vd * eC);
+      // b_d has no flux along d (getflux sets transport=.false., src/vacphys.mhd0.t:204-206), and
+      // k_update never reads that slot, so it is not written
 #pragma unroll
       for (int C = 0; C < NDIR; ++C)
-        Fw(d, E + 1 + C)[c] = (C == d) ? (S)0 : (S)(-(vC[C] * (bd + bgd)) + vd * bgC[C] + vd * bC[C]);
+        if (C != d) Fw(d, E + 1 + C)[c] = (S)(-(vC[C] * (bd + bgd)) + vd * bgC[C] + vd * bC[C]);
     }
     if (mesh) {
         // getpthermal, getcsound2, getcmax: src/vacphys0.t.mhd:95-183
