@@ -49,6 +49,7 @@ struct sac_ctx {
   void* D = nullptr;
   void* F = nullptr;
   void* R = nullptr;
+  void* X = nullptr;  // cross-derivative half-sums (k_cross), allocated with hyperdiffusion
   double* x = nullptr;
   double* dx = nullptr;
   double* drv = nullptr;
@@ -174,11 +175,11 @@ bool grav_module(int u) {
 void release(sac_ctx* c) {
   for (auto& p : c->P)
     if (p) cudaFree(p), p = nullptr;
-  for (void* p : {(void*)c->BG, c->D, c->F, c->R, (void*)c->x, (void*)c->dx, (void*)c->drv,
+  for (void* p : {(void*)c->BG, c->D, c->F, c->R, c->X, (void*)c->x, (void*)c->dx, (void*)c->drv,
                   (void*)c->stg, (void*)c->red, (void*)c->fixB, (void*)c->d_type, (void*)c->d_fixed})
     if (p) cudaFree(p);
   c->BG = c->x = c->dx = c->drv = c->stg = c->fixB = nullptr;
-  c->D = c->F = c->R = nullptr;
+  c->D = c->F = c->R = c->X = nullptr;
   c->red = nullptr;
   c->d_type = nullptr;
   c->d_fixed = nullptr;
@@ -240,6 +241,7 @@ sac_status advect1_t(sac_ctx* c, const std::string& method, double qdt, int dmin
     a.D = c->D;
     a.F = c->F;
     a.R = c->R;
+    a.X = c->X;
     a.dx = c->dx;
     a.drv = c->drv;
     a.ctot = c->red;
@@ -282,6 +284,7 @@ sac_status advect1_t(sac_ctx* c, const std::string& method, double qdt, int dmin
     if (visc) {
       Prof pr(c, SAC_K_NU);
       launch_nu<S>(a, c->stream);
+      if (c->X) launch_cross<S>(a, c->stream);
     }
     {
       Prof pr(c, SAC_K_STAGE);
@@ -573,6 +576,8 @@ sac_status sac_set_grid(sac_ctx* c, int ndim, int ndir, const int ixGhi[3], cons
   CK(cudaMalloc(&c->D, c->es * (ndir + 3) * N));
   CK(cudaMalloc(&c->F, c->es * (size_t)ndim * g.np * N));
   CK(cudaMalloc(&c->R, c->es * (size_t)nr_pairs(ndim) * N));
+  if (visc_on(c) && ndim > 1 && c->prec == SAC_PREC_FP64)  // the FP64 update reads them (k_cross)
+    CK(cudaMalloc(&c->X, c->es * (size_t)n_cross(ndim) * N));
   CK(cudaMalloc(&c->x, sizeof(double) * ndim * N));
   CK(cudaMalloc(&c->dx, sizeof(double) * ndim * N));
   if (!hdrv.empty()) CK(cudaMalloc(&c->drv, sizeof(double) * 2 * N));

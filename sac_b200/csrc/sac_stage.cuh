@@ -195,7 +195,9 @@ __device__ __forceinline__ void nu_cell(const Stage2Args& a, const Geom& g, cons
 
 // optional source terms of the update, compiled in per instantiation so that the
 // default stage carries none of their registers
-enum StageOpt { OPT_DIVB = 1, OPT_RES = 2 };
+// OPT_PRE: the cross-derivative half-sums come precomputed from k_cross (the
+// single-grid path); without it the update computes them at both neighbours.
+enum StageOpt { OPT_DIVB = 1, OPT_RES = 2, OPT_PRE = 4 };
 
 // Levi-Civita symbol of 0-based indices (lvc, src/vacdef.t:91)
 __host__ __device__ constexpr int lvc3(int i, int j, int k) {
@@ -360,11 +362,15 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
               const int pl = pos[l] + (sg ? 1 : -1);
               T H = T(0);
               if (pl >= g.lo[l] && pl <= g.hi[l]) {  // nu vanishes outside the mesh
-                const T dxkj = (T)__ldg(a.fDX[k] + o.X + j);
-                T njl, njr;
-                nus(PR::v(l, k), k, j, dxkj, njl, njr);
-                const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
-                H = gC * (njl + njr + T(2) * T(0)) / T(2) / T(2);
+                if constexpr ((OPT & OPT_PRE) != 0) {
+                  H = ld((const S*)a.fX[Cross<NDIM>::m(l, k)] + o.I, j);
+                } else {
+                  const T dxkj = (T)__ldg(a.fDX[k] + o.X + j);
+                  T njl, njr;
+                  nus(PR::v(l, k), k, j, dxkj, njl, njr);
+                  const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
+                  H = gC * (njl + njr + T(2) * T(0)) / T(2) / T(2);
+                }
               }
               Tm[sg] = ld(rtf, j) * H;
               Te[sg] = ld(W(1 + k), j) * H;
@@ -398,11 +404,15 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
               const int pl = pos[l] + (sg ? 1 : -1);
               T Kv = T(0);
               if (pl >= g.lo[l] && pl <= g.hi[l]) {
-                const T dxkj = (T)__ldg(a.fDX[k] + o.X + j);
-                T njl, njr;
-                nus(PR::b(l, k), k, j, dxkj, njl, njr);
-                const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
-                Kv = gC * (njl + njr) / T(2);
+                if constexpr ((OPT & OPT_PRE) != 0) {
+                  Kv = ld((const S*)a.fX[Cross<NDIM>::b(l, k)] + o.I, j);
+                } else {
+                  const T dxkj = (T)__ldg(a.fDX[k] + o.X + j);
+                  T njl, njr;
+                  nus(PR::b(l, k), k, j, dxkj, njl, njr);
+                  const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
+                  Kv = gC * (njl + njr) / T(2);
+                }
               }
               K[sg] = Kv;
               Ke[sg] = Kv * ld(W(B0 + 1 + k), j);
@@ -569,7 +579,8 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
 // ---------------------------------------------------------------------------
 // resident blocks per SM of the face and setnu passes (measured at 128^3, like
 // the update's below: face 1.11 -> 0.82 ms in FP64 at 4 blocks, nu 1.04 -> 0.98
-// ms in FP64 at 6; FP32 setnu is fastest without a bound)
+// ms in FP64 at 6; FP32 setnu is fastest at the 80 registers of 3 blocks, which
+// the compiler chose without a bound until the argument struct grew)
 #ifndef SAC_FACE_MINB_F64
 #define SAC_FACE_MINB_F64 4
 #endif
@@ -580,7 +591,7 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
 #define SAC_NU_MINB_F64 6
 #endif
 #ifndef SAC_NU_MINB_F32
-#define SAC_NU_MINB_F32 1
+#define SAC_NU_MINB_F32 3
 #endif
 
 template <int NDIM, int NDIR, typename S>
@@ -620,6 +631,55 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_NU_MINB_F64 : SAC_NU
   for (int d = 0; d < 3; ++d) p[d] += (d < NDIM) ? g.lo[d] - 1 : 0;
   const int c = p[0] + (int)g.st[1] * p[1] + (int)g.st[2] * p[2];
   nu_cell<NDIM, NDIR, S>(a, g, Offs{0, 0, 0, 0}, c, p, a.ctot);
+}
+
+// k_cross body at the mesh cell pos: for every l != k the centred half-sums of
+// addsource_visc's cross derivatives at this cell, which the update of the cells
+// on either side along l uses (src/vacusr.viscosity.t:117-118 for the momenta,
+// :195-197 for the field) -- the same expressions as the update's inline form
+template <int NDIM, int NDIR, typename S>
+__device__ __forceinline__ void cross_cell(const Stage2Args& a, const Geom& g, const Offs& o, const int pos[3]) {
+  using PR = Pairs<NDIM>;
+  using CR = Cross<NDIM>;
+  using T = S;
+  constexpr int B0 = NDIR + 1;
+  const int st[3] = {1, (int)g.st[1], (int)g.st[2]};
+  const int c = pos[0] + st[1] * pos[1] + st[2] * pos[2];
+#pragma unroll
+  for (int k = 0; k < NDIM; ++k) {
+    const int sk = st[k];
+    const bool z1 = (a.zero1[k][0] && pos[k] == g.lo[k]) || (a.zero1[k][1] && pos[k] == g.hi[k]);
+    const T dxk = (T)__ldg(a.fDX[k] + o.X + c);
+#pragma unroll
+    for (int l = 0; l < NDIM; ++l) {
+      if (l == k) continue;
+      {  // momentum: v_l along k
+        const S* q = (const S*)a.fD[1 + l] + o.I;
+        const S* Qp = (const S*)a.fQ[PR::v(l, k)] + o.I;
+        const T nr = ld(Qp, c) * dxk, nl = ld(Qp, c - sk) * dxk;
+        const T gC = z1 ? T(0) : (ld(q, c + sk) - ld(q, c - sk)) / dxk / T(2);
+        ((S*)a.fX[CR::m(l, k)] + o.I)[c] = gC * (nl + nr + T(2) * T(0)) / T(2) / T(2);
+      }
+      {  // field: b_l along k
+        const S* q = (const S*)a.fW[B0 + 1 + l] + o.P;
+        const S* Qp = (const S*)a.fQ[PR::b(l, k)] + o.I;
+        const T nr = ld(Qp, c) * dxk, nl = ld(Qp, c - sk) * dxk;
+        const T gC = z1 ? T(0) : (ld(q, c + sk) - ld(q, c - sk)) / dxk / T(2);
+        ((S*)a.fX[CR::b(l, k)] + o.I)[c] = gC * (nl + nr) / T(2);
+      }
+    }
+  }
+}
+
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_cross(const Stage2Args a) {
+  const Geom& g = a.g;
+  int pos[3];
+  pos[0] = g.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  pos[1] = g.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  pos[2] = g.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
+  if (pos[0] <= g.hi[0] && pos[1] <= g.hi[1] && pos[2] <= g.hi[2])
+    cross_cell<NDIM, NDIR, S>(a, g, Offs{0, 0, 0, 0}, pos);
 }
 
 // Resident blocks of 256 threads per SM that the register budget is sized for.
@@ -855,23 +915,46 @@ void launch_update(const Stage2Args& a0, cudaStream_t st) {
     // the optional sources present for this shape: Powell's needs ndim > 1, the
     // resistive one a current component (ndir > 1)
     const int opt = ((NDIM > 1 && a.divb_on) ? OPT_DIVB : 0) | ((NDIR > 1 && a.res_on) ? OPT_RES : 0);
+    // the FP64 single grid takes the precomputed cross terms (k_cross runs
+    // whenever hyperdiffusion does; without it the terms are never reached):
+    // measured at 128^3 the update fell from 5.53 to 4.41 ms per step for 0.59
+    // ms of k_cross.  The FP32 update, held to 32 registers, was slower with
+    // them (2.11 -> 2.39 ms) and computes them inline.
+    constexpr int P = sizeof(S) == 8 ? OPT_PRE : 0;
     if constexpr (NDIM > 1) {
       if (opt == OPT_DIVB) {
-        k_update<NDIM, NDIR, S, OPT_DIVB><<<grd, blk, 0, st>>>(a);
+        k_update<NDIM, NDIR, S, P | OPT_DIVB><<<grd, blk, 0, st>>>(a);
         return;
       }
       if (opt == (OPT_DIVB | OPT_RES)) {
-        k_update<NDIM, NDIR, S, OPT_DIVB | OPT_RES><<<grd, blk, 0, st>>>(a);
+        k_update<NDIM, NDIR, S, P | OPT_DIVB | OPT_RES><<<grd, blk, 0, st>>>(a);
         return;
       }
     }
     if constexpr (NDIR > 1) {
       if (opt == OPT_RES) {
-        k_update<NDIM, NDIR, S, OPT_RES><<<grd, blk, 0, st>>>(a);
+        k_update<NDIM, NDIR, S, P | OPT_RES><<<grd, blk, 0, st>>>(a);
         return;
       }
     }
-    k_update<NDIM, NDIR, S, 0><<<grd, blk, 0, st>>>(a);
+    k_update<NDIM, NDIR, S, P><<<grd, blk, 0, st>>>(a);
+  });
+}
+
+template <typename S>
+void launch_cross(const Stage2Args& a0, cudaStream_t st) {
+  Stage2Args a = a0;
+  fill_field_ptrs(a, sizeof(S));
+  const Geom& g = a.g;
+  if (g.ndim < 2 || sizeof(S) != 8) return;  // no pair l != k; FP32 computes them inline
+  dispatch_nd(g, [&](auto ND, auto NR) {
+    constexpr int NDIM = decltype(ND)::value;
+    if constexpr (NDIM > 1) {
+      const dim3 blk = NDIM == 2 ? dim3(32, 8, 1) : dim3(32, 4, 2);
+      const int n0 = g.hi[0] - g.lo[0] + 1, n1 = g.hi[1] - g.lo[1] + 1, n2 = g.hi[2] - g.lo[2] + 1;
+      const dim3 grd((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, (n2 + blk.z - 1) / blk.z);
+      k_cross<NDIM, decltype(NR)::value, S><<<grd, blk, 0, st>>>(a);
+    }
   });
 }
 

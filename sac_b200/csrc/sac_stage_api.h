@@ -24,6 +24,18 @@ struct Pairs {
 
 inline int nr_pairs(int ndim) { return 2 * ndim + ndim * ndim + ndim * (ndim - 1); }
 
+// addsource_visc's cross-derivative pairs (l != k): the centred half-sums of the
+// momentum terms (v_l along k) and of the field terms (b_l along k), stored per
+// cell by k_cross for the single-grid update
+template <int NDIM>
+struct Cross {
+  static constexpr int N = 2 * NDIM * (NDIM - 1);
+  static __host__ __device__ constexpr int m(int l, int k) { return l * (NDIM - 1) + (k < l ? k : k - 1); }
+  static __host__ __device__ constexpr int b(int l, int k) { return NDIM * (NDIM - 1) + m(l, k); }
+};
+
+inline int n_cross(int ndim) { return 2 * ndim * (ndim - 1); }
+
 struct Stage2Args {
   Geom g;
   long sP, sB, sI, sX;  // field strides of the four families
@@ -36,6 +48,7 @@ struct Stage2Args {
   const void* D;     // S[ndir+3][N] rho+rhob, v.., e173, p'_tot
   const void* F;     // S[ndim*np][N] fluxes, F[d*np+iw]
   const void* R;     // S[NR][N]   setnu face quotients
+  const void* X;     // S[n_cross][N] cross-derivative half-sums (single grid), or nullptr
   const double* dx;  // double[ndim][N]
   const double* drv; // driver profiles [2][N] or nullptr
   const unsigned long long* ctot;
@@ -58,6 +71,7 @@ struct Stage2Args {
   const void* fD[6];      // rho+rhob, v.., e173, p'_tot
   const double* fBG[5];   // eb, rhob, bg..
   const double* fDX[3];   // dx per dimension
+  const void* fX[12];     // cross-derivative half-sums per pair
 };
 
 // Fill the per-field pointers of a from its block pointers and family strides
@@ -79,6 +93,7 @@ inline void fill_field_ptrs(Stage2Args& a, size_t es) {
   for (int i = 0; i < 6; ++i) a.fD[i] = (i < g.ndir + 3) ? off(a.D, i, a.sI) : nullptr;
   for (int i = 0; i < 5; ++i) a.fBG[i] = (i < g.nw - g.np) ? a.bgv + (size_t)i * a.sB : nullptr;
   for (int d = 0; d < 3; ++d) a.fDX[d] = (d < g.ndim) ? a.dx + (size_t)d * a.sX : nullptr;
+  for (int i = 0; i < 12; ++i) a.fX[i] = (i < n_cross(g.ndim)) ? off(a.X, i, a.sI) : nullptr;
 }
 
 struct BatchStageArgs {
@@ -96,6 +111,8 @@ template <typename S>
 void launch_nu(const Stage2Args& a, cudaStream_t st);
 template <typename S>
 void launch_update(const Stage2Args& a, cudaStream_t st);
+template <typename S>
+void launch_cross(const Stage2Args& a, cudaStream_t st);
 
 template <typename S>
 void launch_batch_face(const BatchStageArgs& b, double gamma, cudaStream_t st);
@@ -120,5 +137,7 @@ extern template void launch_nu<double>(const Stage2Args&, cudaStream_t);
 extern template void launch_nu<float>(const Stage2Args&, cudaStream_t);
 extern template void launch_update<double>(const Stage2Args&, cudaStream_t);
 extern template void launch_update<float>(const Stage2Args&, cudaStream_t);
+extern template void launch_cross<double>(const Stage2Args&, cudaStream_t);
+extern template void launch_cross<float>(const Stage2Args&, cudaStream_t);
 
 }  // namespace sacgpu

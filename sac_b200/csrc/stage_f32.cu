@@ -6,6 +6,7 @@ namespace sacgpu {
 template void launch_face<float>(const Stage2Args&, int, cudaStream_t);
 template void launch_nu<float>(const Stage2Args&, cudaStream_t);
 template void launch_update<float>(const Stage2Args&, cudaStream_t);
+template void launch_cross<float>(const Stage2Args&, cudaStream_t);
 template void launch_batch_face<float>(const BatchStageArgs&, double, cudaStream_t);
 template void launch_batch_nu<float>(const BatchStageArgs&, cudaStream_t);
 template void launch_batch_update<float>(const BatchStageArgs&, dim3, cudaStream_t);

@@ -6,6 +6,7 @@ namespace sacgpu {
 template void launch_face<double>(const Stage2Args&, int, cudaStream_t);
 template void launch_nu<double>(const Stage2Args&, cudaStream_t);
 template void launch_update<double>(const Stage2Args&, cudaStream_t);
+template void launch_cross<double>(const Stage2Args&, cudaStream_t);
 template void launch_batch_face<double>(const BatchStageArgs&, double, cudaStream_t);
 template void launch_batch_nu<double>(const BatchStageArgs&, cudaStream_t);
 template void launch_batch_update<double>(const BatchStageArgs&, dim3, cudaStream_t);
