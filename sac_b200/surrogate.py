@@ -1,6 +1,6 @@
 """FNO surrogate of the 2D flux-tube workload: data, training, judged roll-out.
 
-    python -m sac_b200.surrogate --ntrain 2000 --ntest 200 --epochs 4 --out gpurun_out/fno
+    python -m sac_b200.surrogate --ntrain 2000 --ntest 200 --epochs 4 --out fno_run
 
 * Data: FP32 solver trajectories of the flux tube (sac_b200.problems.flux_tube,
   256 x 256) with seeded drivers, A log-uniform in [1e-4, 1e-2] and omega uniform
