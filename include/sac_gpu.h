@@ -194,8 +194,8 @@ sac_status sac_getdt_static(sac_ctx* c, double* dt, int it);
  * vac run: the same parameters (sac_params, shared), its own mesh nx(ndim) with
  * two ghost layers per side, its own coordinates and state.  Boundary types that
  * store ghost values (fixed, fixed1, grad1) and the Slog driver are not available
- * here (SAC_ERR_UNSUPPORTED), nor is resistivity (eta != 0); the Powell source
- * (divbfix) is, for ndim = 2.  The Gaussian drivers (strat, tube) take their
+ * here (SAC_ERR_UNSUPPORTED), nor is a user resistivity (eta < 0); constant
+ * resistivity (eta > 0) and the Powell source (divbfix, ndim = 2) are.  The Gaussian drivers (strat, tube) take their
  * amplitude and frequency per instance (sac_batch_set_driver).
  *
  * Host arrays are the instances' Fortran-order blocks one after another:

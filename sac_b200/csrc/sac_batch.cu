@@ -158,9 +158,10 @@ __global__ void kb_zero(InstDyn* dyn, int n, int what) {
 }
 
 // the dt block of program vac per instance (src/vac.t:61-70): getdt_courant,
-// getdt_visc (src/vacusr.viscosity.t:509-542), getdt_grav (fixed at itmin)
+// getdt_res (src/vacphys.mhdres.t:5-45), getdt_visc (src/vacusr.viscosity.t:509-542),
+// getdt_grav (fixed at itmin)
 __global__ void kb_dt(InstDyn* dyn, int n, int ndim, double courantpar, double dtpar, int visc, int grav,
-                      int cantgrow) {
+                      int cantgrow, double eta, double dtdiffpar) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   InstDyn& D = dyn[i];
@@ -172,11 +173,20 @@ __global__ void kb_dt(InstDyn* dyn, int n, int ndim, double courantpar, double d
     const double cm = __longlong_as_double((long long)D.courant);
     if (!(cm == cm) || isinf(cm)) D.bad = 1;
     if (courantpar > 0.0 && cm > kSmallD) dt = fmin(dt, courantpar / cm);
+    if (eta > 0.0) {
+      // dtdiffpar*minval(dx(ixM,1:ndim))**2/eta; min over dimensions of the min of
+      // dx^2 is that square, rounding being monotonic.  dtdiffpar is the parameter
+      // until getdt_visc has overwritten it with 0.25 at an earlier step.
+      double m2 = kBig;
+      for (int d = 0; d < ndim; ++d) m2 = fmin(m2, D.mindx2[d]);
+      dt = fmin(dt, (D.visc_dt_seen ? 0.25 : dtdiffpar) * m2 / eta);
+    }
     if (grav && visc) {
       const double mv = __longlong_as_double((long long)D.maxnu);
       if (!(mv == mv)) D.bad = 1;
       for (int d = 0; d < ndim; ++d) dt = fmin(dt, 0.25 / ((mv + 0.0) / D.mindx2[d]));
       D.maxnu = 0ull;
+      D.visc_dt_seen = 1;
     }
     if (grav) dt = fmin(dt, D.dtgrav);
     if (cantgrow && D.it > 0) dt = fmin(dt, D.dt);  // dtcantgrow, src/vac.t:68
@@ -269,6 +279,8 @@ Stage2Args stage_base(sac_batch* b) {
   a.grav_on = (b->par.sourceunsplit && grav_mod(b->par.user)) ? 1 : 0;
   a.visc_on = (b->par.sourceunsplit && visc_on_b(b)) ? 1 : 0;
   a.divb_on = (b->par.sourceunsplit && b->par.divbfix && b->ndim > 1) ? 1 : 0;  // src/vacphys.mhd0.t:255
+  a.res_on = (b->par.sourceunsplit && std::fabs(b->par.eta) > kSmallD) ? 1 : 0;
+  a.eta = b->par.eta;
   a.driver = DRV_NONE;
   if (b->par.sourceunsplit && b->drv)
     a.driver = b->par.user == SAC_USR_STRAT ? DRV_STRAT : DRV_TUBE;  // amplitude and omega per instance
@@ -291,7 +303,8 @@ void enqueue_step(sac_batch* b) {
   cb.ntiles = b->n_cour;
   launch_batch_courant<S>(cb, b->par.gamma, b->stream);
   kb_dt<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst, b->ndim, b->par.courantpar, b->par.dtpar,
-                                   visc_on_b(b) ? 1 : 0, ngrav, b->par.dtcantgrow ? 1 : 0);
+                                   visc_on_b(b) ? 1 : 0, ngrav, b->par.dtcantgrow ? 1 : 0, b->par.eta,
+                                   b->par.dtdiffpar);
   void *w = b->P[0], *w1 = b->P[1], *w2 = b->P[2], *w3 = b->P[3];
   const void* wct[4] = {w, w1, w2, w3};
   void* out[4] = {w1, w2, w3, w};
@@ -409,7 +422,7 @@ sac_status sac_batch_create(const sac_params* p, int ndim, int ndir, int ninst, 
   if (std::string(p->typeadvance) != "fourstep") return SAC_ERR_UNSUPPORTED;
   if (p->precision != SAC_PREC_FP64 && p->precision != SAC_PREC_FP32) return SAC_ERR_UNSUPPORTED;
   if (p->user == SAC_USR_SLOG || (p->user == SAC_USR_TUBE && ndim < 2)) return SAC_ERR_UNSUPPORTED;
-  if (p->eta != 0.0) return SAC_ERR_UNSUPPORTED;  // resistivity runs on the single-grid path only
+  if (p->eta < 0.0) return SAC_ERR_UNSUPPORTED;  // a user specialeta; eta > 0 is built
   sac_batch* b = new sac_batch();
   b->par = *p;
   b->dev = p->device;

@@ -57,6 +57,7 @@ struct InstDyn {
                        // takes dt = 0 steps that leave its state untouched
   unsigned long long ctot[3], maxnu, courant;  // bits of non-negative maxima
   int it, bad;       // step counter; set when a reduction met NaN/Inf
+  int visc_dt_seen;  // getdt_visc has run once, overwriting dtdiffpar with 0.25
 };
 
 // one unit of work: a tile of blockDim cells starting at p (local coordinates)

@@ -994,16 +994,28 @@ void launch_batch_update(const BatchStageArgs& b0, dim3 blk, cudaStream_t st) {
   fill_field_ptrs(b.a, sizeof(S));
   if (!b.ntiles) return;
   dispatch_nd(b.a.g, [&](auto ND, auto NR) {
-    // the batch has no resistivity (rejected at creation); Powell's term for ndim > 1
+    // Powell's term for ndim > 1, the resistive one for ndir > 1
     constexpr int NDIM = decltype(ND)::value;
+    constexpr int NDIR = decltype(NR)::value;
     const unsigned grid = persistent_grid(b.ntiles, 2);
+    const int opt = ((NDIM > 1 && b.a.divb_on) ? OPT_DIVB : 0) | ((NDIR > 1 && b.a.res_on) ? OPT_RES : 0);
     if constexpr (NDIM > 1) {
-      if (b.a.divb_on) {
-        kb_update<NDIM, decltype(NR)::value, S, OPT_DIVB><<<grid, blk, 0, st>>>(b);
+      if (opt == OPT_DIVB) {
+        kb_update<NDIM, NDIR, S, OPT_DIVB><<<grid, blk, 0, st>>>(b);
+        return;
+      }
+      if (opt == (OPT_DIVB | OPT_RES)) {
+        kb_update<NDIM, NDIR, S, OPT_DIVB | OPT_RES><<<grid, blk, 0, st>>>(b);
         return;
       }
     }
-    kb_update<NDIM, decltype(NR)::value, S, 0><<<grid, blk, 0, st>>>(b);
+    if constexpr (NDIR > 1) {
+      if (opt == OPT_RES) {
+        kb_update<NDIM, NDIR, S, OPT_RES><<<grid, blk, 0, st>>>(b);
+        return;
+      }
+    }
+    kb_update<NDIM, NDIR, S, 0><<<grid, blk, 0, st>>>(b);
   });
 }
 

@@ -119,6 +119,38 @@ def test_divbfix_2d_fp32():
     _check(Ps, b, 10, FP32_RTOL)
 
 
+def _resistive_problems(ndim, dtpar=None, eta=0.01):
+    if ndim == 2:
+        types = ["cont", "cont1", "periodic", "periodic"]
+        Ps = [problems.random_problem(n, ndir=3, seed=s, types=types) for n, s in (((14, 12), 6), ((20, 10), 7))]
+    else:
+        Ps = [problems.random_problem((n,), ndir=3, seed=n, types=["cont", "symm"]) for n in (40, 33)]
+    prm = Ps[0].params
+    prm.eta = eta
+    prm.divbfix = 1 if ndim == 2 else 0
+    if dtpar is not None:
+        prm.dtpar = dtpar
+    for P in Ps:
+        P.params = prm
+    return Ps, prm
+
+
+@pytest.mark.parametrize("ndim,eta", [(1, 0.01), (2, 0.01), (2, 0.5)])
+def test_resistive_fp64(ndim, eta):
+    # at eta = 0.5 getdt_res sets dt, with dtdiffpar 0.5 at the first step and the
+    # 0.25 that getdt_visc leaves after it
+    Ps, prm = _resistive_problems(ndim, eta=eta)
+    _check(Ps, _batch_of(Ps, prm), 12, RTOL)
+
+
+def test_resistive_2d_fp32():
+    Ps, prm = _resistive_problems(2, dtpar=2.0e-3)
+    prm.precision = params.PREC_FP32
+    b = _batch_of(Ps, prm)
+    prm.precision = params.PREC_FP64
+    _check(Ps, b, 10, FP32_RTOL)
+
+
 def test_1d_instances():
     Ps = [problems.random_problem((n,), ndir=2, seed=n, types=["cont", "symm"]) for n in (40, 64, 33)]
     prm = Ps[0].params
@@ -176,7 +208,7 @@ def test_unsupported_options_are_errors():
     with pytest.raises(abi.SacError):
         batch.Batch(prm, 2, 2, [(16, 16)])
     prm = batch.ot_params()
-    prm.eta = 0.01  # resistivity runs on the single-grid path only
+    prm.eta = -0.01  # a user specialeta
     with pytest.raises(abi.SacError):
         batch.Batch(prm, 2, 2, [(16, 16)])
     prm = batch.ot_params()

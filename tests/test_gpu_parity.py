@@ -169,6 +169,14 @@ def test_resistive_random(nx, ndir):
     _steps(P, 100)
 
 
+def test_resistive_dt_limit_binds():
+    # getdt_res sets dt: dtdiffpar 0.5 at the first step, 0.25 after getdt_visc
+    P = problems.random_problem((14, 12), ndir=3, seed=6, types=["cont", "cont1", "periodic", "periodic"])
+    P.params.eta = 0.5
+    P.params.divbfix = 1
+    _steps(P, 30)
+
+
 def test_resistive_with_divbfix_3d():
     P = problems.random_problem((12, 10, 8), seed=45, types=["cont", "cont", "periodic", "periodic", "fixed", "cont"])
     P.params.eta = 0.01
