@@ -62,3 +62,48 @@ def test_default_params_match_par_default():
     p = params.SacParams()
     lib.sac_default_params(ctypes.byref(p))
     assert p.courantpar == 0.8 and p.dtpar == -1.0 and p.typeadvance == b"twostep" and p.sourceunsplit == 1
+
+
+C_CALLER = r"""
+#include <stdio.h>
+#include <string.h>
+#include "sac_gpu.h"
+#include "sac_fno.h"
+
+int main(void) {
+  sac_params p;
+  sac_ctx* c = NULL;
+  sac_status st;
+  sac_default_params(&p);
+  strcpy(p.typeadvance, "fourstep");
+  st = sac_create(&p, &c);
+  printf("%d %zu %d %s %.17g %d\n", (int)st, sizeof(sac_params), p.sourceunsplit, p.typeadvance, p.courantpar,
+         c == NULL);
+  if (c) sac_destroy(c);
+  return 0;
+}
+"""
+
+
+def test_headers_compile_as_c99_and_a_c_caller_links(tmp_path):
+    """A C host (the Fortran shim's ISO_C_BINDING side sees the same layout)
+    includes both headers with a strict C99 compiler, links the library and
+    calls it; without a GPU sac_create returns SAC_ERR_NODEVICE and no context."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc")
+    if cc is None:
+        pytest.skip("gcc not found")
+    path = build.build()
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), path, "-Wl,-rpath," + os.path.dirname(path)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    status = params.STATUS[int(out[0])]
+    assert status in ("SAC_OK", "SAC_ERR_NODEVICE")
+    assert out[5] == ("1" if status == "SAC_ERR_NODEVICE" else "0")
+    assert int(out[1]) == ctypes.sizeof(params.SacParams)
+    assert out[2] == "1" and out[3] == "fourstep" and float(out[4]) == 0.8
