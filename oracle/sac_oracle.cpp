@@ -7,9 +7,11 @@
 // be compiled here (it is Fortran; no Fortran compiler exists on these machines),
 // so its outputs cannot be produced: parity of this restatement is unpinned by
 // reference outputs.  It is pinned instead by the reference's own initial-data
-// scripts (inipar/*.py, run to make tests/golden fixtures), by an independent
-// numpy transcription of the same Fortran array statements (oracle/vac_numpy.py)
-// and by physics invariants (tests/test_oracle_*.py).
+// scripts (inipar/*.py, run to make tests/golden fixtures), by numpy
+// transcriptions of the Fortran array statements of the optional sources
+// (tests/test_oracle_sources.py), by physics invariants
+// (tests/test_oracle_physics.py) and by the independently written per-cell CUDA
+// path agreeing with it to 1e-12 (tests/test_gpu_*.py).
 //
 // Indexing: 0-based, w[iw*ncell + i1 + n1*(i2 + n2*i3)], i.e. the reference's
 // Fortran layout w(ix1,ix2,ix3,iw) with x1 fastest.  Dimension d = idim-1.
