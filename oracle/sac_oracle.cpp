@@ -8,8 +8,10 @@
 // so its outputs cannot be produced: parity of this restatement is unpinned by
 // reference outputs.  It is pinned instead by the reference's own initial-data
 // scripts (inipar/*.py, run to make tests/golden fixtures), by numpy
-// transcriptions of the Fortran array statements of the optional sources
-// (tests/test_oracle_sources.py), by physics invariants
+// transcriptions of the Fortran array statements of centdiff4, addsource_visc
+// with setnu, and the Powell and resistive sources, each equal to this file's
+// one-step update bit for bit (tests/test_oracle_centdiff.py,
+// tests/test_oracle_visc.py, tests/test_oracle_sources.py), by physics invariants
 // (tests/test_oracle_physics.py) and by the independently written per-cell CUDA
 // path agreeing with it to 1e-12 (tests/test_gpu_*.py).
 //

@@ -45,3 +45,32 @@ def rel_l2(a, b):
 
 def gpu_ctx(params):
     return abi.Context(params)
+
+
+def gridsetup1_dx(P):
+    """Cell widths as gridsetup1 (src/vacgrid.t:585-629) makes them: the ghost
+    coordinates, and one more layer, are extrapolated from the two edge mesh cells,
+    (1+n) x(edge) - n x(edge-+1), one dimension after the other over the whole
+    extended grid; then dx = (x(+1) - x(-1))/2.  Returns dx[..., d] on the full grid."""
+    nd = P.ndim
+    G = [n + 4 for n in P.nx]
+    qx = np.zeros([g + 2 for g in G] + [nd])
+    qx[tuple(slice(1, 1 + g) for g in G)] = P.x
+
+    def at(d, i):
+        return tuple(i if e == d else slice(None) for e in range(nd))
+
+    for d in range(nd):
+        lo, hi = 3, P.nx[d] + 2  # the first and last mesh cell in extended coordinates
+        for ix in range(hi + 1, G[d] + 2):
+            n = ix - hi
+            qx[at(d, ix)] = float(1 + n) * qx[at(d, hi)] - float(n) * qx[at(d, hi - 1)]
+        for ix in range(lo - 1, -1, -1):
+            n = lo - ix
+            qx[at(d, ix)] = float(1 + n) * qx[at(d, lo)] - float(n) * qx[at(d, lo + 1)]
+    dx = np.zeros(tuple(G) + (nd,))
+    for d in range(nd):
+        sl = lambda k: tuple(slice(1 + (k if e == d else 0), 1 + (k if e == d else 0) + G[e])  # noqa: E731
+                             for e in range(nd))
+        dx[..., d] = 0.5 * (qx[sl(1) + (d,)] - qx[sl(-1) + (d,)])
+    return dx
