@@ -208,3 +208,29 @@ def test_negative_eta_is_rejected():
         o.getdt(0)
     with pytest.raises(abi.SacError):
         o.advect(0.01, 0.0, 0)
+
+
+# ---------------------------------------------------------------------------
+# gravity, addsource_grav (src/vacusr.gravity.t:24-81)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("nx,ndir", [((30,), 2), ((14, 12), 3), ((10, 9, 8), 3)])
+def test_gravity_source_step_matches_numpy(nx, ndir):
+    types = ["cont", "fixed", "periodic", "periodic", "cont", "symm"][: 2 * len(nx)]
+    grav = (-0.7, 0.3, 0.2)
+    P = problems.random_problem(nx, ndir=ndir, seed=39, types=types, user=params.USR_GRAVVISC, nu=0.0,
+                                grav=grav, typeadvance="onestep")
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    qdt = 37.0  # the increment dominates w, so its last bits show
+    o.advect(qdt, 0.0, 0, method="source")
+    got = _util.mesh(P, o.download())
+    v = problems.var_index(P.ndir)
+    want = _view(P, w0).copy()
+    rho = _view(P, w0[..., v["rho"]])
+    rt = _view(P, w0[..., v["rho"]] + w0[..., v["rhob"]])
+    for d in range(P.ndim):  # dm_i/dt = +g_i rho' (the perturbed density only)
+        want[..., v["m0"] + 1 + d] = want[..., v["m0"] + 1 + d] + qdt * grav[d] * rho
+    for d in range(P.ndim):  # de/dt = +g_i rho' m_i/(rho'+rho_b)
+        want[..., v["e"]] = want[..., v["e"]] + qdt * grav[d] * rho * _view(P, w0[..., v["m0"] + 1 + d]) / rt
+    nadv = 2 * P.ndir + 2
+    np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
