@@ -249,3 +249,28 @@ def test_hyperdiffusion_step_matches_numpy(nx, ndir, types):
     nadv = 2 * P.ndir + 2
     assert np.abs(got[..., :nadv] - _util.mesh(P, w0)[..., :nadv]).max() > 1e-6  # the source acts
     np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
+
+
+@pytest.mark.parametrize("nx,ndir", [((30,), 2), ((14, 12), 3), ((10, 9, 8), 3)])
+def test_first_dt_matches_numpy(nx, ndir):
+    """getdt at the first step (src/vac.t:61-70): getdt_courant (src/vac.t:641-699),
+    getdt_visc with maxviscoef still 0 (an infinite limit), and getdt_grav, whose
+    limit takes every gravity component over the cell widths of every dimension
+    (src/vacusr.gravity.t:97-138)."""
+    types = ["cont", "fixed", "periodic", "periodic", "cont", "symm"][: 2 * len(nx)]
+    grav = (-0.7, 0.3, 0.2)
+    P = problems.random_problem(nx, ndir=ndir, seed=40, types=types, user=params.USR_GRAVVISC, grav=grav)
+    o = _util.start(Oracle, P)
+    dt = o.getdt(0)
+    V = Visc(P, o.download(), 0.0)
+    courantmax = 0.0
+    for d in range(P.ndim):
+        courantmax = max(courantmax, float((_reg(P, V.cmax(d)) / V.dx(0, d)).max()))
+    want = 1.0e99
+    want = min(want, P.params.courantpar / courantmax)
+    dtgrav = 1.0e99
+    for d in range(P.ndim):
+        m = max(float((abs(grav[d]) / V.dx(0, j)).max()) for j in range(P.ndim))
+        dtgrav = min(dtgrav, 1.0 / np.sqrt(m))
+    want = min(want, dtgrav)
+    assert dt == want
