@@ -9,10 +9,11 @@
 // reference outputs.  It is pinned instead by the reference's own initial-data
 // scripts (inipar/*.py, run to make tests/golden fixtures), by numpy
 // transcriptions of the Fortran array statements of centdiff4, addsource_visc
-// with setnu, the gravity, Powell and resistive sources, the first getdt and
-// getboundary, each equal to this file's result bit for bit
-// (tests/test_oracle_centdiff.py, tests/test_oracle_visc.py,
-// tests/test_oracle_sources.py, tests/test_oracle_boundaries.py), by physics invariants
+// with setnu, the gravity, Powell and resistive sources, the first getdt,
+// getboundary and, composed from them, a whole RK4 step, each equal to this
+// file's result bit for bit (tests/test_oracle_centdiff.py,
+// tests/test_oracle_visc.py, tests/test_oracle_sources.py,
+// tests/test_oracle_boundaries.py, tests/test_oracle_rk4.py), by physics invariants
 // (tests/test_oracle_physics.py) and by the independently written per-cell CUDA
 // path agreeing with it to 1e-12 (tests/test_gpu_*.py).
 //

@@ -1,0 +1,83 @@
+"""A full RK4 step of the oracle against the numpy transcriptions composed (CPU).
+
+advect's 'fourstep' (src/vac.t:439-455): w1 = w + dt/2 R(w), w2 = w + dt/2 R(w1),
+w3 = w + dt R(w2), each advect1 (src/vac.t:490-549) adding centdiff4's flux
+divergence and then addsource2's sources (gravity, hyperdiffusion) to its base,
+and filling the boundaries (getboundary); then w1 = (w1 + 2 w2 + w3 - 4 w)/3 and
+w = w + dt/6 R(w3) + w1 over the whole grid, ghosts and background included.
+Composed from the transcriptions of test_oracle_centdiff, test_oracle_visc and
+test_oracle_boundaries, it must equal the oracle's step bit for bit."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from sac_b200 import params, problems
+
+import _util
+from test_oracle_boundaries import _fill
+from test_oracle_centdiff import _getflux, _getptotal_bg, _gradient4, _mesh
+from test_oracle_visc import Visc
+
+
+def _advect1(P, qdt, wct, base):
+    v = problems.var_index(P.ndir)
+    gamma = P.params.gamma
+    dims = list(range(P.ndim))
+    new = _mesh(P, base).copy()
+    # centdiff4 (src/vaccd.t:35-70): fluxes from wCT, background work from the output array
+    for d in dims:
+        vel = wct[..., v["m0"] + 1 + d] / (wct[..., v["rho"]] + wct[..., v["rhob"]])
+        for iw in range(v["eb"]):
+            f, transport = _getflux(wct, v, P.ndir, gamma, iw, d)
+            if transport:
+                f = f + vel * wct[..., iw]
+            new[..., iw] = new[..., iw] - qdt * _gradient4(P, f, d)
+            if iw == v["e"]:
+                fb = _mesh(P, _getptotal_bg(base, v, P.ndir, gamma))
+                new[..., iw] = new[..., iw] - qdt * _gradient4(P, vel, d) * fb
+                for di in dims:
+                    bgi = _mesh(P, base[..., v["bg0"] + 1 + di])
+                    bgd = _mesh(P, base[..., v["bg0"] + 1 + d])
+                    new[..., iw] = new[..., iw] + qdt * bgi * bgd * _gradient4(P, vel, di)
+    # addsource2 -> specialsource with qdt*(idimmax-idimmin+1)/ndim (src/vaccd.t:73-75),
+    # which rounds in 3D: gravity (src/vacusr.gravity.t:24-81), then hyperdiffusion
+    qdt = qdt * (float(len(dims) - 1) + 1.0) / float(P.ndim)
+    g = list(P.params.grav)
+    rho = _mesh(P, wct[..., v["rho"]])
+    rt = _mesh(P, wct[..., v["rho"]] + wct[..., v["rhob"]])
+    for d in dims:
+        if abs(g[d]) > 1e-99:
+            new[..., v["m0"] + 1 + d] = new[..., v["m0"] + 1 + d] + qdt * g[d] * rho
+    for d in dims:
+        if abs(g[d]) > 1e-99:
+            new[..., v["e"]] = new[..., v["e"]] + qdt * g[d] * rho * _mesh(P, wct[..., v["m0"] + 1 + d]) / rt
+    new = Visc(P, wct, qdt).step(new)
+    out = base.copy()
+    out[tuple(slice(2, 2 + n) for n in P.nx)] = new
+    return _fill(P, out)
+
+
+def _fourstep(P, w, dt):
+    w1 = _advect1(P, dt / 2, w, w)
+    w2 = _advect1(P, dt / 2, w1, w)
+    w3 = _advect1(P, dt, w2, w)
+    w1 = (w1 + 2.0 * w2 + w3 - 4.0 * w) / 3.0
+    w = _advect1(P, dt / 6, w3, w)
+    return w + w1
+
+
+@pytest.mark.parametrize("nx,ndir,types", [
+    ((24,), 2, ["cont", "symm"]),
+    ((14, 12), 3, ["cont1", "contCD4", "periodic", "periodic"]),
+    ((10, 9, 8), 3, ["periodic", "periodic", "cont", "asymm", "cont", "symm"]),
+])
+def test_rk4_step_matches_the_composed_transcriptions(nx, ndir, types):
+    P = problems.random_problem(nx, ndir=ndir, seed=41, types=types, typeadvance="fourstep")
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    dt = 0.2 * o.getdt(0)
+    o.advect(dt, 0.0, 0)
+    got = o.download()
+    want = _fourstep(P, w0, dt)
+    assert np.abs(got - w0).max() > 1e-6
+    np.testing.assert_array_equal(got, want)

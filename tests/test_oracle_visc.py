@@ -160,10 +160,11 @@ class Visc:
         return R, L
 
     # ---- addsource_visc --------------------------------------------------------
-    def step(self):
+    def step(self, base=None):
+        """The mesh of base (default: w itself) plus addsource_visc of w."""
         P, w, v, qdt = self.P, self.w, self.v, self.qdt
-        nd, nr = P.ndim, P.ndir
-        new = _reg(P, w).copy()
+        nd = P.ndim
+        new = (_reg(P, w) if base is None else base).copy()
         inner = tuple(slice(1, 1 + x) for x in P.nx)
         nushk = 0.0
         # density and the "173" energy, :45-64
