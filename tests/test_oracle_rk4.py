@@ -81,3 +81,38 @@ def test_rk4_step_matches_the_composed_transcriptions(nx, ndir, types):
     want = _fourstep(P, w0, dt)
     assert np.abs(got - w0).max() > 1e-6
     np.testing.assert_array_equal(got, want)
+
+
+def _integrate(P, w, dt, method, pred):
+    """advect's other time integrators (src/vac.t:402-476); w1 starts as a copy of w."""
+    nul = lambda wct, base: _fill(P, base.copy())  # noqa: E731  advect1 with method 'nul'
+    if method == "onestep":
+        return _advect1(P, dt, w.copy(), w)
+    if method == "twostep":
+        w1 = _advect1(P, dt / 2, w, w) if pred == "cd4" else nul(w, w)
+        return _advect1(P, dt, w1, w)
+    if method == "threestep":
+        w1 = _advect1(P, dt, w, w)
+        w2 = 3 * 0.25 * w + 0.25 * w1
+        w2 = _advect1(P, dt / 4, w1, w2)
+        w = w / 3 + w2 * (2.0 / 3)
+        return _advect1(P, dt * 2.0 / 3, w2, w)
+    # sterck's first fraction is the single-precision literal 0.12 (src/vac.t:459)
+    f = (dt * float(np.float32(0.12)), dt / 4, dt / 2) if method == "sterck" else (dt / 4, dt / 3, dt / 2)
+    w1 = _advect1(P, f[0], w, w)
+    w2 = _advect1(P, f[1], w1, w)
+    w1 = _advect1(P, f[2], w2, w)
+    return _advect1(P, dt, w1, w)
+
+
+@pytest.mark.parametrize("method,pred", [("onestep", "nul"), ("twostep", "nul"), ("twostep", "cd4"),
+                                          ("threestep", "nul"), ("sterck", "nul"), ("jameson", "nul")])
+def test_other_integrators_match_the_composed_transcriptions(method, pred):
+    P = problems.random_problem((14, 12), ndir=3, seed=42, types=["cont", "symm", "periodic", "periodic"],
+                                typeadvance=method, courantpar=0.2)
+    P.params.typepred = pred.encode()
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    dt = o.getdt(0)
+    o.advect(dt, 0.0, 0)
+    np.testing.assert_array_equal(o.download(), _integrate(P, w0, dt, method, pred))
