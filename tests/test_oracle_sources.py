@@ -234,3 +234,62 @@ def test_gravity_source_step_matches_numpy(nx, ndir):
         want[..., v["e"]] = want[..., v["e"]] + qdt * grav[d] * rho * _view(P, w0[..., v["m0"] + 1 + d]) / rt
     nadv = 2 * P.ndir + 2
     np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
+
+
+# ---------------------------------------------------------------------------
+# the reference's Slog user module, specialsource (src/vacusr.f:1255-1382):
+# gravity, hyperdiffusion (eqpar(nu_)=1), then the vortex velocity driver
+# ---------------------------------------------------------------------------
+def test_slog_source_step_matches_its_fortran():
+    import math
+
+    from test_oracle_visc import Visc
+
+    P = problems.random_problem((10, 8, 8), seed=43, user=params.USR_SLOG,
+                                types=["cont", "cont", "periodic", "periodic", "periodic", "periodic"],
+                                typeadvance="onestep")
+    P.x[...] *= 1.0e6  # the module's lengths are in metres (Mm scale), x1 vertical
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    qdt, qt = 37.0, 30.0
+    o.advect(qdt, qt, 0, method="source")
+    got = _util.mesh(P, o.download())
+
+    v = problems.var_index(P.ndir)
+    new = _view(P, w0).copy()
+    grav = list(P.params.grav)
+    rho = _view(P, w0[..., v["rho"]])
+    rt = _view(P, w0[..., v["rho"]] + w0[..., v["rhob"]])
+    for d in range(3):
+        if abs(grav[d]) > 1e-99:
+            new[..., v["m0"] + 1 + d] = new[..., v["m0"] + 1 + d] + qdt * grav[d] * rho
+    for d in range(3):
+        if abs(grav[d]) > 1e-99:
+            new[..., v["e"]] = new[..., v["e"]] + qdt * grav[d] * rho * _view(P, w0[..., v["m0"] + 1 + d]) / rt
+    new = Visc(P, w0, qdt).step(new)
+    # the driver, with the single-precision literals pi, 0.1 and 0.05, and the
+    # density already updated by the hyperdiffusion
+    f32 = lambda a: float(np.float32(a))  # noqa: E731
+    pi = f32(math.pi)
+    xc1, xc2, xc3 = f32(0.1) * 1.0e6, 1.0 * 1.0e6, 1.0 * 1.0e6
+    dz, dxx, dyy = 0.05e6, 0.5e6, 0.5e6
+    AA, B, s_period = 10.0, f32(0.05), 240.0
+    tdep = math.sin(qt * 2.0 * pi / s_period)
+    X = [_view(P, P.x[..., d]) for d in range(3)]
+    rb = _view(P, w0[..., v["rhob"]])
+    for idx in np.ndindex(*P.nx):
+        xx, yy, zz = X[1][idx] - xc2, X[2][idx] - xc3, X[0][idx] - xc1
+        exp_z = math.exp(-(zz * zz) / (dz * dz))
+        exp_x = math.exp(-(xx * xx) / (dxx * dxx))
+        exp_y = math.exp(-(yy * yy) / (dyy * dyy))
+        exp_xyz = exp_x * exp_y * exp_z
+        theta, phi = math.atan2(yy, xx), math.atan2(1.0, B)
+        ux, uy = math.cos(theta + phi), math.sin(theta + phi)
+        vvx = (ux / math.sqrt(ux * ux + uy * uy)) * exp_xyz * tdep * AA
+        vvy = (uy / math.sqrt(ux * ux + uy * uy)) * exp_xyz * tdep * AA
+        r = new[idx + (v["rho"],)] + rb[idx]
+        new[idx + (v["m0"] + 2,)] = new[idx + (v["m0"] + 2,)] + r * vvx * qdt
+        new[idx + (v["m0"] + 3,)] = new[idx + (v["m0"] + 3,)] + r * vvy * qdt
+        new[idx + (v["e"],)] = new[idx + (v["e"],)] + r * (vvx * vvx + vvy * vvy + 0.0 * 0.0) * qdt / 2.0
+    nadv = 2 * P.ndir + 2
+    np.testing.assert_array_equal(got[..., :nadv], new[..., :nadv])
