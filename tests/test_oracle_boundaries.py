@@ -16,8 +16,9 @@ from sac_b200 import problems
 import _util
 
 
-def _fill(P, w):
-    """The first getboundary on a copy of w (every variable, default regions)."""
+def _fill(P, w, fix=None):
+    """getboundary on a copy of w (every variable, default regions).  fix: the
+    values captured after the first fill (_capture); None for the first fill."""
     w = w.copy()
     nd = P.ndim
     for iB in range(2 * nd):
@@ -31,6 +32,12 @@ def _fill(P, w):
         for iw in range(w.shape[-1]):
             t = P.typeB[iB][iw]
             a = w[..., iw]
+            if fix is not None and (iB, iw) in fix:
+                e = hi if up else lo
+                for n, i in enumerate(layers):
+                    stored = fix[(iB, iw)][n]
+                    a[at(i)] = stored + a[at(e)] if t == "grad1" else stored
+                continue
             if t in ("cont", "fixed"):
                 e = hi if up else lo
                 for i in layers:
@@ -59,6 +66,25 @@ def _fill(P, w):
             else:
                 raise ValueError(t)
     return w
+
+
+def _capture(P, w):
+    """fixB after the first fill (src/vacgrid.t:476-507): the ghost values of
+    'fixed' and 'fixed1' regions, and for 'grad1' their difference to the edge."""
+    fix = {}
+    nd = P.ndim
+    for iB in range(2 * nd):
+        d, up = iB // 2, iB % 2 == 1
+        lo, hi = 2, 2 + P.nx[d] - 1
+        layers = (hi + 1, hi + 2) if up else (lo - 2, lo - 1)
+        e = hi if up else lo
+        for iw in range(w.shape[-1]):
+            t = P.typeB[iB][iw]
+            if t in ("fixed", "fixed1", "grad1"):
+                a = w[..., iw]
+                at = lambda i: tuple(i if k == d else slice(None) for k in range(nd))  # noqa: E731
+                fix[(iB, iw)] = [a[at(i)] - a[at(e)] if t == "grad1" else a[at(i)].copy() for i in layers]
+    return fix
 
 
 _KINDS = ["cont", "fixed", "cont1", "fixed1", "grad1", "symm", "symm0", "asymm", "contCD4"]
@@ -91,3 +117,19 @@ def test_first_fill_matches_numpy(nx, periodic_dims, seed):
     P.w = w0
     o = _util.start(Oracle, P)
     np.testing.assert_array_equal(o.download(), _fill(P, w0))
+
+
+@pytest.mark.parametrize("nx,periodic_dims,seed", [((12,), (), 7), ((10, 9), (), 8), ((8, 7, 6), (1,), 9)])
+def test_later_fill_restores_the_captured_values(nx, periodic_dims, seed):
+    P = problems.random_problem(nx, ndir=3 if len(nx) > 1 else 2, seed=seed)
+    nw = P.w.shape[-1]
+    P.typeB = _types(len(nx), nw, periodic_dims, seed)
+    o = _util.start(Oracle, P)
+    first = o.download()
+    fix = _capture(P, first)
+    # a changed state, ghosts included, then the next fill
+    rng = np.random.default_rng(seed + 200)
+    w1 = first + 0.1 * rng.standard_normal(first.shape)
+    o.upload(w1)
+    o.getboundary(0.0)
+    np.testing.assert_array_equal(o.download(), _fill(P, w1, fix))
