@@ -19,6 +19,9 @@ from test_oracle_centdiff import _getflux, _getptotal_bg, _gradient4, _mesh
 from test_oracle_visc import Visc
 
 
+_MAXNU = [0.0]  # maxviscoef over the setnu calls since the last getdt
+
+
 def _advect1(P, qdt, wct, base):
     v = problems.var_index(P.ndir)
     gamma = P.params.gamma
@@ -51,7 +54,9 @@ def _advect1(P, qdt, wct, base):
     for d in dims:
         if abs(g[d]) > 1e-99:
             new[..., v["e"]] = new[..., v["e"]] + qdt * g[d] * rho * _mesh(P, wct[..., v["m0"] + 1 + d]) / rt
-    new = Visc(P, wct, qdt).step(new)
+    V = Visc(P, wct, qdt)
+    new = V.step(new)
+    _MAXNU[0] = max(_MAXNU[0], V.maxviscoef)
     out = base.copy()
     out[tuple(slice(2, 2 + n) for n in P.nx)] = new
     return _fill(P, out)
@@ -116,3 +121,32 @@ def test_other_integrators_match_the_composed_transcriptions(method, pred):
     dt = o.getdt(0)
     o.advect(dt, 0.0, 0)
     np.testing.assert_array_equal(o.download(), _integrate(P, w0, dt, method, pred))
+
+
+def test_second_dt_takes_the_viscous_limit_of_the_step():
+    """getdt after an RK4 step: getdt_courant on the new state, getdt_visc with
+    maxviscoef, the largest nu of every setnu call of the step, and dtdiffpar
+    0.25 (src/vacusr.viscosity.t:509-542), and the saved dtgrav."""
+    P = problems.random_problem((14, 12), ndir=3, seed=44, types=["cont", "symm", "periodic", "periodic"],
+                                typeadvance="fourstep")
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    dt0 = o.getdt(0)
+    o.advect(0.5 * dt0, 0.0, 0)
+    dt1 = o.getdt(1)
+    _MAXNU[0] = 0.0
+    w1 = _fourstep(P, w0, 0.5 * dt0)
+    V = Visc(P, w1, 0.0)
+    courantmax = max(float((_mesh(P, V.cmax(d)) / V.dx(0, d)).max()) for d in range(P.ndim))
+    want = min(1.0e99, P.params.courantpar / courantmax)
+    for d in range(P.ndim):
+        dxm = V.dx(0, d)
+        want = min(want, 0.25 / float(((_MAXNU[0] + 0.0) / (dxm * dxm)).max()))
+    grav = list(P.params.grav)
+    dtgrav = 1.0e99
+    for d in range(P.ndim):
+        m = max(float((abs(grav[d]) / V.dx(0, j)).max()) for j in range(P.ndim))
+        dtgrav = min(dtgrav, 1.0 / np.sqrt(m))
+    want = min(want, dtgrav)
+    assert _MAXNU[0] > 0.0
+    assert dt1 == want

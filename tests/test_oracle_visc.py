@@ -38,6 +38,7 @@ class Visc:
         # one) along d unless rho's boundary there is periodic
         self.periodic = [[P.typeB[2 * d + s][0] == "periodic" for s in (0, 1)] for d in range(P.ndim)]
         self.dxg = _util.gridsetup1_dx(P)
+        self.maxviscoef = 0.0
 
     # ---- grid helpers --------------------------------------------------------
     def dx(self, g, d):
@@ -154,6 +155,9 @@ class Visc:
         with np.errstate(divide="ignore", invalid="ignore"):
             nuR = np.where(md1R > 0.0, c_tot * chyp * md3R / md1R * dxm, 0.0)
             nuL = np.where(md1L > 0.0, c_tot * chyp * md3L / md1L * dxm, 0.0)
+        # maxviscoef=MAX(MAXVAL(nuR), maxviscoef), then the same for nuL (:426, :444)
+        self.maxviscoef = max(float(nuR.max()), self.maxviscoef)
+        self.maxviscoef = max(float(nuL.max()), self.maxviscoef)
         R, L = np.zeros([x + 2 for x in P.nx]), np.zeros([x + 2 for x in P.nx])
         inner = tuple(slice(1, 1 + x) for x in P.nx)
         R[inner], L[inner] = nuR, nuL
