@@ -396,6 +396,98 @@ def ours(args, rank, world, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the small configurations' legs (not the headline line): Brio-Wu on the GPU
+# through the C-ABI against the CPU oracle, and the CPU oracle on one 2D
+# Orszag-Tang instance of the batch's mean size (the batch's CPU baseline)
+# ---------------------------------------------------------------------------
+def _start(cls, P):
+    c = cls(P.params)
+    c.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
+    c.set_boundaries(P.typeB_packed, P.nB)
+    c.upload(P.w)
+    c.getboundary(0.0)
+    return c
+
+
+def _to_tmax(c, tmax, max_steps=100000):
+    """program vac's loop (getdt, then advect) until t reaches tmax."""
+    t, it = 0.0, 0
+    while t < tmax and it < max_steps:
+        dt = min(c.getdt(it), tmax - t + 1e-99)
+        c.advect(dt, t, it)
+        t += dt
+        it += 1
+    return it
+
+
+def briowu_workload():
+    """Brio-Wu (1D, nx=800, to t=0.1): the GPU through the C-ABI, each getdt
+    reading its reductions back, with CUDA events around the loop; the CPU
+    oracle on all host threads and on one; the GPU's relative L2 to the oracle."""
+    import ctypes
+
+    import torch
+
+    from oracle import oracle
+
+    from sac_b200 import abi, build, problems
+    build.build()
+    oracle.build()
+    nthreads = oracle.max_threads()
+    P = problems.brio_wu()
+    out = {"workload": "Brio-Wu 1D nx=800 to t=0.1, FP64, RK4, hyperdiffusion, Courant 0.8"}
+    g = _start(abi.Context, P)
+    g.lib.sac_get_stream.argtypes = [ctypes.c_void_p]
+    g.lib.sac_get_stream.restype = ctypes.c_void_p
+    st = torch.cuda.ExternalStream(g.lib.sac_get_stream(g.h))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    n = _to_tmax(g, P.tmax)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    wg = g.download()
+    g.close()
+    out["gpu"] = {"steps": n, "ms": ms, "cell_updates_per_s": P.ncells * n / (ms / 1e3)}
+    for threads in (nthreads, 1):
+        oracle.set_threads(threads)
+        o = _start(oracle.Oracle, P)
+        t0 = time.perf_counter()
+        n2 = _to_tmax(o, P.tmax)
+        el = time.perf_counter() - t0
+        wo = o.download()
+        o.close()
+        out[f"cpu_{threads}_threads"] = {"steps": n2, "s": el, "cell_updates_per_s": P.ncells * n2 / el}
+    oracle.set_threads(nthreads)
+    out["gpu_vs_oracle_rel_l2"] = float(np.linalg.norm((wg - wo)[2:-2, :6]) / np.linalg.norm(wo[2:-2, :6]))
+    return out
+
+
+def batch_cpu_workload(steps=5):
+    """The CPU oracle on one 288 x 288 Orszag-Tang instance (the batch's mean size)
+    on all host threads: one untimed step, then `steps` timed ones."""
+    from oracle import oracle
+
+    from sac_b200 import problems
+    oracle.build()
+    nthreads = oracle.max_threads()
+    Q = problems.orszag_tang((288, 288), beta=2.0)
+    o = _start(oracle.Oracle, Q)
+    t = 0.0
+    for it in range(steps + 1):
+        if it == 1:
+            t0 = time.perf_counter()
+        dt = o.getdt(it)
+        o.advect(dt, t, it)
+        t += dt
+    el = time.perf_counter() - t0
+    o.close()
+    return {"workload": "one Orszag-Tang instance 288 x 288, FP64, RK4, hyperdiffusion (CPU oracle)",
+            "steps": steps, "s": el, "cell_updates_per_s": Q.ncells * steps / el, "threads": nthreads}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -406,7 +498,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--legs", default="fp64,e2e,fp32,cpu",
                     help="comma list of fp64, e2e, fp32, cpu (profiling runs select one kernel family)")
+    ap.add_argument("--workload", default="stratified", choices=["stratified", "briowu", "batch-cpu"],
+                    help="stratified: the headline line; briowu / batch-cpu: the small configurations' legs")
     args = ap.parse_args()
+    if args.workload != "stratified":
+        res = briowu_workload() if args.workload == "briowu" else batch_cpu_workload()
+        print(json.dumps(res), flush=True)
+        return 0
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
