@@ -67,3 +67,56 @@ def test_driver_on_the_device_matches_the_oracle(tmp_path):
     lo = open(tmp_path / "o.log").read().splitlines()
     lg = open(tmp_path / "g.log").read().splitlines()
     assert len(lo) == len(lg)
+
+
+def test_2d_run_applies_the_default_powell_source(tmp_path):
+    """A 2D par without divbfix runs with the Powell source (par/DEFAULT:46), in
+    program vac's dimensionally split loop (xyyx): equal to the oracle driven by
+    hand with divbfix=1 the same way, and different from divbfix=0."""
+    from sac_b200 import params, problems
+
+    P = problems.random_problem((14, 12), ndir=3, seed=45, types=["cont", "cont", "periodic", "periodic"],
+                                grav=(-0.7, 0.3, 0.0), nu=1.0, courantpar=0.4)
+    names = "x y rho m1 m2 m3 e b1 b2 b3 eb rhob bg1 bg2 bg3 gamma eta grav1 grav2 nu"
+    eqpar = np.array([P.params.gamma, 0.0, -0.7, 0.3, 1.0])
+    mesh = (slice(2, 16), slice(2, 14))
+    snap = fileio.Snapshot("2D random state", 0, 0.0, 2, 5, 13, (14, 12), eqpar, names,
+                           np.asfortranarray(P.x[mesh]), np.asfortranarray(P.w[mesh]))
+    ini = tmp_path / "r2d.ini"
+    fileio.write_binary(str(ini), [snap])
+    par = f"""
+ &filelist filenameini='{ini}' typefileini='binary'
+    filename='{tmp_path}/r.log', '{tmp_path}/r.out' typefileout='binary' /
+ &savelist ditsave=100,6 /
+ &stoplist itmax=6 /
+ &methodlist typefull=8*'cd4',5*'nul' typeadvance='fourstep' /
+ &boundlist typeB=13*'cont',13*'cont',13*'periodic',13*'periodic' /
+ &paramlist courantpar=0.4 /
+"""
+    r = vac.Run(par, user="gravvisc", context=Oracle)
+    assert r.params.divbfix == 1 and r.dimsplit
+    r.run(verbose=False)
+    got = fileio.read_binary(str(tmp_path / "r.out"))[-1]
+    assert got.it == 6
+
+    def by_hand(divbfix):
+        prm = r.params
+        prm.divbfix = divbfix
+        o = Oracle(prm)
+        o.set_grid(2, 3, r.ixGhi, r.ixM, r.x)
+        o.set_boundaries(params.pack_typeB(r.types), 4)
+        o.upload(r.w)
+        o.getboundary(0.0)
+        t = 0.0
+        for it in range(6):
+            dt = o.getdt(it)
+            order = (1, 2) if it % 2 == 0 else (2, 1)  # typedimsplit 'xyyx'
+            for d in order:
+                o.advect(dt, t, it, method="cd4", iws=r.iws, idimmin=d, idimmax=d)
+            t += dt
+        w = o.download()
+        o.close()
+        return w[mesh]
+
+    np.testing.assert_array_equal(got.w, by_hand(1))
+    assert np.abs(got.w - by_hand(0)).max() > 1e-10
