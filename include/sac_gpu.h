@@ -136,11 +136,14 @@ sac_status sac_download(sac_ctx* c, double* w);
 sac_status sac_getboundary(sac_ctx* c, double t);
 
 /* On return *dt holds the step of the dt block of the main loop, src/vac.t:61-70
- * (dtpar, getdt_courant, getdt, getdt_special, dtcantgrow).  it is the step number. */
+ * (dtpar, getdt_courant, getdt with getdt_res for eta > 0, getdt_special,
+ * dtcantgrow).  it is the step number. */
 sac_status sac_getdt(sac_ctx* c, double* dt, int it);
 
 /* method: typefull1 ('cd4' | 'source' | 'nul'); iws: iws(1:nw+1), iws(nw+1)=count,
- * or NULL for all advanced variables. */
+ * or NULL for all advanced variables.  The unsplit sources are the user module's
+ * (gravity, hyperdiffusion, driver), then addsource's resistive (eta > 0) and
+ * Powell (divbfix, ndim > 1) terms. */
 sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmin, int idimmax,
                       double dt, double t, int it);
 
@@ -195,8 +198,9 @@ sac_status sac_getdt_static(sac_ctx* c, double* dt, int it);
  * two ghost layers per side, its own coordinates and state.  Boundary types that
  * store ghost values (fixed, fixed1, grad1) and the Slog driver are not available
  * here (SAC_ERR_UNSUPPORTED), nor is a user resistivity (eta < 0); constant
- * resistivity (eta > 0) and the Powell source (divbfix, ndim = 2) are.  The Gaussian drivers (strat, tube) take their
- * amplitude and frequency per instance (sac_batch_set_driver).
+ * resistivity (eta > 0) and the Powell source (divbfix, ndim = 2) are.  The
+ * Gaussian drivers (strat, tube) take their amplitude and frequency per instance
+ * (sac_batch_set_driver).
  *
  * Host arrays are the instances' Fortran-order blocks one after another:
  *   x: instance i contributes x(ixG^T,ndim), w: instance i contributes w(ixG^T,nw),
