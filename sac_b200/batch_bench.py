@@ -16,7 +16,6 @@ import argparse
 import json
 import time
 
-import numpy as np
 
 from . import batch, params
 

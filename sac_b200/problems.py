@@ -12,7 +12,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .params import (USR_NONE, USR_STRAT, USR_TUBE, USR_VISCOSITY, SacParams, make_params,
+from .params import (USR_NONE, USR_STRAT, USR_TUBE, SacParams, make_params,
                      pack_typeB)
 
 DIXB = 2
