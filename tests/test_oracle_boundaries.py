@@ -133,3 +133,29 @@ def test_later_fill_restores_the_captured_values(nx, periodic_dims, seed):
     o.upload(w1)
     o.getboundary(0.0)
     np.testing.assert_array_equal(o.download(), _fill(P, w1, fix))
+
+
+def test_fills_match_for_random_shapes_and_types():
+    """Hypothesis-drawn grids (1D-3D, 5 to 9 mesh cells per dimension), boundary
+    types per region and variable and periodic dimensions: first and later fill."""
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    @settings(max_examples=30, deadline=None, derandomize=True)
+    @given(st.lists(st.integers(5, 9), min_size=1, max_size=3), st.integers(0, 7), st.integers(0, 2 ** 16))
+    def check(nx, periodic_mask, seed):
+        nd = len(nx)
+        periodic_dims = tuple(d for d in range(nd) if (periodic_mask >> d) & 1)
+        P = problems.random_problem(tuple(nx), ndir=3 if nd > 1 else 2, seed=seed)
+        nw = P.w.shape[-1]
+        P.typeB = _types(nd, nw, periodic_dims, seed)
+        o = _util.start(Oracle, P)
+        first = o.download()
+        np.testing.assert_array_equal(first, _fill(P, P.w))
+        w1 = first + 0.1 * np.random.default_rng(seed).standard_normal(first.shape)
+        o.upload(w1)
+        o.getboundary(0.0)
+        np.testing.assert_array_equal(o.download(), _fill(P, w1, _capture(P, first)))
+        o.close()
+
+    check()

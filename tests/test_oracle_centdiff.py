@@ -130,3 +130,33 @@ def test_flux_divergence_step_matches_numpy(nx, ndir, split):
     nadv = 2 * P.ndir + 2
     assert np.abs(got[..., :nadv] - _util.mesh(P, w0)[..., :nadv]).max() > 1e-6  # the fluxes act
     np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
+
+
+def test_flux_divergence_for_random_shapes():
+    """Hypothesis-drawn grids (1D-3D, 5 to 9 mesh cells per dimension), ndir and a
+    split dimension: one cd4 step, bit for bit."""
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    @settings(max_examples=20, deadline=None, derandomize=True)
+    @given(st.lists(st.integers(5, 9), min_size=1, max_size=3), st.integers(0, 2 ** 16), st.booleans(),
+           st.integers(0, 3))
+    def check(nx, seed, ndir3, split):
+        nd = len(nx)
+        ndir = 3 if (ndir3 or nd == 3) else max(nd, 2)
+        P = problems.random_problem(tuple(nx), ndir=ndir, seed=seed, types=["cont", "cont"] * nd,
+                                    user=params.USR_NONE, typeadvance="onestep")
+        o = _util.start(Oracle, P)
+        w0 = o.download()
+        if split == 0 or split > nd:
+            o.advect(37.0, 0.0, 0)
+            dims = list(range(nd))
+        else:
+            o.advect(37.0, 0.0, 0, idimmin=split, idimmax=split)
+            dims = [split - 1]
+        got = _util.mesh(P, o.download())
+        o.close()
+        nadv = 2 * P.ndir + 2
+        np.testing.assert_array_equal(got[..., :nadv], _centdiff4(P, w0, 37.0, dims)[..., :nadv])
+
+    check()

@@ -279,3 +279,31 @@ def test_first_dt_matches_numpy(nx, ndir):
         dtgrav = min(dtgrav, 1.0 / np.sqrt(m))
     want = min(want, dtgrav)
     assert dt == want
+
+
+def test_hyperdiffusion_for_random_shapes():
+    """Hypothesis-drawn grids (1D-3D, 5 to 9 mesh cells per dimension), ndir and
+    periodic dimensions: one hyperdiffusion step, bit for bit."""
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    @settings(max_examples=20, deadline=None, derandomize=True)
+    @given(st.lists(st.integers(5, 9), min_size=1, max_size=3), st.integers(0, 7), st.integers(0, 2 ** 16),
+           st.booleans())
+    def check(nx, periodic_mask, seed, ndir3):
+        nd = len(nx)
+        ndir = 3 if (ndir3 or nd == 3) else max(nd, 2)
+        types = []
+        for d in range(nd):
+            types += ["periodic", "periodic"] if (periodic_mask >> d) & 1 else ["cont", "symm"]
+        P = problems.random_problem(tuple(nx), ndir=ndir, seed=seed, types=types, user=params.USR_GRAVVISC,
+                                    grav=(0.0, 0.0, 0.0), typeadvance="onestep")
+        o = _util.start(Oracle, P)
+        w0 = o.download()
+        o.advect(37.0, 0.0, 0, method="source")
+        got = _util.mesh(P, o.download())
+        o.close()
+        nadv = 2 * P.ndir + 2
+        np.testing.assert_array_equal(got[..., :nadv], Visc(P, w0, 37.0).step()[..., :nadv])
+
+    check()
