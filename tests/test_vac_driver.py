@@ -120,3 +120,33 @@ def test_2d_run_applies_the_default_powell_source(tmp_path):
 
     np.testing.assert_array_equal(got.w, by_hand(1))
     assert np.abs(got.w - by_hand(0)).max() > 1e-10
+
+
+def _par_io(tmp, tag, extra_file="", itmax=5):
+    return f"""
+ &filelist filenameini='{INI}'
+    filename='{tmp}/{tag}.log', '{tmp}/{tag}.out'
+    typefileout='binary' {extra_file} /
+ &savelist itsave(1,2)=0 ditsave=100,1 /
+ &stoplist itmax={itmax} /
+ &methodlist wnames='rhop m1 m2 Ep b1p b2p rhob Eb b1b b2b'
+    typefull=6*'cd4',4*'nul' typeadvance='fourstep' /
+ &boundlist typeB=40*'cont' /
+ &paramlist courantpar=0.8 /
+"""
+
+
+def test_snapshotout_starts_a_new_file_every_n_saves(tmp_path):
+    # savefile (src/vacio.t:901-958): after every snapshotout saves the output
+    # continues in filename_<number of the next save>
+    vac.Run(_par_io(tmp_path, "s", "snapshotout=2"), user="gravvisc", context=Oracle).run(verbose=False)
+    its = {name: [s.it for s in _snapshots(tmp_path / name)] for name in ("s.out", "s.out_3", "s.out_5")}
+    assert its == {"s.out": [0, 1], "s.out_3": [2, 3], "s.out_5": [4, 5]}
+
+
+def test_fullgridout_saves_the_ghost_cells(tmp_path):
+    r = vac.Run(_par_io(tmp_path, "f", "fullgridout=T", itmax=2), user="gravvisc", context=Oracle)
+    r.run(verbose=False)
+    last = _snapshots(tmp_path / "f.out")[-1]
+    assert last.it == 2 and last.nx == tuple(r.ixGhi)
+    np.testing.assert_array_equal(last.w, r.ctx.download())
