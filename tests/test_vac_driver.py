@@ -150,3 +150,23 @@ def test_fullgridout_saves_the_ghost_cells(tmp_path):
     last = _snapshots(tmp_path / "f.out")[-1]
     assert last.it == 2 and last.nx == tuple(r.ixGhi)
     np.testing.assert_array_equal(last.w, r.ctx.download())
+
+
+def test_log_lines_hold_the_volume_weighted_means(tmp_path):
+    """savefilelog_default (src/vacio.t:1094-1149): it, t, dt and, per variable,
+    sum(dvolume w)/volume over the mesh, written (i7,100(1pe13.5))."""
+    import _util
+
+    r = vac.Run(_par(tmp_path, "m"), user="gravvisc", context=Oracle).run(verbose=False)
+    snaps = {s.it: s for s in _snapshots(tmp_path / "m.out")}
+    lines = open(tmp_path / "m.log").read().splitlines()[2:]
+    dv = _util.gridsetup1_dx(r)[2:-2, 0]  # 1D: dvolume = dx on the mesh
+    # the log saves every 5 steps from it=5; the .out file also at it=0 (itsave(1,2)=0)
+    assert [int(x[:7]) for x in lines] == [5, 10, 15, 20]
+    for line in lines:
+        it = int(line[:7])
+        vals = [float(line[7 + 13 * k: 20 + 13 * k]) for k in range((len(line) - 7) // 13)]
+        s = snaps[it]
+        assert vals[0] == pytest.approx(s.t, rel=1e-5, abs=1e-12)
+        want = (dv[:, None] * s.w).sum(axis=0) / dv.sum()
+        np.testing.assert_allclose(vals[2:2 + r.nw], want, rtol=1e-5, atol=1e-9)
