@@ -114,6 +114,11 @@ class Run:
         self.tmax = float(g("stoplist", "tmax", BIG))
         self.tmaxexact = bool(g("stoplist", "tmaxexact", False))
         self.dtmin = float(g("stoplist", "dtmin", SMALL))
+        # steady-state stop on the residual ||w_n+1 - w_n||, src/vac.t:88-98, 596-597
+        self.residmin = float(g("stoplist", "residmin", 0.0))
+        self.residmax = float(g("stoplist", "residmax", BIG))
+        self.use_residual = self.residmin > 0.0 or self.residmax < BIG
+        self.residual = BIG
         self.dtsave = [float(v) for v in _list(g("savelist", "dtsave"), 2, BIG)]
         self.ditsave = [int(v) for v in _list(g("savelist", "ditsave"), 2, BIGINT)]
         self.tsave = [[BIG], [BIG]]
@@ -160,6 +165,10 @@ class Run:
             typeadvance=typeadvance, typepred=pred, sourceunsplit=int(sourceunsplit),
             divbfix=int(divbfix), user=USER[user], device=device)
         self.slowsteps = int(g("paramlist", "slowsteps", 0))
+        if self.slowsteps == 1 and float(g("paramlist", "dtpar", -1.0)) > 0.0:
+            # src/vac.t:76 resets dtpar after the first step; the context's
+            # parameters are fixed at its creation
+            raise NotImplementedError("slowsteps=1 with dtpar>0 is outside the implemented path")
         self.types = params.typeB_from_par(pf, nw, 2 * ndim)
         self.wnames = g("methodlist", "wnames", snap.varnames)
         self.fileheadout = snap.header
@@ -232,8 +241,9 @@ class Run:
             name = self.filename[0]
             with open(name, "a" if self.log_open else "w") as f:
                 if not self.log_open:
-                    fileio.write_log_header(f, self.fileheadout, self.wnames, False)
-                f.write(fileio.format_log_line(self.it, self.t, self.dt, list(d.wmean)[: self.nw]) + "\n")
+                    fileio.write_log_header(f, self.fileheadout, self.wnames, self.use_residual)
+                f.write(fileio.format_log_line(self.it, self.t, self.dt, list(d.wmean)[: self.nw],
+                                               self.residual if self.use_residual else None) + "\n")
             self.log_open = True
 
     outname = None
@@ -242,7 +252,8 @@ class Run:
 
     # -- the main loop, src/vac.t:55-106 ---------------------------------------------
     def timetofinish(self):
-        return self.it >= self.itmax or self.t >= self.tmax or self.dt < self.dtmin
+        return (self.it >= self.itmax or self.t >= self.tmax or self.dt < self.dtmin
+                or (self.it > self.itmin and (self.residual < self.residmin or self.residual > self.residmax)))
 
     def step(self):
         for ifile in (0, 1):
@@ -257,6 +268,7 @@ class Run:
         if self.tmaxexact:
             dt = min(dt, self.tmax - self.t + SMALL)
         self.dt = dt
+        wold = self.ctx.download() if self.use_residual else None
         if self.dimsplit and self.ndim > 1:
             order = range(1, self.ndim + 1)
             if not ((self.it // 2) * 2 == self.it or self.typedimsplit == "xy"):
@@ -265,9 +277,24 @@ class Run:
                 self.ctx.advect(dt, self.t, self.it, method=self.method, iws=self.iws, idimmin=d, idimmax=d)
         else:
             self.ctx.advect(dt, self.t, self.it, method=self.method, iws=self.iws)
+        if self.use_residual:
+            self.residual = self.getresidual(wold, self.ctx.download())
         self.it += 1
         self.t += dt
         return True
+
+    def getresidual(self, wold, w):
+        """sqrt(sum over iw of ||w - wold||^2 / ||w||^2 (1 where ||w||^2 < smalldouble)
+        / nw) over the mesh, src/vac.t:88-98."""
+        sl = tuple(slice(2, 2 + n) for n in self.nx)
+        residual = 0.0
+        for iw in range(self.nw):
+            a, b = w[sl + (iw,)], wold[sl + (iw,)]
+            wnrm2 = float((a * a).sum())
+            if wnrm2 < SMALL:
+                wnrm2 = 1.0
+            residual = residual + float(((a - b) * (a - b)).sum()) / wnrm2
+        return float(np.sqrt(residual / self.nw))
 
     def run(self, verbose=True):
         t0 = time.time()

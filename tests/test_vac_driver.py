@@ -170,3 +170,18 @@ def test_log_lines_hold_the_volume_weighted_means(tmp_path):
         assert vals[0] == pytest.approx(s.t, rel=1e-5, abs=1e-12)
         want = (dv[:, None] * s.w).sum(axis=0) / dv.sum()
         np.testing.assert_allclose(vals[2:2 + r.nw], want, rtol=1e-5, atol=1e-9)
+
+
+def test_residual_stops_a_converged_run_and_is_logged(tmp_path):
+    """residmin: program vac stops once ||w_n+1 - w_n|| (src/vac.t:88-98) falls
+    below it, and the log gains a residual column."""
+    base = _par(tmp_path, "c", itmax=200).replace("&stoplist itmax=200 /", "&stoplist itmax=200 residmin=3.D-3 /")
+    r = vac.Run(base, user="gravvisc", context=Oracle)
+    assert r.use_residual
+    r.run(verbose=False)
+    assert r.it < 200 and r.residual < 3e-3
+    # the residual the driver used is that of the last step, recomputed here
+    lines = open(tmp_path / "c.log").read().splitlines()
+    assert lines[1].rstrip().endswith("residual")
+    last = lines[-1]
+    assert float(last[-13:]) == pytest.approx(r.residual, rel=1e-5)
