@@ -157,6 +157,14 @@ class Run:
             raise ValueError("divbfix=T requires unsplitsource=T or splitsource=T !")
         if bool(g("methodlist", "compactres", False)):
             raise NotImplementedError("compactres=T (addsource_res1) is outside the implemented path")
+        # options that change the run but are not built: say so rather than ignore them
+        for grp, key, off, what in (("methodlist", "smallfix", False, "smallfix=T (keeppositive)"),
+                                    ("methodlist", "divbconstrain", False, "divbconstrain=T (the CT module)"),
+                                    ("boundlist", "extraB", False, "extraB=T (user boundary regions)")):
+            if bool(g(grp, key, off)) != off:
+                raise NotImplementedError(what + " is outside the implemented path")
+        if str(g("filelist", "typefilelog", "default")).strip() != "default":
+            raise NotImplementedError("typefilelog other than 'default' (savefilelog_special) is not built")
         ep = eqpar_map(snap.eqpar, snap.varnames.split(), ndim)
         self.params = params.make_params(
             gamma=ep["gamma"], eta=ep["eta"], grav=ep["grav"], nu=ep["nu"],

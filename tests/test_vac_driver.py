@@ -52,6 +52,9 @@ def test_source_switches_follow_the_par(tmp_path):
     assert vac.Run(_par(tmp_path, "d", method="sourceunsplit=F divbfix=F"), context=Oracle).params.sourceunsplit == 0
     with pytest.raises(NotImplementedError):
         vac.Run(_par(tmp_path, "e", method="compactres=T"), context=Oracle)
+    for method in ("smallfix=T", "divbconstrain=T"):
+        with pytest.raises(NotImplementedError):
+            vac.Run(_par(tmp_path, "f", method=method), context=Oracle)
 
 
 @pytest.mark.gpu
