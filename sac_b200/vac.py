@@ -119,6 +119,9 @@ class Run:
         self.residmax = float(g("stoplist", "residmax", BIG))
         self.use_residual = self.residmin > 0.0 or self.residmax < BIG
         self.residual = BIG
+        # stop once this much CPU time has passed since the start, src/vac.t:599-600
+        self.cputimemax = float(g("stoplist", "cputimemax", BIG))
+        self.time0 = time.process_time()
         self.dtsave = [float(v) for v in _list(g("savelist", "dtsave"), 2, BIG)]
         self.ditsave = [int(v) for v in _list(g("savelist", "ditsave"), 2, BIGINT)]
         self.tsave = [[BIG], [BIG]]
@@ -260,8 +263,11 @@ class Run:
 
     # -- the main loop, src/vac.t:55-106 ---------------------------------------------
     def timetofinish(self):
-        return (self.it >= self.itmax or self.t >= self.tmax or self.dt < self.dtmin
-                or (self.it > self.itmin and (self.residual < self.residmin or self.residual > self.residmax)))
+        ok = (self.it >= self.itmax or self.t >= self.tmax or self.dt < self.dtmin
+              or (self.it > self.itmin and (self.residual < self.residmin or self.residual > self.residmax)))
+        if self.cputimemax < BIG and not ok:
+            ok = self.cputimemax <= time.process_time() - self.time0
+        return ok
 
     def step(self):
         for ifile in (0, 1):

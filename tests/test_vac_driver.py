@@ -188,3 +188,9 @@ def test_residual_stops_a_converged_run_and_is_logged(tmp_path):
     assert lines[1].rstrip().endswith("residual")
     last = lines[-1]
     assert float(last[-13:]) == pytest.approx(r.residual, rel=1e-5)
+
+
+def test_cputimemax_stops_the_run(tmp_path):
+    base = _par(tmp_path, "p", itmax=100000).replace("&stoplist itmax=100000 /", "&stoplist itmax=100000 cputimemax=0.D0 /")
+    r = vac.Run(base, user="gravvisc", context=Oracle).run(verbose=False)
+    assert r.it == 0  # the time budget is spent before the first step
