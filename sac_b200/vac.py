@@ -67,6 +67,26 @@ def eqpar_map(eqpar, names, ndim):
     return out
 
 
+def header_strings(fileheadout, varnames, ndim, ndir, user):
+    """setheaderstrings (src/vacio.t:844-898): a headline without '_' gains
+    '_mhd<ndim><ndir>'; varnames gains the equation parameter names 'gamma eta'
+    and, for the gravity modules, 'grav1 .. grav<ndim>' when missing (the
+    Stuart user parameters, sac/src/vacusrpar.t.stuart:10-12).  The reference
+    stops when the headline names another configuration than it was built for;
+    this library takes its configuration from the file, so it keeps the name."""
+    head = fileheadout.rstrip()
+    if "_" not in head:
+        head = head + "_mhd%d%d" % (ndim, ndir)
+    names = varnames.rstrip()
+    if names != "default":
+        if "gamma eta" not in names:
+            names = names + "   gamma eta"
+        special = " ".join("grav%d" % (d + 1) for d in range(ndim))
+        if user in ("gravvisc", "slog", "strat", "tube") and special not in names:
+            names = names + "   " + special
+    return head, names
+
+
 class Run:
     def __init__(self, par_text: str, user: str = "gravvisc", default_text: str = DEFAULT_PAR, device=0,
                  context=None):
@@ -168,7 +188,22 @@ class Run:
                 raise NotImplementedError(what + " is outside the implemented path")
         if str(g("filelist", "typefilelog", "default")).strip() != "default":
             raise NotImplementedError("typefilelog other than 'default' (savefilelog_special) is not built")
-        ep = eqpar_map(snap.eqpar, snap.varnames.split(), ndim)
+        # &methodlist is read after the initial file, so its eqpar and fileheadout
+        # override the file's (src/vacio.t:208-246)
+        eqpar = [float(v) for v in snap.eqpar]
+        mth = pf.groups.get("methodlist", {})
+        if "eqpar" in mth:
+            vals = mth["eqpar"] if isinstance(mth["eqpar"], list) else [mth["eqpar"]]
+            for i, val in enumerate(vals):
+                if i < len(eqpar):
+                    eqpar[i] = float(val)
+        for k, val in mth.items():
+            if k.startswith("eqpar(") and k.endswith(")"):
+                i = int(k[6:-1]) - 1
+                if 0 <= i < len(eqpar):
+                    eqpar[i] = float(val)
+        self.eqpar = eqpar
+        ep = eqpar_map(eqpar, snap.varnames.split(), ndim)
         self.params = params.make_params(
             gamma=ep["gamma"], eta=ep["eta"], grav=ep["grav"], nu=ep["nu"],
             courantpar=float(g("paramlist", "courantpar", 0.8)), dtpar=float(g("paramlist", "dtpar", -1.0)),
@@ -182,7 +217,8 @@ class Run:
             raise NotImplementedError("slowsteps=1 with dtpar>0 is outside the implemented path")
         self.types = params.typeB_from_par(pf, nw, 2 * ndim)
         self.wnames = g("methodlist", "wnames", snap.varnames)
-        self.fileheadout = snap.header
+        self.fileheadout, self.varnames = header_strings(str(g("methodlist", "fileheadout", snap.header)),
+                                                         snap.varnames, ndim, ndir, user)
         # state of the save logic, src/vac.t:179-184
         self.tsavelast = [self.t, self.t]
         self.itsavelast = [self.it, self.it]
@@ -239,8 +275,8 @@ class Run:
             else:
                 sl = tuple(slice(2, 2 + n) for n in self.nx)
                 xs, ws, nx = self.x[sl], w[sl], self.nx
-            s = fileio.Snapshot(self.fileheadout, self.it, self.t, self.ndim, len(self.snap.eqpar), self.nw,
-                                tuple(nx), np.asarray(self.snap.eqpar), self.snap.varnames, np.asfortranarray(xs),
+            s = fileio.Snapshot(self.fileheadout, self.it, self.t, self.ndim, len(self.eqpar), self.nw,
+                                tuple(nx), np.asarray(self.eqpar), self.varnames, np.asfortranarray(xs),
                                 np.asfortranarray(ws))
             if self.typefileout == "ascii":
                 fileio.write_ascii(self.outname, s, append=append)

@@ -194,3 +194,15 @@ def test_cputimemax_stops_the_run(tmp_path):
     base = _par(tmp_path, "p", itmax=100000).replace("&stoplist itmax=100000 /", "&stoplist itmax=100000 cputimemax=0.D0 /")
     r = vac.Run(base, user="gravvisc", context=Oracle).run(verbose=False)
     assert r.it == 0  # the time budget is spent before the first step
+
+
+def test_par_eqpar_and_fileheadout_override_the_initial_file(tmp_path):
+    base = _par(tmp_path, "q", itmax=2).replace("typefull=6*'cd4',4*'nul'",
+                                                "typefull=6*'cd4',4*'nul' eqpar(1)=1.4D0 fileheadout='par header'")
+    r = vac.Run(base, user="gravvisc", context=Oracle)
+    assert r.params.gamma == 1.4 and r.eqpar[0] == 1.4
+    r.run(verbose=False)
+    snap = _snapshots(tmp_path / "q.out")[-1]
+    # setheaderstrings: the physics suffix and the gravity module's parameter names
+    assert snap.header.strip() == "par header_mhd12" and snap.eqpar[0] == 1.4
+    assert snap.varnames.split()[-1] == "grav1" and "gamma eta" in snap.varnames
