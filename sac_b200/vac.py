@@ -314,7 +314,9 @@ class Run:
         if self.timetofinish():
             return False
         if self.slowsteps > self.it - self.itmin + 1:
-            dt = dt * (1.0 - (1.0 - (self.it - self.itmin + 1.0) / self.slowsteps) ** 2)
+            # dt*(one-(one-(it-itmin+one)/slowsteps)**2), src/vac.t:79; **2 is a product
+            q = 1.0 - (self.it - self.itmin + 1.0) / self.slowsteps
+            dt = dt * (1.0 - q * q)
         if self.tmaxexact:
             dt = min(dt, self.tmax - self.t + SMALL)
         self.dt = dt
