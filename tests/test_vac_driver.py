@@ -206,3 +206,31 @@ def test_par_eqpar_and_fileheadout_override_the_initial_file(tmp_path):
     # setheaderstrings: the physics suffix and the gravity module's parameter names
     assert snap.header.strip() == "par header_mhd12" and snap.eqpar[0] == 1.4
     assert snap.varnames.split()[-1] == "grav1" and "gamma eta" in snap.varnames
+
+
+def test_slowsteps_scale_the_first_steps(tmp_path):
+    """slowsteps=3 (src/vac.t:79): dt times 1-(1-k/3)^2 for the steps k=1, 2."""
+    from sac_b200 import params
+
+    base = _par(tmp_path, "w", itmax=4).replace("&paramlist courantpar=0.8 /", "&paramlist courantpar=0.8 slowsteps=3 /")
+    r = vac.Run(base, user="gravvisc", context=Oracle)
+    r.run(verbose=False)
+    got = _snapshots(tmp_path / "w.out")[-1]
+
+    o = Oracle(r.params)
+    o.set_grid(1, 2, r.ixGhi, r.ixM, r.x)
+    o.set_boundaries(params.pack_typeB(r.types), 2)
+    o.upload(r.w)
+    o.getboundary(0.0)
+    t = 0.0
+    for it in range(4):
+        dt = o.getdt(it)
+        if 3 > it + 1:
+            q = 1.0 - (it + 1.0) / 3
+            dt = dt * (1.0 - q * q)
+        o.advect(dt, t, it, method="cd4", iws=r.iws)
+        t += dt
+    w = o.download()
+    o.close()
+    assert got.t == t
+    np.testing.assert_array_equal(got.w, w[2:-2])
