@@ -107,3 +107,24 @@ def test_headers_compile_as_c99_and_a_c_caller_links(tmp_path):
     assert out[5] == ("1" if status == "SAC_ERR_NODEVICE" else "0")
     assert int(out[1]) == ctypes.sizeof(params.SacParams)
     assert out[2] == "1" and out[3] == "fourstep" and float(out[4]) == 0.8
+
+
+def test_params_field_offsets_match_the_c_layout(tmp_path):
+    """Every field of sac_b200.params.SacParams sits at the offset the C compiler
+    gives the same field of sac_params (include/sac_gpu.h)."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc")
+    if cc is None:
+        pytest.skip("gcc not found")
+    names = [f[0] for f in params.SacParams._fields_]
+    src = tmp_path / "offsets.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "sac_gpu.h"\nint main(void) {\n'
+                   + "".join(f'  printf("%zu\\n", offsetof(sac_params, {n}));\n' for n in names)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "offsets"
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = [getattr(params.SacParams, n).offset for n in names]
+    assert got == want, list(zip(names, got, want))
