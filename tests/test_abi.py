@@ -109,22 +109,33 @@ def test_headers_compile_as_c99_and_a_c_caller_links(tmp_path):
     assert out[2] == "1" and out[3] == "fourstep" and float(out[4]) == 0.8
 
 
-def test_params_field_offsets_match_the_c_layout(tmp_path):
-    """Every field of sac_b200.params.SacParams sits at the offset the C compiler
-    gives the same field of sac_params (include/sac_gpu.h)."""
+def _c_offsets(tmp_path, header, ctype, names):
     import shutil
     import subprocess
 
     cc = shutil.which("gcc")
     if cc is None:
         pytest.skip("gcc not found")
-    names = [f[0] for f in params.SacParams._fields_]
-    src = tmp_path / "offsets.c"
-    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "sac_gpu.h"\nint main(void) {\n'
-                   + "".join(f'  printf("%zu\\n", offsetof(sac_params, {n}));\n' for n in names)
-                   + "  return 0;\n}\n")
-    exe = tmp_path / "offsets"
+    src = tmp_path / f"offsets_{ctype}.c"
+    src.write_text(f'#include <stdio.h>\n#include <stddef.h>\n#include "{header}"\nint main(void) {{\n'
+                   + "".join(f'  printf("%zu\\n", offsetof({ctype}, {n}));\n' for n in names)
+                   + f'  printf("%zu\\n", sizeof({ctype}));\n  return 0;\n}}\n')
+    exe = tmp_path / f"offsets_{ctype}"
     subprocess.run([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
-    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
-    want = [getattr(params.SacParams, n).offset for n in names]
-    assert got == want, list(zip(names, got, want))
+    return [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+
+
+@pytest.mark.parametrize("header,ctype,mirror", [("sac_gpu.h", "sac_params", "sac_b200.params:SacParams"),
+                                                 ("sac_fno.h", "sac_fno_gemm_desc", "sac_b200.fno_abi:GemmDesc"),
+                                                 ("sac_fno.h", "sac_fno_config", "sac_b200.fno_abi:FnoConfig")])
+def test_struct_layouts_match_the_c_headers(tmp_path, header, ctype, mirror):
+    """Every field of the ctypes mirrors sits at the offset the C compiler gives
+    the same field of the header's struct, and the sizes agree."""
+    import importlib
+
+    mod, cls = mirror.split(":")
+    S = getattr(importlib.import_module(mod), cls)
+    names = [f[0] for f in S._fields_]
+    got = _c_offsets(tmp_path, header, ctype, names)
+    want = [getattr(S, n).offset for n in names] + [ctypes.sizeof(S)]
+    assert got == want, list(zip(names + ["sizeof"], got, want))
