@@ -102,6 +102,17 @@ typedef struct sac_params {
   int alias_nu_grav3;  /* reproduce eqpar(nu_)==eqpar(grav3_) (src/vacusrpar.f:4-5) */
   int precision;       /* SAC_PREC_FP64 | SAC_PREC_FP32 */
   int device;          /* CUDA ordinal (ignored by the CPU oracle) */
+  /* &methodlist smallfix and its floors, src/vacio.t:44-45 (defaults :99-101 and
+   * par/DEFAULT:54).  With smallfix set, every boundary fill first runs
+   * keeppositive (src/vacphys.t:8-49) on the mesh: where rho'+rhob < smallrho the
+   * cell gets the vacuum state (m=0, rho'=vacuumrho-rhob, e' from smallp and b');
+   * then, if any thermal pressure is below max(0,smallp), nerror(toosmallp_) counts
+   * the fill and, for smallp > 0, e' is rebuilt from max(p,smallp) on the whole
+   * mesh.  The batched contexts reject smallfix with SAC_ERR_UNSUPPORTED. */
+  int smallfix;
+  double smallp;       /* default -1 */
+  double smallrho;     /* default -1 */
+  double vacuumrho;    /* default -1 */
 } sac_params;
 
 typedef struct sac_diag_out {
@@ -111,6 +122,14 @@ typedef struct sac_diag_out {
   double maxviscoef;       /* running max of nu over the current step (setnu) */
   double ctot[3];          /* last c_tot per dimension used by setnu */
   int nonfinite;           /* 1 if a NaN/Inf was seen in the mesh */
+  /* keeppositive's error record (smallfix): nerror(toosmallp_), the fills whose
+   * thermal pressure went below max(0,smallp); the step number of the first such
+   * fill (the it last passed to sac_getdt or sac_advect, 0 before either) and the
+   * minimum pressure over the mesh at that fill, which the reference prints then
+   * (src/vacphys.t:34-41) */
+  int nerror_toosmallp;
+  int toosmallp_it;
+  double toosmallp_min;
 } sac_diag_out;
 
 typedef struct sac_ctx sac_ctx;

@@ -77,6 +77,10 @@ struct Oracle {
   double ctot_last[3] = {0, 0, 0};
   int itmin = 0;
   bool itmin_set = false;
+  int it_now = 0;  // the step number last passed to getdt or advect
+  // nerror(toosmallp_) and what the first keeppositive error reports, src/vacphys.t:34-41
+  int nerror_toosmallp = 0, toosmallp_it = 0;
+  double toosmallp_min = 0;
   std::string err;
 
   long id(int i, int j, int k) const { return i + (long)nG[0] * (j + (long)nG[1] * k); }
@@ -864,9 +868,55 @@ void centdiff4(Oracle& o, double qdt, const std::vector<int>& iws, int dmin, int
 }
 
 // ---------------------------------------------------------------------------
+// keeppositive, src/vacphys.t:8-49, on ixM
+// ---------------------------------------------------------------------------
+void keeppositive(Oracle& o, Arr& w) {
+  const double g = o.par.gamma, smallp = o.par.smallp;
+  double *rho = o.V(w, o.rho_), *e = o.V(w, o.e_);
+  const double *rhob = o.V(w, o.rhob_), *eb = o.V(w, o.eb_);
+  auto sq = [&](int iw0, long c) {  // ^C&w(ix^S,iw0+^C)**2+
+    double s = 0;
+    for (int C = 1; C <= o.ndir; ++C) s += o.V(w, iw0 + C)[c] * o.V(w, iw0 + C)[c];
+    return s;
+  };
+  // where((rho+rhob) < smallrho): m=0, rho=vacuumrho-rhob, e=smallp/(gamma-1)+b**2/2-eb, :21-26
+  forR(o, o.ixM, [&](long c) {
+    if (rho[c] + rhob[c] < o.par.smallrho) {
+      for (int C = 1; C <= o.ndir; ++C) o.V(w, o.m0_ + C)[c] = 0.0;
+      rho[c] = o.par.vacuumrho - rhob[c];
+      e[c] = smallp / (g - 1.0) + 0.5 * sq(o.b0_, c) - eb[c];
+    }
+  });
+  Arr tmp(o.ncell, 0.0);
+  getpthermal(o, w, o.ixM, tmp);  // :29
+  const double floor = std::max(0.0, smallp);
+  bool toosmallp = false;
+  double mn = bigdouble;
+  for (int k = o.ixM.lo[2]; k <= o.ixM.hi[2]; ++k)
+    for (int j = o.ixM.lo[1]; j <= o.ixM.hi[1]; ++j)
+      for (int i = o.ixM.lo[0]; i <= o.ixM.hi[0]; ++i) {
+        const double p = tmp[o.id(i, j, k)];
+        if (p < floor) toosmallp = true;  // any(tmp(ix^S)<max(zero,smallp)), :32
+        mn = std::min(mn, p);
+      }
+  if (!toosmallp) return;
+  if (++o.nerror_toosmallp == 1) {  // :35-41
+    o.toosmallp_it = o.it_now;
+    o.toosmallp_min = mn;
+  }
+  // e = max(p,smallp)/(gamma-1) + (m**2/rho + b**2)/2 - eb over the whole mesh, :43-45;
+  // the kinetic term divides by the perturbed density alone, as written there
+  if (smallp > 0.0)
+    forR(o, o.ixM, [&](long c) {
+      e[c] = std::max(tmp[c], smallp) / (g - 1.0) + 0.5 * (sq(o.m0_, c) / rho[c] + sq(o.b0_, c)) - eb[c];
+    });
+}
+
+// ---------------------------------------------------------------------------
 // boundaries, src/vacgrid.t:9-512
 // ---------------------------------------------------------------------------
 void getboundary(Oracle& o, Arr& w) {
+  if (o.par.smallfix) keeppositive(o, w);  // src/vacgrid.t:220
   for (int iB = 0; iB < o.nB; ++iB) {
     const int d = o.idimB[iB];
     const Rg r = o.ixB[iB];
@@ -1330,6 +1380,7 @@ int oracle_getdt(oracle_ctx* cx, double* dt, int it) {
     o.itmin = it;
     o.itmin_set = true;
   }
+  o.it_now = it;
   double d;
   if (o.par.dtpar > 0.0) {
     d = o.par.dtpar;
@@ -1362,9 +1413,9 @@ int oracle_getdt(oracle_ctx* cx, double* dt, int it) {
 
 int oracle_advect(oracle_ctx* cx, const char* method, const int* iws, int idimmin, int idimmax, double dt,
                   double t, int it) {
-  (void)it;
   Oracle& o = cx->o;
   if (!o.state_set || !o.bc_set) return SAC_ERR_STATE;
+  o.it_now = it;
   std::vector<int> v;
   if (iws) {
     int n = iws[o.nw];
@@ -1423,6 +1474,9 @@ int oracle_diag(oracle_ctx* cx, sac_diag_out* out) {
   out->maxviscoef = o.maxviscoef;
   for (int d = 0; d < 3; ++d) out->ctot[d] = o.ctot_last[d];
   out->nonfinite = nonfinite;
+  out->nerror_toosmallp = o.nerror_toosmallp;
+  out->toosmallp_it = o.toosmallp_it;
+  out->toosmallp_min = o.toosmallp_min;
   return SAC_OK;
 }
 

@@ -45,6 +45,10 @@ class SacParams(ctypes.Structure):
         ("alias_nu_grav3", ctypes.c_int),
         ("precision", ctypes.c_int),
         ("device", ctypes.c_int),
+        ("smallfix", ctypes.c_int),
+        ("smallp", ctypes.c_double),
+        ("smallrho", ctypes.c_double),
+        ("vacuumrho", ctypes.c_double),
     ]
 
 
@@ -56,6 +60,9 @@ class SacDiag(ctypes.Structure):
         ("maxviscoef", ctypes.c_double),
         ("ctot", ctypes.c_double * 3),
         ("nonfinite", ctypes.c_int),
+        ("nerror_toosmallp", ctypes.c_int),
+        ("toosmallp_it", ctypes.c_int),
+        ("toosmallp_min", ctypes.c_double),
     ]
 
 
@@ -77,6 +84,8 @@ def default_params() -> SacParams:
     p.alias_nu_grav3 = 0
     p.precision = PREC_FP64
     p.device = 0
+    p.smallfix = 0  # par/DEFAULT:54
+    p.smallp = p.smallrho = p.vacuumrho = -1.0  # src/vacio.t:99-101
     return p
 
 
