@@ -104,7 +104,7 @@ typedef struct sac_params {
   int device;          /* CUDA ordinal (ignored by the CPU oracle) */
   /* &methodlist smallfix and its floors, src/vacio.t:44-45 (defaults :99-101 and
    * par/DEFAULT:54).  With smallfix set, every boundary fill first runs
-   * keeppositive (src/vacphys.t:8-49) on the mesh: where rho'+rhob < smallrho the
+   * keeppositive (src/vacphys.t.mhd:8-49) on the mesh: where rho'+rhob < smallrho the
    * cell gets the vacuum state (m=0, rho'=vacuumrho-rhob, e' from smallp and b');
    * then, if any thermal pressure is below max(0,smallp), nerror(toosmallp_) counts
    * the fill and, for smallp > 0, e' is rebuilt from max(p,smallp) on the whole
@@ -126,7 +126,7 @@ typedef struct sac_diag_out {
    * thermal pressure went below max(0,smallp); the step number of the first such
    * fill (the it last passed to sac_getdt or sac_advect, 0 before either) and the
    * minimum pressure over the mesh at that fill, which the reference prints then
-   * (src/vacphys.t:34-41) */
+   * (src/vacphys.t.mhd:34-41) */
   int nerror_toosmallp;
   int toosmallp_it;
   double toosmallp_min;

@@ -10,10 +10,11 @@
 // scripts (inipar/*.py, run to make tests/golden fixtures), by numpy
 // transcriptions of the Fortran array statements of centdiff4, addsource_visc
 // with setnu, the gravity, Powell and resistive sources, the first getdt,
-// getboundary and, composed from them, a whole RK4 step, each equal to this
-// file's result bit for bit (tests/test_oracle_centdiff.py,
+// getboundary, keeppositive and, composed from them, a whole RK4 step, each
+// equal to this file's result bit for bit (tests/test_oracle_centdiff.py,
 // tests/test_oracle_visc.py, tests/test_oracle_sources.py,
-// tests/test_oracle_boundaries.py, tests/test_oracle_rk4.py), by physics invariants
+// tests/test_oracle_boundaries.py, tests/test_oracle_keeppositive.py,
+// tests/test_oracle_rk4.py), by physics invariants
 // (tests/test_oracle_physics.py) and by the independently written per-cell CUDA
 // path agreeing with it to 1e-12 (tests/test_gpu_*.py).
 //
@@ -78,7 +79,7 @@ struct Oracle {
   int itmin = 0;
   bool itmin_set = false;
   int it_now = 0;  // the step number last passed to getdt or advect
-  // nerror(toosmallp_) and what the first keeppositive error reports, src/vacphys.t:34-41
+  // nerror(toosmallp_) and what the first keeppositive error reports, src/vacphys.t.mhd:34-41
   int nerror_toosmallp = 0, toosmallp_it = 0;
   double toosmallp_min = 0;
   std::string err;
@@ -868,7 +869,7 @@ void centdiff4(Oracle& o, double qdt, const std::vector<int>& iws, int dmin, int
 }
 
 // ---------------------------------------------------------------------------
-// keeppositive, src/vacphys.t:8-49, on ixM
+// keeppositive, src/vacphys.t.mhd:8-49, on ixM
 // ---------------------------------------------------------------------------
 void keeppositive(Oracle& o, Arr& w) {
   const double g = o.par.gamma, smallp = o.par.smallp;

@@ -56,6 +56,8 @@ struct sac_ctx {
   double* stg = nullptr;  // FP64 staging block for FP32 upload/download
   double drvA = 0.0;
   unsigned long long* red = nullptr;  // 0..2 ctot, 3 maxnu, 4 courant, 5 divb max, 6 divb sq (as double)
+  unsigned long long* kp = nullptr;   // keeppositive's words (smallfix only), see k_keeppos_scan
+  int it_now = 0;                     // the step number last passed to sac_getdt or sac_advect
   double* fixB = nullptr;
   long fixoff[6] = {0, 0, 0, 0, 0, 0}, slab[6] = {0, 0, 0, 0, 0, 0};
   int8_t* d_type = nullptr;
@@ -176,11 +178,12 @@ void release(sac_ctx* c) {
   for (auto& p : c->P)
     if (p) cudaFree(p), p = nullptr;
   for (void* p : {(void*)c->BG, c->D, c->F, c->R, c->X, (void*)c->x, (void*)c->dx, (void*)c->drv,
-                  (void*)c->stg, (void*)c->red, (void*)c->fixB, (void*)c->d_type, (void*)c->d_fixed})
+                  (void*)c->stg, (void*)c->red, (void*)c->kp, (void*)c->fixB, (void*)c->d_type,
+                  (void*)c->d_fixed})
     if (p) cudaFree(p);
   c->BG = c->x = c->dx = c->drv = c->stg = c->fixB = nullptr;
   c->D = c->F = c->R = c->X = nullptr;
-  c->red = nullptr;
+  c->red = c->kp = nullptr;
   c->d_type = nullptr;
   c->d_fixed = nullptr;
 }
@@ -218,6 +221,8 @@ void launch_bound(sac_ctx* c, const BcArgs& b, int nvar) {
   Prof pr(c, SAC_K_BOUND);
   k_bound<S><<<(unsigned)((tot + bs - 1) / bs), bs, 0, c->stream>>>(b, ns[0], ns[1], ns[2], nvar);
 }
+
+sac_status keeppositive(sac_ctx* c, void* A);
 
 // advect1 (src/vac.t:490-549): out = base + qdt R(wct), then getboundary(out)
 template <typename S>
@@ -293,6 +298,11 @@ sac_status advect1_t(sac_ctx* c, const std::string& method, double qdt, int dmin
   } else if (base != out) {
     CK(cudaMemcpyAsync(out, base, c->es * g.np * g.ncell, cudaMemcpyDeviceToDevice, c->stream));
   }
+  if (c->par.smallfix) {  // getboundary's keeppositive, src/vacgrid.t:220
+    if (epi != EPI_PLAIN) return fail(c, SAC_ERR_STATE, "smallfix needs the unfused Runge-Kutta stages");
+    sac_status st = keeppositive(c, out);
+    if (st != SAC_OK) return st;
+  }
   BcArgs b = bc_args(c, out);
   if (epi == EPI_RK4_S3) {
     b.mode = 1;
@@ -325,6 +335,209 @@ template <typename S>
 __global__ void k_lin_threestep_b(S* w, const S* w2, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
     w[i] = w[i] / S(3) + w2[i] * S(2.0 / 3);
+}
+
+// The two whole-grid combinations of 'fourstep' (src/vac.t:450,454), for runs
+// whose fills change the mesh (keeppositive), so that they cannot be folded into
+// the stage stores: w1 = (w1 + 2 w2 + w3 - 4 w)/3, and w = w + w1.
+template <typename S>
+__global__ void k_rk4_acc(S* w1, const S* w2, const S* w3, const S* w, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    w1[i] = (w1[i] + S(2) * w2[i] + w3[i] - S(4) * w[i]) / S(3);
+}
+template <typename S>
+__global__ void k_rk4_final(S* w, const S* w1, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    w[i] = w[i] + w1[i];
+}
+
+// ---------------------------------------------------------------------------
+// keeppositive (src/vacphys.t.mhd:8-49) on the mesh of one advanced array, run at
+// the start of every boundary fill when smallfix is set (src/vacgrid.t:220).
+// kp[0]: a mesh pressure fell below max(0,smallp) in this fill; kp[1]: the
+// order key of this fill's minimum pressure; kp[2]: nerror(toosmallp_);
+// kp[3], kp[4]: step number and minimum-pressure key of the first error.
+// ---------------------------------------------------------------------------
+// a 64-bit key whose unsigned order is the order of the doubles (no NaN)
+__device__ __forceinline__ unsigned long long order_key(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+double order_key_value(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  double v;
+  std::memcpy(&v, &b, sizeof(v));
+  return v;
+}
+
+// getpthermal (src/vacphys0.t.mhd:163-183) of one cell from its loaded fields
+template <int NDIR>
+__device__ __forceinline__ double thermal_pressure(const double* m, const double* b, const double* bg, double rho,
+                                                   double rhob, double e, double gamma) {
+  double m2 = m[0] * m[0], b2 = b[0] * b[0], bb = b[0] * bg[0];
+#pragma unroll
+  for (int C = 1; C < NDIR; ++C) {
+    m2 = m2 + m[C] * m[C];
+    b2 = b2 + b[C] * b[C];
+    bb = bb + b[C] * bg[C];
+  }
+  double q = 0.5 * m2 / (rho + rhob);
+  q = q + 0.5 * b2 + bb;
+  return (gamma - 1.0) * (e - q);
+}
+
+struct KeepPar {
+  double gamma, smallp, smallrho, vacuumrho;
+};
+
+// Pass 1: the vacuum state where rho'+rhob < smallrho (:21-26), then the thermal
+// pressure against max(0,smallp) (:29-32); one OR and one minimum per block.
+template <int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_keeppos_scan(const __grid_constant__ Geom g, S* __restrict__ wp,
+                                                      const double* __restrict__ bgv, const KeepPar k,
+                                                      unsigned long long* kp) {
+  __shared__ unsigned long long sh[8];
+  const long N = g.ncell;
+  constexpr int E = NDIR + 1;
+  const double pfloor = fmax(0.0, k.smallp);
+  bool low = false;
+  unsigned long long kmin = ~0ull;
+  // 32-bit decode: sac_set_grid keeps the grid's cell offsets below 2^31
+  const unsigned nm0 = g.hi[0] - g.lo[0] + 1, nm1 = g.hi[1] - g.lo[1] + 1, nm2 = g.hi[2] - g.lo[2] + 1;
+  const unsigned tot = nm0 * nm1 * nm2;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+    const unsigned q = t / nm0;
+    const long c = (g.lo[0] + (long)(t - q * nm0)) + g.st[1] * (g.lo[1] + (long)(q % nm1)) +
+                   g.st[2] * (g.lo[2] + (long)(q / nm1));
+    const double rhob = bgv[N + c], eb = bgv[c];
+    double rho = (double)wp[c], e = (double)wp[E * N + c];
+    double m[NDIR], b[NDIR], bg[NDIR];
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) {
+      m[C] = (double)wp[(1 + C) * N + c];
+      b[C] = (double)wp[(E + 1 + C) * N + c];
+      bg[C] = bgv[(2 + C) * N + c];
+    }
+    if (rho + rhob < k.smallrho) {
+      double b2 = b[0] * b[0];
+#pragma unroll
+      for (int C = 1; C < NDIR; ++C) b2 = b2 + b[C] * b[C];
+#pragma unroll
+      for (int C = 0; C < NDIR; ++C) {
+        m[C] = 0.0;
+        wp[(1 + C) * N + c] = S(0);
+      }
+      const S rs = (S)(k.vacuumrho - rhob), es = (S)(k.smallp / (k.gamma - 1.0) + 0.5 * b2 - eb);
+      wp[c] = rs;
+      wp[E * N + c] = es;
+      rho = (double)rs;  // the stored values, which the pressure below reads
+      e = (double)es;
+    }
+    const double p = thermal_pressure<NDIR>(m, b, bg, rho, rhob, e, k.gamma);
+    low = low || (p < pfloor);
+    if (p == p) kmin = min(kmin, order_key(p));
+  }
+  low = __syncthreads_or(low) != 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = kmin;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) kmin = min(kmin, sh[i]);
+    atomicMin(kp + 1, kmin);
+    if (low) atomicOr(kp, 1ull);
+  }
+}
+
+// Pass 2 (smallp > 0, after an error in this fill): e' rebuilt from max(p,smallp)
+// over the whole mesh, the kinetic term over rho' alone as the reference writes
+// it (:43-45).  p is recomputed from the same stored fields as pass 1 read.
+template <int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_keeppos_energy(const __grid_constant__ Geom g, S* __restrict__ wp,
+                                                        const double* __restrict__ bgv, const KeepPar k,
+                                                        const unsigned long long* kp) {
+  if (kp[0] == 0) return;
+  const long N = g.ncell;
+  constexpr int E = NDIR + 1;
+  const unsigned nm0 = g.hi[0] - g.lo[0] + 1, nm1 = g.hi[1] - g.lo[1] + 1, nm2 = g.hi[2] - g.lo[2] + 1;
+  const unsigned tot = nm0 * nm1 * nm2;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+    const unsigned q = t / nm0;
+    const long c = (g.lo[0] + (long)(t - q * nm0)) + g.st[1] * (g.lo[1] + (long)(q % nm1)) +
+                   g.st[2] * (g.lo[2] + (long)(q / nm1));
+    const double rhob = bgv[N + c], eb = bgv[c];
+    const double rho = (double)wp[c], e = (double)wp[E * N + c];
+    double m[NDIR], b[NDIR], bg[NDIR];
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) {
+      m[C] = (double)wp[(1 + C) * N + c];
+      b[C] = (double)wp[(E + 1 + C) * N + c];
+      bg[C] = bgv[(2 + C) * N + c];
+    }
+    const double p = thermal_pressure<NDIR>(m, b, bg, rho, rhob, e, k.gamma);
+    double m2 = m[0] * m[0], b2 = b[0] * b[0];
+#pragma unroll
+    for (int C = 1; C < NDIR; ++C) {
+      m2 = m2 + m[C] * m[C];
+      b2 = b2 + b[C] * b[C];
+    }
+    wp[E * N + c] = (S)(fmax(p, k.smallp) / (k.gamma - 1.0) + 0.5 * (m2 / rho + b2) - eb);
+  }
+}
+
+// Pass 3 (one thread): count the error, keep the first one's step and minimum,
+// and reset the per-fill words for the next fill.
+__global__ void k_keeppos_close(unsigned long long* kp, int it) {
+  if (kp[0]) {
+    kp[2] += 1;
+    if (kp[2] == 1) {
+      kp[3] = (unsigned long long)(long long)it;
+      kp[4] = kp[1];
+    }
+  }
+  kp[0] = 0;
+  kp[1] = ~0ull;
+}
+
+// keeppositive on the mesh of the advanced array A, at the start of a fill
+sac_status keeppositive(sac_ctx* c, void* A) {
+  if (!c->par.smallfix) return SAC_OK;
+  if (!c->kp) return fail(c, SAC_ERR_STATE, "smallfix: no error words (sac_set_grid allocates them)");
+  const Geom& g = c->g;
+  const KeepPar k{c->par.gamma, c->par.smallp, c->par.smallrho, c->par.vacuumrho};
+  const long nm = (long)(g.hi[0] - g.lo[0] + 1) * (g.hi[1] - g.lo[1] + 1) * (g.hi[2] - g.lo[2] + 1);
+  const int bs = 256;  // k_keeppos_scan reduces over exactly 8 warps
+  const unsigned nb = (unsigned)std::min<long>((nm + bs - 1) / bs, 148L * 8);
+  const bool energy = c->par.smallp > 0.0;
+  auto launch = [&](auto S0, auto ND) {
+    using S = decltype(S0);
+    constexpr int NDIR = decltype(ND)::value;
+    {
+      Prof pr(c, SAC_K_OTHER);
+      k_keeppos_scan<NDIR, S><<<nb, bs, 0, c->stream>>>(g, (S*)A, c->BG, k, c->kp);
+    }
+    if (energy) {
+      Prof pr(c, SAC_K_OTHER);
+      k_keeppos_energy<NDIR, S><<<nb, bs, 0, c->stream>>>(g, (S*)A, c->BG, k, c->kp);
+    }
+  };
+  auto by_ndir = [&](auto S0) {
+    switch (g.ndir) {
+      case 1: launch(S0, std::integral_constant<int, 1>{}); break;
+      case 2: launch(S0, std::integral_constant<int, 2>{}); break;
+      default: launch(S0, std::integral_constant<int, 3>{}); break;
+    }
+  };
+  if (c->prec == SAC_PREC_FP32)
+    by_ndir(0.0f);
+  else
+    by_ndir(0.0);
+  {
+    Prof pr(c, SAC_K_OTHER);
+    k_keeppos_close<<<1, 1, 0, c->stream>>>(c->kp, c->it_now);
+  }
+  CK(cudaGetLastError());
+  return SAC_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -453,6 +666,7 @@ void sac_default_params(sac_params* p) {
   p->sourceunsplit = 1;  // par/DEFAULT:44
   p->user = SAC_USR_NONE;
   p->precision = SAC_PREC_FP64;
+  p->smallp = p->smallrho = p->vacuumrho = -1.0;  // src/vacio.t:99-101; smallfix F, par/DEFAULT:54
 }
 
 sac_status sac_create(const sac_params* p, sac_ctx** out) {
@@ -584,6 +798,11 @@ sac_status sac_set_grid(sac_ctx* c, int ndim, int ndir, const int ixGhi[3], cons
   if (c->prec == SAC_PREC_FP32) CK(cudaMalloc(&c->stg, sizeof(double) * g.np * N));
   CK(cudaMalloc(&c->red, 8 * sizeof(unsigned long long)));
   CK(cudaMemsetAsync(c->red, 0, 8 * sizeof(unsigned long long), c->stream));
+  if (c->par.smallfix) {
+    static const unsigned long long kp0[5] = {0, ~0ull, 0, 0, ~0ull};
+    CK(cudaMalloc(&c->kp, sizeof(kp0)));
+    CK(cudaMemcpyAsync(c->kp, kp0, sizeof(kp0), cudaMemcpyHostToDevice, c->stream));
+  }
   CK(cudaMemsetAsync(c->R, 0, c->es * (size_t)nr_pairs(ndim) * N, c->stream));
   CK(cudaMemcpyAsync(c->x, hx.data(), sizeof(double) * ndim * N, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->dx, hdx.data(), sizeof(double) * ndim * N, cudaMemcpyHostToDevice, c->stream));
@@ -714,6 +933,8 @@ sac_status sac_getboundary(sac_ctx* c, double t) {
   if (!c->state_set || !c->bc_set) return fail(c, SAC_ERR_STATE, "state and boundaries must be set");
   CK(cudaSetDevice(c->dev));
   const Geom& g = c->g;
+  sac_status st = keeppositive(c, c->P[0]);  // src/vacgrid.t:220
+  if (st != SAC_OK) return st;
   BcArgs b = bc_args(c, c->P[0]);
   b.init = c->bc_init_done ? 0 : 1;
   if (c->prec == SAC_PREC_FP32)
@@ -757,6 +978,7 @@ static sac_status getdt_impl(sac_ctx* c, double* dt, int it, bool static_scratch
     c->itmin = it;
     c->itmin_set = true;
   }
+  c->it_now = it;
   const Geom& g = c->g;
   double d;
   if (c->par.dtpar > 0.0) {
@@ -842,7 +1064,6 @@ sac_status sac_getdt_static(sac_ctx* c, double* dt, int it) { return getdt_impl(
 
 sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmin, int idimmax, double dt, double t,
                       int it) {
-  (void)it;
   if (!c || !method) return SAC_ERR_ARG;
   if (!c->state_set || !c->bc_set) return fail(c, SAC_ERR_STATE, "state and boundaries must be set");
   if (!c->bc_init_done) return fail(c, SAC_ERR_STATE, "call sac_getboundary once before the first advect");
@@ -864,6 +1085,7 @@ sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmi
   } else {
     mask = (1u << g.np) - 1u;
   }
+  c->it_now = it;
   const int dmin = idimmin - 1, dmax = idimmax - 1;
   void *w = c->P[0], *w1 = c->P[1], *w2 = c->P[2], *w3 = c->P[3];
   const size_t bytes = c->es * g.np * g.ncell;
@@ -874,7 +1096,31 @@ sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmi
     st = (x);                     \
     if (st != SAC_OK) return st;  \
   } while (0)
-  if (ta == "fourstep") {
+  if (ta == "fourstep" && c->par.smallfix) {
+    // keeppositive changes the mesh of w3 and of w at their fills, before the
+    // combinations read them: the combinations run as passes of their own
+    const long n = (long)g.np * g.ncell;
+    RUN(advect1(c, m, dt / 2, dmin, dmax, t, w, w, w1, mask));
+    RUN(advect1(c, m, dt / 2, dmin, dmax, t, w1, w, w2, mask));
+    RUN(advect1(c, m, dt, dmin, dmax, t, w2, w, w3, mask));
+    {
+      Prof pr(c, SAC_K_OTHER);
+      if (c->prec == SAC_PREC_FP32)
+        k_rk4_acc<float><<<592, 256, 0, c->stream>>>((float*)w1, (const float*)w2, (const float*)w3,
+                                                     (const float*)w, n);
+      else
+        k_rk4_acc<double><<<592, 256, 0, c->stream>>>((double*)w1, (const double*)w2, (const double*)w3,
+                                                      (const double*)w, n);
+    }
+    RUN(advect1(c, m, dt / 6, dmin, dmax, t, w3, w, w, mask));
+    {
+      Prof pr(c, SAC_K_OTHER);
+      if (c->prec == SAC_PREC_FP32)
+        k_rk4_final<float><<<592, 256, 0, c->stream>>>((float*)w, (const float*)w1, n);
+      else
+        k_rk4_final<double><<<592, 256, 0, c->stream>>>((double*)w, (const double*)w1, n);
+    }
+  } else if (ta == "fourstep") {
     RUN(advect1(c, m, dt / 2, dmin, dmax, t, w, w, w1, mask));
     RUN(advect1(c, m, dt / 2, dmin, dmax, t, w1, w, w2, mask));
     RUN(advect1(c, m, dt, dmin, dmax, t, w2, w, w3, mask, EPI_RK4_S3, w1, w2));
@@ -986,6 +1232,13 @@ sac_status sac_diag(sac_ctx* c, sac_diag_out* out) {
   std::memcpy(&out->maxviscoef, &bits[3], sizeof(double));
   for (int d = 0; d < 3; ++d) std::memcpy(&out->ctot[d], &bits[d], sizeof(double));
   out->nonfinite = nonfinite;
+  if (c->kp) {
+    unsigned long long kp[5];
+    CK(cudaMemcpy(kp, c->kp, sizeof(kp), cudaMemcpyDeviceToHost));
+    out->nerror_toosmallp = (int)kp[2];
+    out->toosmallp_it = (int)(long long)kp[3];
+    out->toosmallp_min = kp[2] ? order_key_value(kp[4]) : 0.0;
+  }
   return SAC_OK;
 }
 

@@ -181,8 +181,7 @@ class Run:
         if bool(g("methodlist", "compactres", False)):
             raise NotImplementedError("compactres=T (addsource_res1) is outside the implemented path")
         # options that change the run but are not built: say so rather than ignore them
-        for grp, key, off, what in (("methodlist", "smallfix", False, "smallfix=T (keeppositive)"),
-                                    ("methodlist", "divbconstrain", False, "divbconstrain=T (the CT module)"),
+        for grp, key, off, what in (("methodlist", "divbconstrain", False, "divbconstrain=T (the CT module)"),
                                     ("boundlist", "extraB", False, "extraB=T (user boundary regions)")):
             if bool(g(grp, key, off)) != off:
                 raise NotImplementedError(what + " is outside the implemented path")
@@ -209,7 +208,11 @@ class Run:
             courantpar=float(g("paramlist", "courantpar", 0.8)), dtpar=float(g("paramlist", "dtpar", -1.0)),
             dtdiffpar=float(g("paramlist", "dtdiffpar", 0.5)), dtcantgrow=int(bool(g("paramlist", "dtcantgrow", False))),
             typeadvance=typeadvance, typepred=pred, sourceunsplit=int(sourceunsplit),
-            divbfix=int(divbfix), user=USER[user], device=device)
+            divbfix=int(divbfix), user=USER[user], device=device,
+            # keeppositive's switch and floors, src/vacio.t:44-45,99-101
+            smallfix=int(bool(g("methodlist", "smallfix", False))),
+            smallp=float(g("methodlist", "smallp", -1.0)), smallrho=float(g("methodlist", "smallrho", -1.0)),
+            vacuumrho=float(g("methodlist", "vacuumrho", -1.0)))
         self.slowsteps = int(g("paramlist", "slowsteps", 0))
         if self.slowsteps == 1 and float(g("paramlist", "dtpar", -1.0)) > 0.0:
             # src/vac.t:76 resets dtpar after the first step; the context's
@@ -359,7 +362,27 @@ class Run:
                 self.savefile(ifile)
         if verbose:
             print(f"Finish Advance {time.time() - t0:10.3f} sec   it={self.it} t={self.t:.6g}")
+            for line in self.final_report():
+                print(line)
         return self
+
+    def final_report(self):
+        """What program vac prints after the loop (src/vac.t:117-136): the dtmin and
+        cputimemax warnings and, with smallfix, keeppositive's error, first as it
+        reports it at the first occurrence (src/vacphys.t.mhd:36-40), then its count."""
+        out = []
+        if self.dt < self.dtmin:
+            out.append(" Warning: dt<dtmin !!!")
+        if time.process_time() - self.time0 > self.cputimemax:
+            out.append(" Warning: cputimemax exceeded !!!")
+        if self.params.smallfix:
+            d = self.ctx.diag()
+            if d.nerror_toosmallp > 0:
+                out.append(f"Too small pressure (code= 1) at it={d.toosmallp_it:7d}")
+                out.append(f" Value < smallp:  {d.toosmallp_min!r} {self.params.smallp!r}")
+                out.append(f"Error (code= 1) occurred {d.nerror_toosmallp:5d} times !!!")
+                out.append("Error description: Pressure below psmall")
+        return out
 
 
 def main(argv=None):

@@ -126,6 +126,7 @@ def _c_offsets(tmp_path, header, ctype, names):
 
 
 @pytest.mark.parametrize("header,ctype,mirror", [("sac_gpu.h", "sac_params", "sac_b200.params:SacParams"),
+                                                 ("sac_gpu.h", "sac_diag_out", "sac_b200.params:SacDiag"),
                                                  ("sac_fno.h", "sac_fno_gemm_desc", "sac_b200.fno_abi:GemmDesc"),
                                                  ("sac_fno.h", "sac_fno_config", "sac_b200.fno_abi:FnoConfig")])
 def test_struct_layouts_match_the_c_headers(tmp_path, header, ctype, mirror):

@@ -1,0 +1,106 @@
+"""keeppositive (smallfix) on the CUDA path against the CPU oracle.
+
+getboundary runs keeppositive (src/vacphys.t.mhd:8-49) on the mesh before every
+ghost fill when smallfix is set (src/vacgrid.t:220).  Its floors act on the
+Orszag-Tang vortex, which carries the whole state as perturbation: smallp at
+the initial pressure lifts every cell that falls below it, and smallrho just
+below the initial density puts rarefied cells into the vacuum state.  The FP64
+bar is the path's: 1e-12 relative L2 per variable of the oracle; the error
+record (count, first step, minimum pressure) must agree too."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from sac_b200 import abi, batch, params, problems
+
+import _util
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+FP32_RTOL = 1e-5
+
+
+def _ot(typeadvance="fourstep", smallrho=2.75):
+    P = problems.orszag_tang((32, 32), typeadvance=typeadvance)
+    P.params.smallfix = 1
+    P.params.smallp = 0.5  # the initial thermal pressure
+    P.params.smallrho = smallrho
+    P.params.vacuumrho = 2.75
+    return P
+
+
+def _compare(P, o, g, rtol):
+    wo = _util.mesh(P, o.download())
+    wg = _util.mesh(P, g.download())
+    assert np.isfinite(wg).all()
+    err = _util.rel_l2(wg, wo)[: 2 * P.ndir + 2]
+    assert err.max() <= rtol, f"{P.name}: rel L2 per variable {err}"
+
+
+def _records_agree(o, g, rtol=1e-12):
+    do, dg = o.diag(), g.diag()
+    assert dg.nerror_toosmallp == do.nerror_toosmallp > 0
+    assert dg.toosmallp_it == do.toosmallp_it
+    np.testing.assert_allclose(dg.toosmallp_min, do.toosmallp_min, rtol=rtol)
+
+
+@pytest.mark.parametrize("typeadvance", ["fourstep", "onestep", "twostep", "threestep", "sterck", "jameson"])
+def test_orszag_tang_floors_match_oracle(typeadvance):
+    P = _ot(typeadvance)
+    o = _util.start(Oracle, P)
+    g = _util.start(abi.Context, P)
+    dts = _util.run(o, 20)
+    dg = _util.run(g, 20)
+    np.testing.assert_allclose(dg, dts, rtol=1e-12, atol=0)
+    _compare(P, o, g, RTOL)
+    _records_agree(o, g)
+
+
+def test_floors_change_the_run():
+    """The floors act: with them the state differs from the run without."""
+    P = _ot()
+    g = _util.start(abi.Context, P)
+    dts = _util.run(g, 10)
+    P.params.smallfix = 0
+    h = _util.start(abi.Context, P)
+    _util.run(h, 10, dts=dts)
+    v = problems.var_index(P.ndir)
+    wg, wh = _util.mesh(P, g.download()), _util.mesh(P, h.download())
+    assert np.abs(wg[..., v["e"]] - wh[..., v["e"]]).max() > 1e-6
+    assert np.abs(wg[..., v["rho"]] - wh[..., v["rho"]]).max() > 1e-6
+    assert g.diag().nerror_toosmallp == 1 + 4 * 10
+
+
+def test_counting_only_leaves_the_state_to_the_oracle():
+    """smallp and smallrho at their defaults (-1): keeppositive only counts the
+    fills with a negative perturbed pressure (every one, in a background
+    problem); the 'fourstep' combinations run as passes of their own."""
+    P = problems.random_problem((14, 12), seed=51, types=["cont", "fixed", "periodic", "periodic"])
+    P.params.smallfix = 1
+    o = _util.start(Oracle, P)
+    g = _util.start(abi.Context, P)
+    dts = _util.run(o, 20, it0=3)
+    dg = _util.run(g, 20, it0=3)
+    np.testing.assert_allclose(dg, dts, rtol=1e-12, atol=0)
+    _compare(P, o, g, RTOL)
+    _records_agree(o, g)
+    assert g.diag().nerror_toosmallp == 1 + 4 * 20
+
+
+def test_fp32_orszag_tang_floors():
+    P = _ot(smallrho=-1.0)
+    o = _util.start(Oracle, P)
+    P.params.precision = params.PREC_FP32
+    g = _util.start(abi.Context, P)
+    dts = _util.run(o, 20)
+    _util.run(g, 20, dts=dts)
+    _compare(P, o, g, FP32_RTOL)
+    assert g.diag().nerror_toosmallp == o.diag().nerror_toosmallp
+
+
+def test_batch_rejects_smallfix():
+    prm = batch.ot_params()
+    prm.smallfix = 1
+    with pytest.raises(abi.SacError):
+        batch.Batch(prm, 2, 2, [(16, 16)])

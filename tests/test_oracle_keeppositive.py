@@ -1,6 +1,6 @@
 """The oracle's keeppositive against a numpy transcription of the Fortran (CPU).
 
-keeppositive (src/vacphys.t:8-49), which getboundary runs on the mesh before the
+keeppositive (src/vacphys.t.mhd:8-49), which getboundary runs on the mesh before the
 ghost fill when smallfix is set (src/vacgrid.t:220): the vacuum state where
 rho'+rhob < smallrho, the thermal pressure of getpthermal
 (src/vacphys0.t.mhd:163-183) against max(0,smallp), the error count, and for

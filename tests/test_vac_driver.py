@@ -52,9 +52,31 @@ def test_source_switches_follow_the_par(tmp_path):
     assert vac.Run(_par(tmp_path, "d", method="sourceunsplit=F divbfix=F"), context=Oracle).params.sourceunsplit == 0
     with pytest.raises(NotImplementedError):
         vac.Run(_par(tmp_path, "e", method="compactres=T"), context=Oracle)
-    for method in ("smallfix=T", "divbconstrain=T"):
-        with pytest.raises(NotImplementedError):
-            vac.Run(_par(tmp_path, "f", method=method), context=Oracle)
+    with pytest.raises(NotImplementedError):
+        vac.Run(_par(tmp_path, "f", method="divbconstrain=T"), context=Oracle)
+
+
+def test_smallfix_runs_keeppositive_and_reports(tmp_path):
+    """smallfix=T with its floors from &methodlist: with the defaults (-1) the
+    fills only count negative perturbed pressures and the snapshots equal those
+    of a run without it; with floors the run changes, and the end report gives
+    the first error and the count (src/vac.t:117-136, src/vacphys.t.mhd:36-40)."""
+    ref = vac.Run(_par(tmp_path, "r"), context=Oracle).run(verbose=False)
+    assert ref.final_report() == []
+    cnt = vac.Run(_par(tmp_path, "c", method="smallfix=T"), context=Oracle).run(verbose=False)
+    assert cnt.params.smallfix == 1 and cnt.params.smallp == -1.0
+    for a, b in zip(_snapshots(tmp_path / "c.out"), _snapshots(tmp_path / "r.out")):
+        np.testing.assert_array_equal(a.w, b.w)
+    rep = cnt.final_report()
+    assert rep[0].startswith("Too small pressure (code= 1) at it=") and rep[-1].endswith("Pressure below psmall")
+    n = int(rep[2].split("occurred")[1].split("times")[0])
+    assert 0 < n <= 1 + 4 * 20
+    flo = vac.Run(_par(tmp_path, "f", method="smallfix=T smallp=0.2D0 smallrho=0.2D0 vacuumrho=0.15D0"),
+                  context=Oracle).run(verbose=False)
+    assert (flo.params.smallp, flo.params.smallrho, flo.params.vacuumrho) == (0.2, 0.2, 0.15)
+    wf, wr = _snapshots(tmp_path / "f.out")[-1].w, _snapshots(tmp_path / "r.out")[-1].w
+    assert np.isfinite(wf).all() and np.abs(wf - wr).max() > 1e-3
+    assert "occurred    81 times" in flo.final_report()[2]
 
 
 @pytest.mark.gpu
