@@ -75,9 +75,9 @@ typedef struct sac_params {
   /* equation parameters eqpar(1:neqpar+nspecialpar), src/vacpar.t.mhd:26,
    * src/vacusrpar.f:3-6 */
   double gamma;   /* eqpar(gamma_) */
-  double eta;     /* eqpar(eta_): 0, or a constant resistivity > 0 (addsource_res2 with
-                   * compactres=F and getdt_res, src/vacphys.mhdres.t); eta < 0 (a user
-                   * specialeta) is SAC_ERR_UNSUPPORTED */
+  double eta;     /* eqpar(eta_): 0, or a constant resistivity > 0 (addsource_res2, or
+                   * addsource_res1 with compactres, and getdt_res, src/vacphys.mhdres.t);
+                   * eta < 0 (a user specialeta) is SAC_ERR_UNSUPPORTED */
   double grav[3]; /* eqpar(grav1_..grav3_) */
   double nu;      /* eqpar(nu_): hyperdiffusion on when |nu|>smalldouble */
   /* &paramlist, src/vacio.t:47 */
@@ -113,6 +113,11 @@ typedef struct sac_params {
   double smallp;       /* default -1 */
   double smallrho;     /* default -1 */
   double vacuumrho;    /* default -1 */
+  /* &methodlist compactres (par/DEFAULT:57, F): the resistive source in its compact
+   * form addsource_res1 (src/vacphys.mhdres.t:96-220), eta times the 3-point
+   * Laplacian of B into b and e plus eta J^2 into e, instead of addsource_res2.  The
+   * batched contexts reject it with SAC_ERR_UNSUPPORTED. */
+  int compactres;
 } sac_params;
 
 typedef struct sac_diag_out {

@@ -820,14 +820,62 @@ void addsource_res2(Oracle& o, double qdt, const std::vector<int>& iws, const Ar
   }
 }
 
+// addsource_res1, src/vacphys.mhdres.t:96-220 (compactres=T), for a constant
+// eta = eqpar(eta_) > 0: ensurebound(1,...) keeps ixO=ixM, and getcurrent runs on
+// ixO.  Per idir: tmp = eta * sum over idim of the 3-point Laplacian of
+// B_idir = b_idir + bg_idir, added to b_idir and, times B_idir, to e; then
+// eta * J**2 to e.
+void addsource_res1(Oracle& o, double qdt, const std::vector<int>& iws, const Arr& w, Arr& wnew, Work& wk) {
+  wk.init(o.ncell);
+  const long n = o.ncell;
+  Arr J[3];
+  for (Arr& a : J) a.assign(n, 0.0);
+  const Rg ixO = o.ixM;
+  const int idirmin = getcurrent(o, w, ixO, J, wk.f, wk.tmp);
+  const double eta = o.par.eta;  // eta(ixG^S)=eqpar(eta_), set at it==itmin (:121-122)
+  Arr &tmp = wk.f, &tmp2 = wk.tmp;
+  for (int idir = 0; idir < o.ndir; ++idir) {
+    forR(o, ixO, [&](long c) { tmp[c] = 0.0; });
+    const double *b = o.V(w, o.b0_ + 1 + idir), *bg = o.V(w, o.bg0_ + 1 + idir);
+    forR(o, o.ixG, [&](long c) { tmp2[c] = b[c] + bg[c]; });
+    for (int idim = 0; idim < o.ndim; ++idim) {  // :160-173
+      const long s = o.st[idim];
+      const double* dx = o.dx.data() + (long)idim * n;
+      forR(o, ixO, [&](long c) { tmp[c] = tmp[c] + (tmp2[c + s] - 2 * tmp2[c] + tmp2[c - s]) / (dx[c] * dx[c]); });
+    }
+    forR(o, ixO, [&](long c) { tmp[c] = tmp[c] * eta; });
+    for (int iw : iws) {  // :191-201
+      double* wn = o.V(wnew, iw);
+      if (iw == o.b0_ + 1 + idir)
+        forR(o, ixO, [&](long c) { wn[c] = wn[c] + qdt * tmp[c]; });
+      else if (iw == o.e_)
+        forR(o, ixO, [&](long c) { wn[c] = wn[c] + qdt * tmp[c] * (b[c] + bg[c]); });
+    }
+  }
+  for (int iw : iws) {  // de/dt += eta*J**2, :205-214
+    if (iw != o.e_) continue;
+    double* wn = o.V(wnew, iw);
+    forR(o, ixO, [&](long c) {
+      double s = 0.0;
+      for (int i = idirmin; i < 3; ++i) s = s + J[i][c] * J[i][c];
+      wn[c] = wn[c] + qdt * eta * s;
+    });
+  }
+}
+
 // addsource2, src/vac.t:552-582: specialsource, then addsource
 // (src/vacphys.mhd0.t:225-258): the resistive term when |eta| > smalldouble
-// (compactres=F, par/DEFAULT:57, selects addsource_res2), then the Powell term
+// (addsource_res2, or addsource_res1 with compactres), then the Powell term
 // when divbfix is set and ndim > 1 ({^NOONED}).
 void addsource2(Oracle& o, double qdt, const std::vector<int>& iws, double qtC, const Arr& wCT,
                 double qt, Arr& w, Work& wk) {
   specialsource(o, qdt, iws, qtC, wCT, qt, w, wk);
-  if (std::fabs(o.par.eta) > smalldouble) addsource_res2(o, qdt, iws, wCT, w, wk);
+  if (std::fabs(o.par.eta) > smalldouble) {
+    if (o.par.compactres)
+      addsource_res1(o, qdt, iws, wCT, w, wk);
+    else
+      addsource_res2(o, qdt, iws, wCT, w, wk);
+  }
   if (o.par.divbfix && o.ndim > 1) addsource_divb(o, qdt, iws, wCT, w, wk);
 }
 

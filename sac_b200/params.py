@@ -49,6 +49,7 @@ class SacParams(ctypes.Structure):
         ("smallp", ctypes.c_double),
         ("smallrho", ctypes.c_double),
         ("vacuumrho", ctypes.c_double),
+        ("compactres", ctypes.c_int),
     ]
 
 
@@ -86,6 +87,7 @@ def default_params() -> SacParams:
     p.device = 0
     p.smallfix = 0  # par/DEFAULT:54
     p.smallp = p.smallrho = p.vacuumrho = -1.0  # src/vacio.t:99-101
+    p.compactres = 0  # par/DEFAULT:57
     return p
 
 

@@ -1,8 +1,8 @@
 """The oracle's optional source terms against direct numpy restatements (CPU).
 
 Powell's div B source (addsource_divb, src/vacphys.mhd0.t:263-297) and the
-resistive source (addsource_res2, src/vacphys.mhdres.t:231-301, constant eta)
-are checked on one 'source' step of typeadvance='onestep' with no user module,
+resistive source (addsource_res2, src/vacphys.mhdres.t:231-301, and its compact
+form addsource_res1, :96-220, both for a constant eta) are checked on one 'source' step of typeadvance='onestep' with no user module,
 where the mesh update is exactly w_new = w + qdt S(w).  The Powell term is also
 checked to be compiled out of 1D runs ({^NOONED}, src/vacphys.mhd0.t:255), and
 the resistive dt limit (getdt_res, src/vacphys.mhdres.t:5-45) by its formula."""
@@ -182,6 +182,65 @@ def test_resistive_source_step_matches_numpy(nx, ndir):
     nadv = 2 * P.ndir + 2
     assert np.abs(got[..., :nadv] - _util.mesh(P, w0)[..., :nadv]).max() > 1e-6  # the source acts
     np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
+
+
+def _resist1_step(P, w, qdt, eta):
+    """addsource_res1 (compactres=T, src/vacphys.mhdres.t:96-220) on the mesh:
+    per idir, eta times the 3-point Laplacian of B_idir into b_idir and, times
+    B_idir, into e; then eta J**2 into e, J from getcurrent on the mesh."""
+    v = problems.var_index(P.ndir)
+    B = [w[..., v["b0"] + 1 + c] + w[..., v["bg0"] + 1 + c] for c in range(P.ndir)]
+    dxg = _util.gridsetup1_dx(P)
+    k0 = 6 - 2 * P.ndir
+    J, idirmin = {}, 3
+    for i in range(max(k0, 0), 3):
+        J[i] = np.zeros(P.nx)
+        for j in range(P.ndim):
+            for k in range(P.ndir):
+                sgn = _lvc(i, j, k)
+                if sgn:
+                    gr = -(_view(P, B[k], j, 1) - _view(P, B[k], j, -1)) / _view(P, dxg[..., j]) / 2.0
+                    J[i] = J[i] + gr if sgn == 1 else J[i] - gr
+                    idirmin = min(idirmin, i)
+    new = _view(P, w).copy()
+    for i in range(P.ndir):
+        tmp = np.zeros(P.nx)
+        for d in range(P.ndim):
+            dx = _view(P, dxg[..., d])
+            tmp = tmp + (_view(P, B[i], d, 1) - 2 * _view(P, B[i]) + _view(P, B[i], d, -1)) / (dx * dx)
+        tmp = tmp * eta
+        new[..., v["b0"] + 1 + i] = new[..., v["b0"] + 1 + i] + qdt * tmp
+        new[..., v["e"]] = new[..., v["e"]] + qdt * tmp * _view(P, B[i])
+    j2 = np.zeros(P.nx)
+    for i in range(idirmin, 3):
+        j2 = j2 + J[i] * J[i]
+    new[..., v["e"]] = new[..., v["e"]] + qdt * eta * j2
+    return new
+
+
+@pytest.mark.parametrize("nx,ndir", [((30,), 1), ((30,), 2), ((30,), 3), ((14, 12), 2), ((14, 12), 3),
+                                     ((10, 9, 8), 3)])
+def test_compact_resistive_source_step_matches_numpy(nx, ndir):
+    types = ["cont", "fixed", "periodic", "periodic", "cont", "symm"][: 2 * len(nx)]
+    P = problems.random_problem(nx, ndir=ndir, seed=37, types=types, user=params.USR_NONE,
+                                typeadvance="onestep")
+    eta = 0.02
+    P.params.eta = eta
+    P.params.compactres = 1
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    qdt = 37.0
+    o.advect(qdt, 0.0, 0, method="source")
+    got = _util.mesh(P, o.download())
+    want = _resist1_step(P, w0, qdt, eta)
+    nadv = 2 * P.ndir + 2
+    assert np.abs(got[..., :nadv] - _util.mesh(P, w0)[..., :nadv]).max() > 1e-6
+    np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
+    # the two forms differ (the compact one is not conservative)
+    P.params.compactres = 0
+    o2 = _util.start(Oracle, P)
+    o2.advect(qdt, 0.0, 0, method="source")
+    assert np.abs(_util.mesh(P, o2.download())[..., :nadv] - got[..., :nadv]).max() > 1e-9
 
 
 def test_resistive_dt_limit():
