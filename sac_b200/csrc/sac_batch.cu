@@ -424,6 +424,7 @@ sac_status sac_batch_create(const sac_params* p, int ndim, int ndir, int ninst, 
   if (p->user == SAC_USR_SLOG || (p->user == SAC_USR_TUBE && ndim < 2)) return SAC_ERR_UNSUPPORTED;
   if (p->eta < 0.0) return SAC_ERR_UNSUPPORTED;  // a user specialeta; eta > 0 is built
   if (p->smallfix) return SAC_ERR_UNSUPPORTED;    // keeppositive runs on single-grid contexts only
+  if (p->compactres) return SAC_ERR_UNSUPPORTED;  // so does the compact resistive form
   sac_batch* b = new sac_batch();
   b->par = *p;
   b->dev = p->device;

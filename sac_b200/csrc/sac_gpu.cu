@@ -268,6 +268,7 @@ sac_status advect1_t(sac_ctx* c, const std::string& method, double qdt, int dmin
     // addsource (src/vacphys.mhd0.t:225-258): resistivity when |eta| > smalldouble,
     // Powell's term when divbfix is set, compiled out of 1D builds ({^NOONED}, :255)
     a.res_on = (c->par.sourceunsplit && std::fabs(c->par.eta) > smalldouble) ? 1 : 0;
+    a.res_compact = c->par.compactres ? 1 : 0;
     a.eta = c->par.eta;
     a.divb_on = (c->par.sourceunsplit && c->par.divbfix && g.ndim > 1) ? 1 : 0;
     a.driver = DRV_NONE;

@@ -197,7 +197,9 @@ __device__ __forceinline__ void nu_cell(const Stage2Args& a, const Geom& g, cons
 // default stage carries none of their registers
 // OPT_PRE: the cross-derivative half-sums come precomputed from k_cross (the
 // single-grid path); without it the update computes them at both neighbours.
-enum StageOpt { OPT_DIVB = 1, OPT_RES = 2, OPT_PRE = 4 };
+// OPT_RES1: the resistive source in the compact form addsource_res1 instead of
+// addsource_res2's (OPT_RES); the two are never combined.
+enum StageOpt { OPT_DIVB = 1, OPT_RES = 2, OPT_PRE = 4, OPT_RES1 = 8 };
 
 // Levi-Civita symbol of 0-based indices (lvc, src/vacdef.t:91)
 __host__ __device__ constexpr int lvc3(int i, int j, int k) {
@@ -468,27 +470,27 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
     // J eta qdt (b) or of B J eta qdt (e) on the mesh.  Walking the neighbour
     // direction d outermost keeps the reference's order of additions: d is jdir of
     // the b loop and idir of the e loop.
+    constexpr int IDM = res_idirmin(NDIM, NDIR);
+    auto curr = [&](int n, T J[3]) {
+#pragma unroll
+      for (int i = IDM; i < 3; ++i) {
+        J[i] = T(0);
+#pragma unroll
+        for (int j = 0; j < NDIM; ++j)
+#pragma unroll
+          for (int k = 0; k < NDIR; ++k) {
+            const int l = lvc3(i, j, k);
+            if (l == 0) continue;
+            const int sj = st[j];
+            const T dxn = (T)__ldg(a.fDX[j] + o.X + n);
+            const T gr = -(Bat(k, n + sj) - Bat(k, n - sj)) / dxn / T(2);
+            J[i] = (l == 1) ? J[i] + gr : J[i] - gr;
+          }
+      }
+    };
     if constexpr ((OPT & OPT_RES) != 0) {
-      constexpr int IDM = res_idirmin(NDIM, NDIR);
       if constexpr (IDM < 3) {
         const T eta = (T)a.eta;
-        auto curr = [&](int n, T J[3]) {
-#pragma unroll
-          for (int i = IDM; i < 3; ++i) {
-            J[i] = T(0);
-#pragma unroll
-            for (int j = 0; j < NDIM; ++j)
-#pragma unroll
-              for (int k = 0; k < NDIR; ++k) {
-                const int l = lvc3(i, j, k);
-                if (l == 0) continue;
-                const int sj = st[j];
-                const T dxn = (T)__ldg(a.fDX[j] + o.X + n);
-                const T gr = -(Bat(k, n + sj) - Bat(k, n - sj)) / dxn / T(2);
-                J[i] = (l == 1) ? J[i] + gr : J[i] - gr;
-              }
-          }
-        };
 #pragma unroll
         for (int d = 0; d < NDIM; ++d) {
           const int s = st[d];
@@ -520,6 +522,38 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
               }
             }
           }
+        }
+      }
+    }
+
+    // --- resistivity, compact form addsource_res1 (src/vacphys.mhdres.t:96-220) --------
+    // per idir in order: eta times the 3-point Laplacian of B_idir = b_idir + bg_idir
+    // (:160-173, the sum starting from zero) into b_idir and, times B_idir, into e
+    // (:191-201); then eta J**2 into e (:205-214), J from getcurrent at this cell
+    if constexpr ((OPT & OPT_RES1) != 0) {
+      const T eta = (T)a.eta;
+#pragma unroll
+      for (int i = 0; i < NDIR; ++i) {
+        const T Bc = Bat(i, c);
+        T lap = T(0);
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+          const int s = st[d];
+          const T dxd = dxv[d];
+          lap = lap + (Bat(i, c + s) - T(2) * Bc + Bat(i, c - s)) / (dxd * dxd);
+        }
+        lap = lap * eta;
+        if ((a.iwmask >> (B0 + 1 + i)) & 1u) acc[B0 + 1 + i] = acc[B0 + 1 + i] + q2 * lap;
+        if ((a.iwmask >> E) & 1u) acc[E] = acc[E] + q2 * lap * Bc;
+      }
+      if constexpr (IDM < 3) {
+        if ((a.iwmask >> E) & 1u) {
+          T J[3];
+          curr(c, J);
+          T j2 = T(0);
+#pragma unroll
+          for (int i = IDM; i < 3; ++i) j2 = j2 + J[i] * J[i];
+          acc[E] = acc[E] + q2 * eta * j2;
         }
       }
     }
@@ -919,7 +953,8 @@ void launch_update(const Stage2Args& a0, cudaStream_t st) {
     constexpr int NDIR = decltype(NR)::value;
     // the optional sources present for this shape: Powell's needs ndim > 1, the
     // resistive one a current component (ndir > 1)
-    const int opt = ((NDIM > 1 && a.divb_on) ? OPT_DIVB : 0) | ((NDIR > 1 && a.res_on) ? OPT_RES : 0);
+    const int ropt = a.res_on ? (a.res_compact ? OPT_RES1 : (NDIR > 1 ? OPT_RES : 0)) : 0;
+    const int opt = ((NDIM > 1 && a.divb_on) ? OPT_DIVB : 0) | ropt;
     // the FP64 single grid takes the precomputed cross terms (k_cross runs
     // whenever hyperdiffusion does; without it the terms are never reached):
     // measured at 128^3 the update fell from 5.53 to 4.41 ms per step for 0.59
@@ -935,12 +970,20 @@ void launch_update(const Stage2Args& a0, cudaStream_t st) {
         k_update<NDIM, NDIR, S, P | OPT_DIVB | OPT_RES><<<grd, blk, 0, st>>>(a);
         return;
       }
+      if (opt == (OPT_DIVB | OPT_RES1)) {
+        k_update<NDIM, NDIR, S, P | OPT_DIVB | OPT_RES1><<<grd, blk, 0, st>>>(a);
+        return;
+      }
     }
     if constexpr (NDIR > 1) {
       if (opt == OPT_RES) {
         k_update<NDIM, NDIR, S, P | OPT_RES><<<grd, blk, 0, st>>>(a);
         return;
       }
+    }
+    if (opt == OPT_RES1) {
+      k_update<NDIM, NDIR, S, P | OPT_RES1><<<grd, blk, 0, st>>>(a);
+      return;
     }
     k_update<NDIM, NDIR, S, P><<<grd, blk, 0, st>>>(a);
   });

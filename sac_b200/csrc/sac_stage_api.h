@@ -62,6 +62,7 @@ struct Stage2Args {
   int grav_on, visc_on, driver, epi;
   int divb_on;            // Powell div B source (divbfix, ndim > 1)
   int res_on;             // resistive source with the constant eta below
+  int res_compact;        // ... in the compact form addsource_res1 (compactres)
   double eta;
   // per-field base pointers (filled by fill_field_ptrs), so that a load is one
   // pointer from parameter space plus the cell offset

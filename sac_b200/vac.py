@@ -178,8 +178,6 @@ class Run:
         sourceunsplit = bool(g("methodlist", "sourceunsplit", True))
         if divbfix and not sourceunsplit:
             raise ValueError("divbfix=T requires unsplitsource=T or splitsource=T !")
-        if bool(g("methodlist", "compactres", False)):
-            raise NotImplementedError("compactres=T (addsource_res1) is outside the implemented path")
         # options that change the run but are not built: say so rather than ignore them
         for grp, key, off, what in (("methodlist", "divbconstrain", False, "divbconstrain=T (the CT module)"),
                                     ("boundlist", "extraB", False, "extraB=T (user boundary regions)")):
@@ -212,7 +210,9 @@ class Run:
             # keeppositive's switch and floors, src/vacio.t:44-45,99-101
             smallfix=int(bool(g("methodlist", "smallfix", False))),
             smallp=float(g("methodlist", "smallp", -1.0)), smallrho=float(g("methodlist", "smallrho", -1.0)),
-            vacuumrho=float(g("methodlist", "vacuumrho", -1.0)))
+            vacuumrho=float(g("methodlist", "vacuumrho", -1.0)),
+            # addsource_res1 instead of addsource_res2 for eta > 0, par/DEFAULT:57
+            compactres=int(bool(g("methodlist", "compactres", False))))
         self.slowsteps = int(g("paramlist", "slowsteps", 0))
         if self.slowsteps == 1 and float(g("paramlist", "dtpar", -1.0)) > 0.0:
             # src/vac.t:76 resets dtpar after the first step; the context's

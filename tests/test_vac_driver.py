@@ -44,14 +44,14 @@ def test_driver_on_the_oracle_writes_the_schedule(tmp_path):
 
 def test_source_switches_follow_the_par(tmp_path):
     # divbfix defaults to T (par/DEFAULT:46) and needs unsplit sources
-    # (src/vacio.t:357-359); compactres=T selects addsource_res1, not built
+    # (src/vacio.t:357-359); compactres=T selects addsource_res1
     assert vac.Run(_par(tmp_path, "a"), context=Oracle).params.divbfix == 1
     assert vac.Run(_par(tmp_path, "b", method="divbfix=F"), context=Oracle).params.divbfix == 0
     with pytest.raises(ValueError):
         vac.Run(_par(tmp_path, "c", method="sourceunsplit=F"), context=Oracle)
     assert vac.Run(_par(tmp_path, "d", method="sourceunsplit=F divbfix=F"), context=Oracle).params.sourceunsplit == 0
-    with pytest.raises(NotImplementedError):
-        vac.Run(_par(tmp_path, "e", method="compactres=T"), context=Oracle)
+    assert vac.Run(_par(tmp_path, "e", method="compactres=T"), context=Oracle).params.compactres == 1
+    assert vac.Run(_par(tmp_path, "e2"), context=Oracle).params.compactres == 0
     with pytest.raises(NotImplementedError):
         vac.Run(_par(tmp_path, "f", method="divbconstrain=T"), context=Oracle)
 
