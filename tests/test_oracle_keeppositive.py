@@ -127,3 +127,33 @@ def test_later_fill_matches_numpy():
     np.testing.assert_array_equal(_util.mesh(P, o.download()), want)
     assert o.diag().nerror_toosmallp == 2
     o.close()
+
+
+def test_first_fill_for_random_shapes_and_floors():
+    """Hypothesis-drawn grids (1D-3D, 5 to 9 mesh cells per dimension), ndir and
+    floors (smallp of either sign, smallrho from none to most cells): the first
+    fill's mesh and error record equal the transcription's."""
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    @settings(max_examples=25, deadline=None, derandomize=True)
+    @given(st.lists(st.integers(5, 9), min_size=1, max_size=3), st.integers(0, 2 ** 16), st.booleans(),
+           st.sampled_from([-1.0, 0.0, 0.003, 0.05]), st.sampled_from([0.0, 0.1, 0.6]))
+    def check(nx, seed, ndir3, smallp, vac_frac):
+        nd = len(nx)
+        P = problems.random_problem(tuple(nx), ndir=3 if (ndir3 or nd == 3) else max(nd, 2), seed=seed,
+                                    types=["periodic"] * (2 * nd), typeadvance="onestep")
+        v = problems.var_index(P.ndir)
+        rt = _util.mesh(P, P.w)[..., v["rho"]] + _util.mesh(P, P.w)[..., v["rhob"]]
+        smallrho = float(np.quantile(rt, vac_frac)) if vac_frac > 0 else -1.0
+        P.params.smallfix, P.params.smallp, P.params.smallrho, P.params.vacuumrho = 1, smallp, smallrho, 0.7
+        want, low, pmin = _keeppositive(P, P.w, smallp, smallrho, 0.7)
+        o = _util.start(Oracle, P)
+        np.testing.assert_array_equal(_util.mesh(P, o.download()), want)
+        d = o.diag()
+        assert d.nerror_toosmallp == int(low)
+        if low:
+            assert d.toosmallp_min == pmin
+        o.close()
+
+    check()
