@@ -10,10 +10,12 @@
  *   sac_upload          host w(ixG^T,nw) -> resident device state      (the COMMON w of program vac, src/vac.t:12)
  *   sac_download        resident device state -> host w                (savefile, src/vacio.t:901)
  *   sac_getboundary     getboundary(t,1,nw,1,ndim,w)                   src/vacgrid.t:195-512
+ *                       (with keeppositive first when smallfix)        src/vacphys.t.mhd:8-49
  *   sac_getdt           vac.t dt block: getdt_courant+getdt+getdt_special src/vac.t:60-70,641-699;
  *                                                                      src/vacphys.mhd0.t:83; src/vacusr.f:1403
  *   sac_advect          advect(method,ixG^L,iws,idim^LIM,w1,w)         src/vac.t:364-487
  *   sac_diag            getdivb + volume means of savefilelog_default  src/vacphys.mhd0.t:106; src/vacio.t:1094
+ *                       + nerror(toosmallp_) of keeppositive           src/vac.t:117-136
  *
  * Conventions
  *   - Arrays crossing the ABI are Fortran order: w(ix1,ix2,ix3,iw), x1 fastest,
