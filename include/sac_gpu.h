@@ -179,8 +179,8 @@ const char* sac_last_error(const sac_ctx* c);
 void sac_destroy(sac_ctx* c);
 
 /* ---- library extensions: no counterpart in the reference ------------------
- * Stream selection lets a host run the path on its own CUDA stream (or capture
- * it); profiling brackets every kernel launch with CUDA events on that stream. */
+ * Stream selection lets a host run the path on its own CUDA stream; profiling
+ * brackets every kernel launch with CUDA events on that stream. */
 #define SAC_K_STAGE 0   /* k_update: the per-cell stage update */
 #define SAC_K_PREP 1    /* k_face: derived fields, fluxes, c_tot */
 #define SAC_K_BOUND 2   /* k_bound: ghost-cell resolve */
@@ -197,10 +197,11 @@ sac_status sac_profile_read(sac_ctx* c, int kernel, double* total_ms, long* laun
 long sac_kernel_launches(const sac_ctx* c);
 
 /* ---- getdt that allocates nothing (library extension; no reference counterpart) ----
- * For callers that cannot allocate device memory where they need dt: a host that
- * gives the whole device to its own pre-sized pool, or code running inside a stream
- * capture or a host callback, where cudaMalloc is not allowed or synchronises the
- * device.  Same result and side effects as sac_getdt.  Its getdt_courant reduction
+ * For callers that cannot allocate device memory where they need dt, such as a
+ * host that gives the whole device to its own pre-sized pool.  Same result and
+ * side effects as sac_getdt; like sac_getdt it launches its reductions on the
+ * context's stream, copies the maximum back and waits for that stream, so it is
+ * an ordinary host call (not for use inside a host callback).  Its getdt_courant reduction
  * runs as a deterministic two-pass block reduction whose scratch (8192 partial
  * maxima and the result, 64 KB) is a file-scope device array of the library, held by
  * every GPU that loads the library until the process exits; the call makes no
@@ -209,8 +210,8 @@ long sac_kernel_launches(const sac_ctx* c);
  *     SAC_ERR_UNSUPPORTED with the sizes in sac_last_error (use sac_getdt there).
  *   - The scratch is one per device, shared by every context on it: calls that
  *     overlap in time (other host threads, other streams) race on it.
- *   - The first call on a device does the set-up (cudaGetSymbolAddress of the
- *     scratch); make it before any stream capture.
+ *   - The first call on a device also looks up the scratch's device address
+ *     (cudaGetSymbolAddress), once per device.
  *   - Nothing in the scratch has to start at zero: each slot that is read was
  *     written earlier in the same call. */
 #define SAC_STATIC_MAX_CELLS 33554432L
