@@ -56,6 +56,14 @@ def test_source_switches_follow_the_par(tmp_path):
         vac.Run(_par(tmp_path, "f", method="divbconstrain=T"), context=Oracle)
 
 
+def test_final_report_warns_of_a_dt_below_dtmin(tmp_path):
+    """The loop stops at the first dt below dtmin and program vac warns of it
+    after the loop (src/vac.t:117)."""
+    par = _par(tmp_path, "m").replace("&stoplist itmax=20 /", "&stoplist itmax=20 dtmin=1.D0 /")
+    r = vac.Run(par, context=Oracle).run(verbose=False)
+    assert r.it == 0 and r.final_report() == [" Warning: dt<dtmin !!!"]
+
+
 def test_smallfix_runs_keeppositive_and_reports(tmp_path):
     """smallfix=T with its floors from &methodlist: with the defaults (-1) the
     fills only count negative perturbed pressures and the snapshots equal those
