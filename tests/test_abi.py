@@ -62,6 +62,14 @@ def test_default_params_match_par_default():
     p = params.SacParams()
     lib.sac_default_params(ctypes.byref(p))
     assert p.courantpar == 0.8 and p.dtpar == -1.0 and p.typeadvance == b"twostep" and p.sourceunsplit == 1
+    # the C defaults and the Python mirror's agree field by field
+    q = params.default_params()
+    for name, ctype in params.SacParams._fields_:
+        a, b = getattr(p, name), getattr(q, name)
+        if isinstance(a, (bytes, int, float)):
+            assert a == b, name
+        else:
+            assert list(a) == list(b), name
 
 
 C_CALLER = r"""
