@@ -243,6 +243,35 @@ def test_compact_resistive_source_step_matches_numpy(nx, ndir):
     assert np.abs(_util.mesh(P, o2.download())[..., :nadv] - got[..., :nadv]).max() > 1e-9
 
 
+def test_resistive_sources_for_random_shapes():
+    """Hypothesis-drawn grids (1D-3D, 5 to 9 mesh cells per dimension), ndir, eta
+    and the form (compactres or not): one 'source' step, bit for bit."""
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    @settings(max_examples=20, deadline=None, derandomize=True)
+    @given(st.lists(st.integers(5, 9), min_size=1, max_size=3), st.integers(0, 2 ** 16), st.integers(1, 3),
+           st.sampled_from([0.003, 0.02, 0.4]), st.booleans())
+    def check(nx, seed, ndir, eta, compact):
+        nd = len(nx)
+        ndir = max(ndir, nd)
+        types = [t for d in range(nd) for t in (("periodic", "periodic") if d == 0 else ("cont", "fixed"))]
+        P = problems.random_problem(tuple(nx), ndir=ndir, seed=seed, types=types, user=params.USR_NONE,
+                                    typeadvance="onestep")
+        P.params.eta = eta
+        P.params.compactres = int(compact)
+        o = _util.start(Oracle, P)
+        w0 = o.download()
+        o.advect(37.0, 0.0, 0, method="source")
+        got = _util.mesh(P, o.download())
+        o.close()
+        want = (_resist1_step if compact else _resist_step)(P, w0, 37.0, eta)
+        nadv = 2 * P.ndir + 2
+        np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
+
+    check()
+
+
 def test_resistive_dt_limit():
     P = problems.random_problem((14, 12), seed=35, types=["cont", "cont", "periodic", "periodic"],
                                 user=params.USR_NONE)
