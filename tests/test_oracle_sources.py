@@ -76,6 +76,32 @@ def test_powell_source_step_matches_numpy(nx, ndir):
     np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
 
 
+def test_powell_source_for_random_shapes():
+    """Hypothesis-drawn 2D/3D grids (5 to 9 mesh cells per dimension), ndir and
+    boundary types: one 'source' step with divbfix, bit for bit."""
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    @settings(max_examples=15, deadline=None, derandomize=True)
+    @given(st.lists(st.integers(5, 9), min_size=2, max_size=3), st.integers(0, 2 ** 16), st.booleans(),
+           st.sampled_from(["cont", "fixed", "symm", "cont1"]))
+    def check(nx, seed, ndir3, edge):
+        nd = len(nx)
+        types = [t for d in range(nd) for t in (("periodic", "periodic") if d == 1 else ("cont", edge))]
+        P = problems.random_problem(tuple(nx), ndir=3 if (ndir3 or nd == 3) else 2, seed=seed, types=types,
+                                    user=params.USR_NONE, typeadvance="onestep")
+        P.params.divbfix = 1
+        o = _util.start(Oracle, P)
+        w0 = o.download()
+        o.advect(37.0, 0.0, 0, method="source")
+        got = _util.mesh(P, o.download())
+        o.close()
+        nadv = 2 * P.ndir + 2
+        np.testing.assert_array_equal(got[..., :nadv], _powell_step(P, w0, 37.0)[..., :nadv])
+
+    check()
+
+
 def test_powell_source_is_off_in_1d():
     P = problems.random_problem((40,), ndir=3, seed=32)
     a = _util.start(Oracle, P)
