@@ -16,13 +16,16 @@ from sac_b200 import params, problems
 import _util
 from test_oracle_boundaries import _fill
 from test_oracle_centdiff import _getflux, _getptotal_bg, _gradient4, _mesh
+from test_oracle_keeppositive import _keeppositive
 from test_oracle_visc import Visc
 
 
 _MAXNU = [0.0]  # maxviscoef over the setnu calls since the last getdt
 
 
-def _advect1(P, qdt, wct, base):
+def _advect1(P, qdt, wct, base, floors=None):
+    """floors: (smallp, smallrho, vacuumrho) when smallfix is set, so that the fill
+    starts with keeppositive on the mesh (src/vacgrid.t:220)."""
     v = problems.var_index(P.ndir)
     gamma = P.params.gamma
     dims = list(range(P.ndim))
@@ -59,15 +62,17 @@ def _advect1(P, qdt, wct, base):
     _MAXNU[0] = max(_MAXNU[0], V.maxviscoef)
     out = base.copy()
     out[tuple(slice(2, 2 + n) for n in P.nx)] = new
+    if floors is not None:
+        out[tuple(slice(2, 2 + n) for n in P.nx)] = _keeppositive(P, out, *floors)[0]
     return _fill(P, out)
 
 
-def _fourstep(P, w, dt):
-    w1 = _advect1(P, dt / 2, w, w)
-    w2 = _advect1(P, dt / 2, w1, w)
-    w3 = _advect1(P, dt, w2, w)
+def _fourstep(P, w, dt, floors=None):
+    w1 = _advect1(P, dt / 2, w, w, floors)
+    w2 = _advect1(P, dt / 2, w1, w, floors)
+    w3 = _advect1(P, dt, w2, w, floors)
     w1 = (w1 + 2.0 * w2 + w3 - 4.0 * w) / 3.0
-    w = _advect1(P, dt / 6, w3, w)
+    w = _advect1(P, dt / 6, w3, w, floors)
     return w + w1
 
 
@@ -85,6 +90,29 @@ def test_rk4_step_matches_the_composed_transcriptions(nx, ndir, types):
     got = o.download()
     want = _fourstep(P, w0, dt)
     assert np.abs(got - w0).max() > 1e-6
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("nx,smallp,vac_frac", [((24,), 0.001, 0.1), ((12, 10), 0.001, 0.15),
+                                                ((9, 8, 7), -1.0, 0.1)])
+def test_rk4_step_with_keeppositive_matches_the_composed_transcriptions(nx, smallp, vac_frac):
+    """smallfix: each of the four fills starts with keeppositive on the mesh of the
+    array it fills, before the ghost layers and before the combinations read it."""
+    ndir = 3 if len(nx) > 1 else 2
+    types = ["cont", "symm", "periodic", "periodic", "cont", "cont"][: 2 * len(nx)]
+    P = problems.random_problem(nx, ndir=ndir, seed=43, types=types, typeadvance="fourstep")
+    v = problems.var_index(ndir)
+    m = _util.mesh(P, P.w)
+    floors = (smallp, float(np.quantile(m[..., v["rho"]] + m[..., v["rhob"]], vac_frac)), 0.9)
+    P.params.smallfix = 1
+    P.params.smallp, P.params.smallrho, P.params.vacuumrho = floors
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    dt = 0.2 * o.getdt(0)
+    o.advect(dt, 0.0, 0)
+    got = o.download()
+    want = _fourstep(P, w0, dt, floors)
+    assert o.diag().nerror_toosmallp == 5
     np.testing.assert_array_equal(got, want)
 
 
