@@ -17,6 +17,7 @@ import _util
 from test_oracle_boundaries import _fill
 from test_oracle_centdiff import _getflux, _getptotal_bg, _gradient4, _mesh
 from test_oracle_keeppositive import _keeppositive
+from test_oracle_sources import _powell_step, _resist1_step, _resist_step
 from test_oracle_visc import Visc
 
 
@@ -60,6 +61,11 @@ def _advect1(P, qdt, wct, base, floors=None):
     V = Visc(P, wct, qdt)
     new = V.step(new)
     _MAXNU[0] = max(_MAXNU[0], V.maxviscoef)
+    # addsource (src/vacphys.mhd0.t:225-258): resistivity, then Powell's term
+    if abs(P.params.eta) > 1e-99:
+        new = (_resist1_step if P.params.compactres else _resist_step)(P, wct, qdt, P.params.eta, new)
+    if P.params.divbfix and P.ndim > 1:
+        new = _powell_step(P, wct, qdt, new)
     out = base.copy()
     out[tuple(slice(2, 2 + n) for n in P.nx)] = new
     if floors is not None:
@@ -114,6 +120,22 @@ def test_rk4_step_with_keeppositive_matches_the_composed_transcriptions(nx, smal
     want = _fourstep(P, w0, dt, floors)
     assert o.diag().nerror_toosmallp == 5
     np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("nx,compact", [((24,), 0), ((24,), 1), ((12, 10), 0), ((12, 10), 1), ((9, 8, 7), 1)])
+def test_rk4_step_with_resistivity_and_powell_matches_the_composed_transcriptions(nx, compact):
+    """Gravity, hyperdiffusion, then addsource's resistive term (either form) and
+    Powell's, in every stage of a fourstep step."""
+    ndir = 3 if len(nx) > 1 else 2
+    types = ["cont", "symm", "periodic", "periodic", "cont1", "cont"][: 2 * len(nx)]
+    P = problems.random_problem(nx, ndir=ndir, seed=44, types=types, typeadvance="fourstep")
+    P.params.eta, P.params.compactres, P.params.divbfix = 0.02, compact, 1
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    dt = 0.2 * o.getdt(0)
+    o.advect(dt, 0.0, 0)
+    got = o.download()
+    np.testing.assert_array_equal(got, _fourstep(P, w0, dt))
 
 
 def _integrate(P, w, dt, method, pred):

@@ -39,7 +39,8 @@ def _gradient4(P, q, d):
     return g
 
 
-def _powell_step(P, w, qdt):
+def _powell_step(P, w, qdt, new=None):
+    """The mesh after Powell's source from w added to new (default: w's mesh)."""
     v = problems.var_index(P.ndir)
     B = [w[..., v["b0"] + 1 + c] + w[..., v["bg0"] + 1 + c] for c in range(P.ndir)]
     divb = np.zeros(P.nx)
@@ -47,7 +48,7 @@ def _powell_step(P, w, qdt):
         divb = divb + _gradient4(P, B[d], d)
     divb = qdt * divb
     rt = _view(P, w[..., v["rho"]] + w[..., v["rhob"]])
-    new = _view(P, w).copy()
+    new = _view(P, w).copy() if new is None else new.copy()
     s = 0.0
     for c in range(P.ndir):
         Bc = _view(P, B[c])
@@ -149,7 +150,8 @@ def _inner(P, T, d=None, k=0):
     return T[tuple(sl)]
 
 
-def _resist_step(P, w, qdt, eta):
+def _resist_step(P, w, qdt, eta, new=None):
+    """The mesh after addsource_res2 from w added to new (default: w's mesh)."""
     v = problems.var_index(P.ndir)
     B = [w[..., v["b0"] + 1 + c] + w[..., v["bg0"] + 1 + c] for c in range(P.ndir)]
     dxg = _util.gridsetup1_dx(P)
@@ -169,7 +171,7 @@ def _resist_step(P, w, qdt, eta):
                     gr = -(_region(P, B[k], 1, j, 1) - _region(P, B[k], 1, j, -1)) / dx(j, 1) / 2.0
                     J[i] = J[i] + gr if sgn == 1 else J[i] - gr
                     idirmin = min(idirmin, i)
-    new = _view(P, w).copy()
+    new = _view(P, w).copy() if new is None else new.copy()
 
     def grad_mesh(T, d):
         return -(_inner(P, T, d, 1) - _inner(P, T, d, -1)) / dx(d, 0) / 2.0
@@ -210,7 +212,7 @@ def test_resistive_source_step_matches_numpy(nx, ndir):
     np.testing.assert_array_equal(got[..., :nadv], want[..., :nadv])
 
 
-def _resist1_step(P, w, qdt, eta):
+def _resist1_step(P, w, qdt, eta, new=None):
     """addsource_res1 (compactres=T, src/vacphys.mhdres.t:96-220) on the mesh:
     per idir, eta times the 3-point Laplacian of B_idir into b_idir and, times
     B_idir, into e; then eta J**2 into e, J from getcurrent on the mesh."""
@@ -228,7 +230,7 @@ def _resist1_step(P, w, qdt, eta):
                     gr = -(_view(P, B[k], j, 1) - _view(P, B[k], j, -1)) / _view(P, dxg[..., j]) / 2.0
                     J[i] = J[i] + gr if sgn == 1 else J[i] - gr
                     idirmin = min(idirmin, i)
-    new = _view(P, w).copy()
+    new = _view(P, w).copy() if new is None else new.copy()
     for i in range(P.ndir):
         tmp = np.zeros(P.nx)
         for d in range(P.ndim):
