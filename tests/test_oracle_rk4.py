@@ -14,7 +14,7 @@ from oracle.oracle import Oracle
 from sac_b200 import params, problems
 
 import _util
-from test_oracle_boundaries import _fill
+from test_oracle_boundaries import _capture, _fill
 from test_oracle_centdiff import _getflux, _getptotal_bg, _gradient4, _mesh
 from test_oracle_keeppositive import _keeppositive
 from test_oracle_sources import _powell_step, _resist1_step, _resist_step
@@ -22,6 +22,7 @@ from test_oracle_visc import Visc
 
 
 _MAXNU = [0.0]  # maxviscoef over the setnu calls since the last getdt
+_FIX = [None]  # the fixB values captured after the first fill, when a test sets them
 
 
 def _advect1(P, qdt, wct, base, floors=None):
@@ -70,7 +71,7 @@ def _advect1(P, qdt, wct, base, floors=None):
     out[tuple(slice(2, 2 + n) for n in P.nx)] = new
     if floors is not None:
         out[tuple(slice(2, 2 + n) for n in P.nx)] = _keeppositive(P, out, *floors)[0]
-    return _fill(P, out)
+    return _fill(P, out, _FIX[0])
 
 
 def _fourstep(P, w, dt, floors=None):
@@ -136,6 +137,25 @@ def test_rk4_step_with_resistivity_and_powell_matches_the_composed_transcription
     o.advect(dt, 0.0, 0)
     got = o.download()
     np.testing.assert_array_equal(got, _fourstep(P, w0, dt))
+
+
+@pytest.mark.parametrize("nx,types", [((24,), ["fixed", "grad1"]), ((12, 10), ["fixed1", "cont", "periodic", "periodic"]),
+                                      ((9, 8, 7), ["periodic", "periodic", "grad1", "fixed", "fixed1", "symm"])])
+def test_rk4_step_with_stored_boundaries_matches_the_composed_transcriptions(nx, types):
+    """'fixed', 'fixed1' and 'grad1' regions: every fill of the step restores the
+    values captured after the first fill (src/vacgrid.t:476-507)."""
+    ndir = 3 if len(nx) > 1 else 2
+    P = problems.random_problem(nx, ndir=ndir, seed=45, types=types, typeadvance="fourstep")
+    o = _util.start(Oracle, P)
+    w0 = o.download()
+    dt = 0.2 * o.getdt(0)
+    o.advect(dt, 0.0, 0)
+    _FIX[0] = _capture(P, w0)
+    try:
+        want = _fourstep(P, w0, dt)
+    finally:
+        _FIX[0] = None
+    np.testing.assert_array_equal(o.download(), want)
 
 
 def _integrate(P, w, dt, method, pred):
