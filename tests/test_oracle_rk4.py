@@ -25,12 +25,13 @@ _MAXNU = [0.0]  # maxviscoef over the setnu calls since the last getdt
 _FIX = [None]  # the fixB values captured after the first fill, when a test sets them
 
 
-def _advect1(P, qdt, wct, base, floors=None):
+def _advect1(P, qdt, wct, base, floors=None, dims=None):
     """floors: (smallp, smallrho, vacuumrho) when smallfix is set, so that the fill
-    starts with keeppositive on the mesh (src/vacgrid.t:220)."""
+    starts with keeppositive on the mesh (src/vacgrid.t:220).  dims: the 0-based
+    idimmin..idimmax of a dimensionally split sweep (default: all)."""
     v = problems.var_index(P.ndir)
     gamma = P.params.gamma
-    dims = list(range(P.ndim))
+    dims = list(range(P.ndim)) if dims is None else dims
     new = _mesh(P, base).copy()
     # centdiff4 (src/vaccd.t:35-70): fluxes from wCT, background work from the output array
     for d in dims:
@@ -53,10 +54,11 @@ def _advect1(P, qdt, wct, base, floors=None):
     g = list(P.params.grav)
     rho = _mesh(P, wct[..., v["rho"]])
     rt = _mesh(P, wct[..., v["rho"]] + wct[..., v["rhob"]])
-    for d in dims:
+    # gravity acts along every dimension, whatever the sweep
+    for d in range(P.ndim):
         if abs(g[d]) > 1e-99:
             new[..., v["m0"] + 1 + d] = new[..., v["m0"] + 1 + d] + qdt * g[d] * rho
-    for d in dims:
+    for d in range(P.ndim):
         if abs(g[d]) > 1e-99:
             new[..., v["e"]] = new[..., v["e"]] + qdt * g[d] * rho * _mesh(P, wct[..., v["m0"] + 1 + d]) / rt
     V = Visc(P, wct, qdt)
@@ -74,12 +76,12 @@ def _advect1(P, qdt, wct, base, floors=None):
     return _fill(P, out, _FIX[0])
 
 
-def _fourstep(P, w, dt, floors=None):
-    w1 = _advect1(P, dt / 2, w, w, floors)
-    w2 = _advect1(P, dt / 2, w1, w, floors)
-    w3 = _advect1(P, dt, w2, w, floors)
+def _fourstep(P, w, dt, floors=None, dims=None):
+    w1 = _advect1(P, dt / 2, w, w, floors, dims)
+    w2 = _advect1(P, dt / 2, w1, w, floors, dims)
+    w3 = _advect1(P, dt, w2, w, floors, dims)
     w1 = (w1 + 2.0 * w2 + w3 - 4.0 * w) / 3.0
-    w = _advect1(P, dt / 6, w3, w, floors)
+    w = _advect1(P, dt / 6, w3, w, floors, dims)
     return w + w1
 
 
@@ -156,6 +158,24 @@ def test_rk4_step_with_stored_boundaries_matches_the_composed_transcriptions(nx,
     finally:
         _FIX[0] = None
     np.testing.assert_array_equal(o.download(), want)
+
+
+@pytest.mark.parametrize("nx,sweeps", [((12, 10), [[0], [1]]), ((12, 10), [[1], [0]]), ((9, 8, 7), [[0], [1], [2]]),
+                                       ((9, 8, 7), [[2], [1], [0]])])
+def test_split_sweeps_match_the_composed_transcriptions(nx, sweeps):
+    """Dimensionally split sweeps (advance_expl, src/vac.t:310-325): one advect per
+    dimension, its fluxes and background work along that dimension only and its
+    sources scaled by 1/ndim, then the next sweep from the result."""
+    P = problems.random_problem(nx, ndir=3, seed=46, types=["cont", "symm", "periodic", "periodic", "cont1",
+                                                            "cont"][: 2 * len(nx)], typeadvance="fourstep")
+    P.params.eta, P.params.divbfix = 0.02, 1
+    o = _util.start(Oracle, P)
+    w = o.download()
+    dt = 0.2 * o.getdt(0)
+    for dims in sweeps:
+        o.advect(dt, 0.0, 0, idimmin=dims[0] + 1, idimmax=dims[0] + 1)
+        w = _fourstep(P, w, dt, dims=dims)
+    np.testing.assert_array_equal(o.download(), w)
 
 
 def _integrate(P, w, dt, method, pred):
