@@ -30,6 +30,17 @@ def cases():
             "oracle_stratified12_020": (st, 20)}
 
 
+def option_cases():
+    """name -> (Problem, steps) for the options off by default: the Orszag-Tang
+    vortex with keeppositive's floors (smallfix) and the compact resistive source
+    (compactres)."""
+    ot = problems.orszag_tang((32, 32))
+    ot.params.smallfix = 1
+    ot.params.smallp, ot.params.smallrho, ot.params.vacuumrho = 0.5, 2.75, 2.75
+    ot.params.eta, ot.params.compactres = 0.01, 1
+    return {"oracle_ot32_smallfix_compactres_020": (ot, 20)}
+
+
 def run(P, steps, ctx_cls=None):
     """The case through program vac's loop on ctx_cls (default: the oracle);
     returns the full grid and the final time."""
@@ -55,7 +66,7 @@ def snapshot(P, w, t, steps):
 
 
 def main():
-    for name, (P, steps) in cases().items():
+    for name, (P, steps) in {**cases(), **option_cases()}.items():
         w, t = run(P, steps)
         fileio.write_binary(os.path.join(HERE, name + ".out"), [snapshot(P, w, t, steps)])
         print("wrote", name + ".out")

@@ -108,3 +108,26 @@ def test_batch_rejects_smallfix():
     prm.smallfix = 1
     with pytest.raises(abi.SacError):
         batch.Batch(prm, 2, 2, [(16, 16)])
+
+
+def test_device_reproduces_the_option_golden_output():
+    """The committed oracle output of the Orszag-Tang vortex with the floors and
+    the compact resistive source (tests/golden/make_oracle_golden.py), 20 steps
+    through program vac's loop: the advanced variables on the mesh within 1e-12."""
+    import os
+    import sys
+
+    from sac_b200 import fileio
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_oracle_golden as G
+
+    for name, (P, steps) in G.option_cases().items():
+        w, t = G.run(P, steps, abi.Context)
+        ref = fileio.read_binary(os.path.join(here, "golden", name + ".out"))[-1]
+        assert ref.it == steps
+        np.testing.assert_allclose(t, ref.t, rtol=1e-12, atol=0)
+        nadv = 2 * P.ndir + 2
+        err = _util.rel_l2(_util.mesh(P, w)[..., :nadv], _util.mesh(P, ref.w)[..., :nadv])
+        assert np.isfinite(w).all() and err.max() <= RTOL, f"{name}: rel L2 per variable {err}"
