@@ -178,6 +178,42 @@ def test_split_sweeps_match_the_composed_transcriptions(nx, sweeps):
     np.testing.assert_array_equal(o.download(), w)
 
 
+def test_rk4_steps_for_random_shapes_and_options():
+    """Hypothesis-drawn grids (1D-3D, 6 to 9 mesh cells per dimension), boundary
+    types (the stored ones included), ndir, resistivity in either form and
+    Powell's term: one fourstep step of the oracle, bit for bit."""
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    kinds = ["cont", "cont1", "symm", "asymm", "contCD4", "fixed", "fixed1", "grad1"]
+
+    @settings(max_examples=12, deadline=None, derandomize=True)
+    @given(st.lists(st.integers(6, 9), min_size=1, max_size=3), st.integers(0, 2 ** 16), st.booleans(),
+           st.lists(st.sampled_from(kinds + ["periodic"]), min_size=3, max_size=3),
+           st.sampled_from([0.0, 0.01]), st.booleans(), st.booleans())
+    def check(nx, seed, ndir3, kind, eta, compact, divb):
+        nd = len(nx)
+        types = []
+        for d in range(nd):
+            types += ["periodic", "periodic"] if kind[d] == "periodic" else [kind[d], kinds[(seed + d) % len(kinds)]]
+        P = problems.random_problem(tuple(nx), ndir=3 if (ndir3 or nd == 3) else max(nd, 2), seed=seed,
+                                    types=types, typeadvance="fourstep")
+        P.params.eta, P.params.compactres, P.params.divbfix = eta, int(compact), int(divb)
+        o = _util.start(Oracle, P)
+        w0 = o.download()
+        dt = 0.2 * o.getdt(0)
+        o.advect(dt, 0.0, 0)
+        _FIX[0] = _capture(P, w0)
+        try:
+            want = _fourstep(P, w0, dt)
+        finally:
+            _FIX[0] = None
+        np.testing.assert_array_equal(o.download(), want)
+        o.close()
+
+    check()
+
+
 def _integrate(P, w, dt, method, pred):
     """advect's other time integrators (src/vac.t:402-476); w1 starts as a copy of w."""
     nul = lambda wct, base: _fill(P, base.copy())  # noqa: E731  advect1 with method 'nul'
