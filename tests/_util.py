@@ -7,7 +7,7 @@ from sac_b200 import abi
 def start(ctx_cls, P, **kw):
     c = ctx_cls(P.params, **kw) if kw else ctx_cls(P.params)
     c.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
-    c.set_boundaries(P.typeB_packed, P.nB)
+    c.set_boundaries(P.typeB_packed, P.nB, regions=getattr(P, "regions", None))
     c.upload(P.w)
     c.getboundary(0.0)
     return c
@@ -74,3 +74,46 @@ def gridsetup1_dx(P):
                              for e in range(nd))
         dx[..., d] = 0.5 * (qx[sl(1) + (d,)] - qx[sl(-1) + (d,)])
     return dx
+
+
+def fp32_rounded(P):
+    """A copy of P whose advanced (perturbed) variables are rounded to FP32, as
+    the FP32 path stores them; the background stays FP64."""
+    import copy
+
+    Q = copy.deepcopy(P)
+    npv = 2 * P.ndir + 2
+    Q.w[..., :npv] = Q.w[..., :npv].astype(np.float32).astype(np.float64)
+    return Q
+
+
+def fp32_twin(P, nsteps, gpu_cls=None):
+    """The FP32 path against the scheme's own sensitivity to FP32 rounding.
+
+    Runs the oracle (FP64) from P's initial state for nsteps with its own getdt,
+    then the oracle from the FP32-rounded initial state (the twin) and the FP32
+    device path from P's state, both on that dt sequence.  Returns the
+    per-variable relative L2 errors over the mesh of the advanced variables:
+    (FP32 path vs oracle, twin vs oracle)."""
+    import copy
+
+    from oracle.oracle import Oracle
+    from sac_b200 import params
+
+    npv = 2 * P.ndir + 2
+    o = start(Oracle, P)
+    dts = run(o, nsteps)
+    wo = mesh(P, o.download())[..., :npv]
+    o.close()
+    ot = start(Oracle, fp32_rounded(P))
+    run(ot, nsteps, dts=dts)
+    etw = rel_l2(mesh(P, ot.download())[..., :npv], wo)
+    ot.close()
+    P32 = copy.deepcopy(P)
+    P32.params.precision = params.PREC_FP32
+    g = start(gpu_cls or abi.Context, P32)
+    run(g, nsteps, dts=dts)
+    w32 = mesh(P, g.download())[..., :npv]
+    g.close()
+    assert np.isfinite(w32).all()
+    return rel_l2(w32, wo), etw

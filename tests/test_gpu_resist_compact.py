@@ -14,7 +14,12 @@ import _util
 pytestmark = pytest.mark.gpu
 
 RTOL = 1e-12
-FP32_RTOL = 1e-5
+# (FP32 error) / (divergence of the FP64 twin from the FP32-rounded initial state),
+# measured on B200: 47-75 on smooth 3D states after 20-100 steps (stratified
+# 16x12x12, compact resistive 12x10x8), 3.4-6.4 on the Orszag-Tang vortex with
+# floors, 1.7-3.4 on the free vortex; the FP32 path rounds at every stage, the twin
+# once, so the ratio grows with the steps over which the rounding accumulates
+FP32_TWIN_FACTOR = 150.0
 
 
 def _pair(P):
@@ -75,14 +80,13 @@ def test_compact_resistive_source_method():
 
 
 def test_fp32_compact_resistive_3d():
+    """FP32 perturbations over 100 steps, held to the scheme's own sensitivity:
+    within FP32_TWIN_FACTOR of the divergence of the FP64 oracle started from the
+    FP32-rounded initial state (the hyperdiffusion switch amplifies rounding)."""
     P = _compact(problems.random_problem((12, 10, 8), seed=45,
                                          types=["cont", "cont", "periodic", "periodic", "fixed", "cont"]), 0.01)
-    o = _util.start(Oracle, P)
-    P.params.precision = params.PREC_FP32
-    g = _util.start(abi.Context, P)
-    dts = _util.run(o, 50)
-    _util.run(g, 50, dts=dts)
-    _compare(P, o, g, FP32_RTOL)
+    e32, etw = _util.fp32_twin(P, 100)
+    assert e32.max() <= FP32_TWIN_FACTOR * etw.max(), (e32, etw)
 
 
 def test_batch_rejects_compactres():

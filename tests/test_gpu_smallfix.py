@@ -18,7 +18,12 @@ import _util
 pytestmark = pytest.mark.gpu
 
 RTOL = 1e-12
-FP32_RTOL = 1e-5
+# (FP32 error) / (divergence of the FP64 twin from the FP32-rounded initial state),
+# measured on B200: 47-75 on smooth 3D states after 20-100 steps (stratified
+# 16x12x12, compact resistive 12x10x8), 3.4-6.4 on the Orszag-Tang vortex with
+# floors, 1.7-3.4 on the free vortex; the FP32 path rounds at every stage, the twin
+# once, so the ratio grows with the steps over which the rounding accumulates
+FP32_TWIN_FACTOR = 150.0
 
 
 def _ot(typeadvance="fourstep", smallrho=2.75):
@@ -89,17 +94,20 @@ def test_counting_only_leaves_the_state_to_the_oracle():
 
 
 def test_fp32_orszag_tang_floors():
-    """The pressure floor in FP32, 5 steps: the floor flattens the pressure into
-    plateaus, where the hyperdiffusion's difference ratios are rounding noise, so
-    FP32 and FP64 runs part at the 1e-5 level after about 20 steps (measured with
-    the oracle from FP32-rounded initial states); after 5 they agree to ~1e-6."""
+    """The pressure floor in FP32 over 20 steps.  The floor flattens the pressure
+    into plateaus, where the hyperdiffusion's difference ratios are rounding
+    noise, so the FP32 run is held to the scheme's own sensitivity: within
+    FP32_TWIN_FACTOR of the divergence of the FP64 oracle started from the
+    FP32-rounded initial state."""
     P = _ot(smallrho=-1.0)
+    e32, etw = _util.fp32_twin(P, 20)
+    assert e32.max() <= FP32_TWIN_FACTOR * etw.max(), (e32, etw)
     o = _util.start(Oracle, P)
-    P.params.precision = params.PREC_FP32
-    g = _util.start(abi.Context, P)
-    dts = _util.run(o, 5)
-    _util.run(g, 5, dts=dts)
-    _compare(P, o, g, FP32_RTOL)
+    _util.run(o, 20)
+    P32 = _ot(smallrho=-1.0)
+    P32.params.precision = params.PREC_FP32
+    g = _util.start(abi.Context, P32)
+    _util.run(g, 20)
     assert g.diag().nerror_toosmallp == o.diag().nerror_toosmallp
 
 
