@@ -6,7 +6,7 @@
  *
  *   sac_create          physini + the method part of readparameters   src/vacphys.mhd0.t:9, src/vacio.t:246-527
  *   sac_set_grid        setixGixMix + gridsetup1 (dx, dvolume)         src/vacio.t:786-841, src/vacgrid.t:556-661
- *   sac_set_boundaries  boundsetup (default regions, periodic pairing)  src/vacgrid.t:9-160
+ *   sac_set_boundaries  boundsetup (default or user regions, pairing)   src/vacgrid.t:9-160
  *   sac_upload          host w(ixG^T,nw) -> resident device state      (the COMMON w of program vac, src/vac.t:12)
  *   sac_download        resident device state -> host w                (savefile, src/vacio.t:901)
  *   sac_getboundary     getboundary(t,1,nw,1,ndim,w)                   src/vacgrid.t:195-512
@@ -153,9 +153,23 @@ sac_status sac_create(const sac_params* p, sac_ctx** out);
 sac_status sac_set_grid(sac_ctx* c, int ndim, int ndir, const int ixGhi[3], const int ixM[6],
                         const double* x, int fullgridini);
 
-/* typeB: CHARACTER*10 typeB(nw,nB) (f10, blank padded), default regions
- * iB=2*idim-1 (lower) / 2*idim (upper).  ipairB may be NULL (auto pairing). */
-sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* ipairB);
+/* boundsetup (src/vacgrid.t:9-160) with &boundlist's nB, typeB, ixB^LIM, idimB,
+ * upperB and ipairB (src/vacio.t:46, src/vacdef.t:107-111).
+ *   typeB  CHARACTER*10 typeB(nw,nB) (f10, blank padded).
+ *   ixB    NULL: the default regions, nB = 2*ndim, iB=2*idim-1 (lower) / 2*idim
+ *          (upper), each a full dixB-deep ghost slab.  Otherwise the user's
+ *          regions: ixBmin(1:ndim,1:nB) followed by ixBmax(1:ndim,1:nB) (1-based,
+ *          Fortran order), with idimB(1:nB) in 1..ndim and upperB(1:nB) 0/1 (both
+ *          required then).  Each region must lie inside the grid (SAC_ERR_ARG, as
+ *          boundsetup's die) and in the ghost layers along its idimB; regions
+ *          2*idim-1 and 2*idim must be the lower and upper boundaries of dimension
+ *          idim, which gradient4, gradient1 and setnu read; regions beyond 2*ndim
+ *          are free (up to nhiB = 10).  getboundary fills the regions in order,
+ *          later ones overwriting earlier ones where they overlap.
+ *   ipairB NULL or ipairB(1:nB), 0 = pair automatically: the periodic regions of the
+ *          same idimB, opposite upperB and equal extent. */
+sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* ixB, const int* idimB,
+                              const int* upperB, const int* ipairB);
 
 sac_status sac_upload(sac_ctx* c, const double* w);
 sac_status sac_download(sac_ctx* c, double* w);
@@ -211,7 +225,12 @@ long sac_kernel_launches(const sac_ctx* c);
  *   - The scratch is one per device, shared by every context on it: calls that
  *     overlap in time (other host threads, other streams) race on it.
  *   - The first call on a device also looks up the scratch's device address
- *     (cudaGetSymbolAddress), once per device.
+ *     (cudaGetSymbolAddress), once per device, and keeps it for the life of the
+ *     process: the device's primary context (the runtime's, which every context
+ *     of this library uses) must not be reset (cudaDeviceReset) while the library
+ *     is loaded, or the kept address no longer names the scratch.
+ *   - With profiling on, its two launches count under SAC_K_COURANT, as the
+ *     reduction of sac_getdt does.
  *   - Nothing in the scratch has to start at zero: each slot that is read was
  *     written earlier in the same call. */
 #define SAC_STATIC_MAX_CELLS 33554432L

@@ -1009,9 +1009,15 @@ void getboundary(Oracle& o, Arr& w) {
           }
         }
       } else if (t == "periodic") {
+        // w(ix^S) = w(ixpair^S): the pair's region moved by dixB along idim (:236-246)
         const Rg pr = o.ixB[o.ipairB[iB]];
-        int shift = up ? (pr.lo[d] + o.dixB) - r.lo[d] : (pr.lo[d] - o.dixB) - r.lo[d];
-        forR(o, r, [&](long c) { a[c] = a[c + (long)shift * s]; });
+        long shift = 0;
+        for (int e = 0; e < o.ndim; ++e) {
+          int se = pr.lo[e] - r.lo[e];
+          if (e == d) se += up ? o.dixB : -o.dixB;
+          shift += (long)se * o.st[e];
+        }
+        forR(o, r, [&](long c) { a[c] = a[c + shift]; });
       } else if (t == "symm" || t == "symm0" || t == "asymm") {
         int ixe = up ? 2 * r.lo[d] - 1 : 2 * r.hi[d] + 1;
         double sg = (t == "asymm") ? -1.0 : 1.0;
@@ -1342,11 +1348,19 @@ int oracle_set_grid(oracle_ctx* cx, int ndim, int ndir, const int ixGhi[3], cons
   return SAC_OK;
 }
 
-// boundsetup with default regions, src/vacgrid.t:53-120
-int oracle_set_boundaries(oracle_ctx* cx, int nB, const char* typeB, const int* ipairB) {
+// boundsetup, src/vacgrid.t:9-160: the default regions (ixB == NULL,
+// :53-70) or the user's (&boundlist ixB^LIM, idimB, upperB, :71-99), which must
+// lie inside the grid; then the periodic pairs (:103-120), matched by direction,
+// orientation and extent.  ixB holds ixBmin(1:ndim,1:nB) then ixBmax(1:ndim,1:nB)
+// (1-based), idimB 1..ndim, upperB 0/1.
+int oracle_set_boundaries(oracle_ctx* cx, int nB, const char* typeB, const int* ixB, const int* idimB,
+                          const int* upperB, const int* ipairB) {
   Oracle& o = cx->o;
   if (!o.grid_set) return SAC_ERR_STATE;
-  if (nB != 2 * o.ndim) return SAC_ERR_UNSUPPORTED;
+  if (nB < 1 || nB > SAC_NHIB) return SAC_ERR_ARG;
+  const bool user = ixB != nullptr;
+  if (user && (!idimB || !upperB)) return SAC_ERR_ARG;
+  if (!user && nB != 2 * o.ndim) return SAC_ERR_ARG;
   o.nB = nB;
   o.typeB.assign((size_t)o.nw * nB, "");
   for (int iB = 0; iB < nB; ++iB)
@@ -1356,24 +1370,48 @@ int oracle_set_boundaries(oracle_ctx* cx, int nB, const char* typeB, const int* 
       o.typeB[iw + (long)o.nw * iB] = s;
     }
   for (int iB = 0; iB < nB; ++iB) {
-    int d = iB / 2;
-    o.idimB[iB] = d;
-    o.upperB[iB] = (iB % 2) == 1;
-    o.ixB[iB] = o.ixG;
-    if (o.upperB[iB]) {
-      o.ixB[iB].lo[d] = o.ixM.hi[d] + 1;
-      o.ixB[iB].hi[d] = o.ixG.hi[d];
+    if (user) {
+      const int d = idimB[iB] - 1;
+      if (d < 0 || d >= o.ndim) {
+        o.err = "Error in BoundSetup: idimB out of range";
+        return SAC_ERR_ARG;
+      }
+      o.idimB[iB] = d;
+      o.upperB[iB] = upperB[iB] != 0;
+      o.ixB[iB] = o.ixG;
+      for (int e = 0; e < o.ndim; ++e) {
+        o.ixB[iB].lo[e] = ixB[e + o.ndim * iB] - 1;
+        o.ixB[iB].hi[e] = ixB[o.ndim * nB + e + o.ndim * iB] - 1;
+        if (o.ixB[iB].lo[e] < o.ixG.lo[e] || o.ixB[iB].hi[e] > o.ixG.hi[e]) {
+          o.err = "Error in BoundSetup: Boundary region is outside grid";
+          return SAC_ERR_ARG;
+        }
+      }
     } else {
-      o.ixB[iB].lo[d] = o.ixG.lo[d];
-      o.ixB[iB].hi[d] = o.ixM.lo[d] - 1;
+      int d = iB / 2;
+      o.idimB[iB] = d;
+      o.upperB[iB] = (iB % 2) == 1;
+      o.ixB[iB] = o.ixG;
+      if (o.upperB[iB]) {
+        o.ixB[iB].lo[d] = o.ixM.hi[d] + 1;
+        o.ixB[iB].hi[d] = o.ixG.hi[d];
+      } else {
+        o.ixB[iB].lo[d] = o.ixG.lo[d];
+        o.ixB[iB].hi[d] = o.ixM.lo[d] - 1;
+      }
     }
     o.ipairB[iB] = ipairB ? ipairB[iB] - 1 : -1;
   }
+  auto same_extent = [&](int iB, int jB) {
+    for (int e = 0; e < o.ndim; ++e)
+      if (o.ixB[iB].hi[e] - o.ixB[iB].lo[e] != o.ixB[jB].hi[e] - o.ixB[jB].lo[e]) return false;
+    return true;
+  };
   for (int iB = 0; iB < nB; ++iB) {
     if (o.typeB[0 + (long)o.nw * iB] == "periodic" && o.ipairB[iB] < 0) {
       for (int jB = iB + 1; jB < nB; ++jB)
         if (o.typeB[(long)o.nw * jB] == "periodic" && o.ipairB[jB] < 0 && o.idimB[iB] == o.idimB[jB] &&
-            o.upperB[iB] != o.upperB[jB]) {
+            o.upperB[iB] != o.upperB[jB] && same_extent(iB, jB)) {
           o.ipairB[iB] = jB;
           o.ipairB[jB] = iB;
         }

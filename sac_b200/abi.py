@@ -45,7 +45,7 @@ def load(path: str = PRODUCT_LIB, prefix: str = "sac_"):
     f = lambda n: getattr(lib, prefix + n)  # noqa: E731
     f("create").argtypes = [ctypes.POINTER(SacParams), ctypes.POINTER(P)]
     f("set_grid").argtypes = [P, ctypes.c_int, ctypes.c_int, ip, ip, dp, ctypes.c_int]
-    f("set_boundaries").argtypes = [P, ctypes.c_int, ctypes.c_char_p, ip]
+    f("set_boundaries").argtypes = [P, ctypes.c_int, ctypes.c_char_p, ip, ip, ip, ip]
     f("upload").argtypes = [P, dp]
     f("download").argtypes = [P, dp]
     f("getboundary").argtypes = [P, ctypes.c_double]
@@ -104,13 +104,27 @@ class Context:
         self.nw = 3 * ndir + 4
         self.shape = tuple(int(v) for v in ixGhi[:ndim])
 
-    def set_boundaries(self, typeB_packed: bytes, nB: int, ipairB=None):
-        ip = None
-        if ipairB is not None:
-            arr = np.ascontiguousarray(ipairB, dtype=np.int32)
-            self._keep = arr
-            ip = _ip(arr)
-        self._call("set_boundaries", int(nB), typeB_packed, ip)
+    def set_boundaries(self, typeB_packed: bytes, nB: int, ipairB=None, regions=None):
+        """boundsetup.  regions: None for the default 2*ndim regions, or the user's
+        as (ixBmin, ixBmax, idimB, upperB): ixBmin/ixBmax [nB][ndim] 1-based
+        inclusive limits, idimB [nB] in 1..ndim, upperB [nB] booleans."""
+        keep = []
+
+        def arr(v):
+            a = np.ascontiguousarray(v, dtype=np.int32).reshape(-1)
+            keep.append(a)
+            return _ip(a)
+
+        ip = arr(ipairB) if ipairB is not None else None
+        ixb = idb = upb = None
+        if regions is not None:
+            lo, hi, idim, upper = regions
+            ixb = arr(np.concatenate([np.asarray(lo, dtype=np.int32).reshape(-1),
+                                      np.asarray(hi, dtype=np.int32).reshape(-1)]))
+            idb = arr(idim)
+            upb = arr([1 if u else 0 for u in upper])
+        self._keep = keep
+        self._call("set_boundaries", int(nB), typeB_packed, ixb, idb, upb, ip)
 
     def upload(self, w):
         w = np.asfortranarray(w, dtype=np.float64)

@@ -66,6 +66,16 @@ struct sac_ctx {
   std::vector<int> h_fixed;
   int pairshift[3][2] = {{0, 0}, {0, 0}, {0, 0}};
   int zero1[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  // user boundary regions (&boundlist ixB^LIM): filled one region per launch, in order
+  struct Region {
+    int lo[3], hi[3];
+    int d, up;
+    long shift, cells, fixoff;
+    bool anyfix;
+  };
+  bool regions = false;
+  int nB = 0;
+  std::vector<Region> reg;
   // host-side grid reductions
   double mindx2[3] = {0, 0, 0};  // min over the mesh of dx*dx per dimension
   double mindx_all = 0;          // min over the mesh and all dimensions of dx
@@ -210,9 +220,40 @@ BcArgs bc_args(sac_ctx* c, void* A) {
   return b;
 }
 
+RegionArgs region_args(sac_ctx* c, void* A, int iB) {
+  const sac_ctx::Region& r = c->reg[iB];
+  RegionArgs a{};
+  a.g = c->g;
+  a.A = A;
+  a.bgA = c->BG;
+  a.type = c->d_type;
+  a.fixed = c->d_fixed;
+  a.fixB = r.anyfix ? c->fixB + r.fixoff : nullptr;
+  for (int e = 0; e < 3; ++e) {
+    a.lo[e] = r.lo[e];
+    a.hi[e] = r.hi[e];
+  }
+  a.shift = r.shift;
+  a.cells = r.cells;
+  a.d = r.d;
+  a.up = r.up;
+  a.iB = iB;
+  a.nB = c->nB;
+  a.fullgridini = c->fullgridini;
+  return a;
+}
+
 template <typename S>
 void launch_bound(sac_ctx* c, const BcArgs& b, int nvar) {
   const Geom& g = c->g;
+  if (c->regions) {  // user regions: one pass per region, in the reference's order
+    for (int iB = 0; iB < c->nB; ++iB) {
+      const RegionArgs a = region_args(c, b.A, iB);
+      Prof pr(c, SAC_K_BOUND);
+      k_bound_region<S><<<(unsigned)((a.cells + 255) / 256), 256, 0, c->stream>>>(a, nvar);
+    }
+    return;
+  }
   long ns[3];
   ghost_slabs(g, ns);
   const long tot = ns[0] + ns[1] + ns[2];
@@ -299,8 +340,9 @@ sac_status advect1_t(sac_ctx* c, const std::string& method, double qdt, int dmin
   } else if (base != out) {
     CK(cudaMemcpyAsync(out, base, c->es * g.np * g.ncell, cudaMemcpyDeviceToDevice, c->stream));
   }
+  if ((c->par.smallfix || c->regions) && epi != EPI_PLAIN)
+    return fail(c, SAC_ERR_STATE, "smallfix and user boundary regions need the unfused Runge-Kutta stages");
   if (c->par.smallfix) {  // getboundary's keeppositive, src/vacgrid.t:220
-    if (epi != EPI_PLAIN) return fail(c, SAC_ERR_STATE, "smallfix needs the unfused Runge-Kutta stages");
     sac_status st = keeppositive(c, out);
     if (st != SAC_OK) return st;
   }
@@ -599,7 +641,10 @@ __global__ void __launch_bounds__(1024) k_courant_final(double* part, int n) {
   if (threadIdx.x == 0) part[kStaticPartials] = best;
 }
 
-// device address of g_courant_scratch per device ordinal, looked up once
+// device address of g_courant_scratch per device ordinal, looked up once.  The
+// address belongs to the module loaded in the device's primary context; it stays
+// valid as long as that context lives (no cudaDeviceReset while the library is
+// loaded), which the header states as a condition of sac_getdt_static.
 std::mutex g_static_mu;
 double* g_static_addr[64] = {};
 
@@ -637,12 +682,17 @@ sac_status courant_max_static(sac_ctx* c, double* cm) {
       default: k_courant_partial<3, S><<<nb, 256, 0, c->stream>>>(g, wp, c->BG, c->dx, part, c->par.gamma); break;
     }
   };
-  if (c->prec == SAC_PREC_FP32)
-    launch(0.0f);
-  else
-    launch(0.0);
-  k_courant_final<<<1, 1024, 0, c->stream>>>(part, nb);
-  c->kernel_launches += 2;
+  {
+    Prof pr(c, SAC_K_COURANT);
+    if (c->prec == SAC_PREC_FP32)
+      launch(0.0f);
+    else
+      launch(0.0);
+  }
+  {
+    Prof pr(c, SAC_K_COURANT);
+    k_courant_final<<<1, 1024, 0, c->stream>>>(part, nb);
+  }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(cm, part + kStaticPartials, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -818,12 +868,72 @@ sac_status sac_set_grid(sac_ctx* c, int ndim, int ndir, const int ixGhi[3], cons
   return SAC_OK;
 }
 
-sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* ipairB) {
+sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* ixB, const int* idimB,
+                              const int* upperB, const int* ipairB) {
   if (!c || !typeB) return SAC_ERR_ARG;
   if (!c->grid_set) return fail(c, SAC_ERR_STATE, "sac_set_grid first");
   const Geom& g = c->g;
-  if (nB != 2 * g.ndim) return fail(c, SAC_ERR_UNSUPPORTED, "only the default 2*ndim boundary regions are implemented");
+  const bool user = ixB != nullptr;
+  if (user && (!idimB || !upperB)) return fail(c, SAC_ERR_ARG, "user boundary regions need ixB, idimB and upperB");
+  if (nB < 1 || nB > SAC_NHIB) return fail(c, SAC_ERR_ARG, "nB must be 1..nhiB (10)");
+  if (!user && nB != 2 * g.ndim) return fail(c, SAC_ERR_ARG, "the default boundary regions are 2*ndim");
   CK(cudaSetDevice(c->dev));
+  // the regions, 0-based and inclusive: the default ones (boundsetup, src/vacgrid.t:53-70)
+  // or the user's, which must lie inside the grid (:71-99)
+  std::vector<sac_ctx::Region> reg((size_t)nB);
+  bool is_default = true;
+  for (int iB = 0; iB < nB; ++iB) {
+    sac_ctx::Region& r = reg[iB];
+    r = sac_ctx::Region{};
+    const int dd = iB / 2;
+    int dlo[3], dhi[3];  // the default region iB (when iB < 2*ndim)
+    for (int e = 0; e < 3; ++e) {
+      dlo[e] = 0;
+      dhi[e] = e < g.ndim ? g.n[e] - 1 : 0;
+    }
+    if (dd < g.ndim) {
+      if (iB % 2) {
+        dlo[dd] = g.hi[dd] + 1;
+      } else {
+        dhi[dd] = g.lo[dd] - 1;
+      }
+    }
+    if (user) {
+      r.d = idimB[iB] - 1;
+      r.up = upperB[iB] ? 1 : 0;
+      if (r.d < 0 || r.d >= g.ndim) return fail(c, SAC_ERR_ARG, "Error in BoundSetup: idimB out of range");
+      for (int e = 0; e < 3; ++e) {
+        r.lo[e] = e < g.ndim ? ixB[e + g.ndim * iB] - 1 : 0;
+        r.hi[e] = e < g.ndim ? ixB[g.ndim * nB + e + g.ndim * iB] - 1 : 0;
+        if (e < g.ndim && (r.lo[e] < 0 || r.hi[e] > g.n[e] - 1 || r.lo[e] > r.hi[e]))
+          return fail(c, SAC_ERR_ARG, "Error in BoundSetup: Boundary region is outside grid (iB=" +
+                                          std::to_string(iB + 1) + ")");
+      }
+      if (r.up ? r.lo[r.d] <= g.hi[r.d] : r.hi[r.d] >= g.lo[r.d])
+        return fail(c, SAC_ERR_UNSUPPORTED, "boundary region " + std::to_string(iB + 1) +
+                                                " reaches into the mesh along idimB; regions must lie in the ghost layers");
+    } else {
+      r.d = dd;
+      r.up = iB % 2;
+      for (int e = 0; e < 3; ++e) {
+        r.lo[e] = dlo[e];
+        r.hi[e] = dhi[e];
+      }
+    }
+    bool same = iB < 2 * g.ndim && r.d == dd && r.up == iB % 2;
+    for (int e = 0; e < 3 && same; ++e) same = r.lo[e] == dlo[e] && r.hi[e] == dhi[e];
+    is_default = is_default && same;
+    r.cells = 1;
+    for (int e = 0; e < 3; ++e) r.cells *= (long)(r.hi[e] - r.lo[e] + 1);
+  }
+  is_default = is_default && nB == 2 * g.ndim;
+  // gradient4, gradient1 and setnu read the boundary of dimension idim from the regions
+  // 2*idim-1 (lower) and 2*idim (upper) (src/vacgrid.t:690-709, src/vacusr.viscosity.t:378-400)
+  if (nB < 2 * g.ndim) return fail(c, SAC_ERR_UNSUPPORTED, "fewer regions than 2*ndim");
+  for (int iB = 0; iB < 2 * g.ndim; ++iB)
+    if (reg[iB].d != iB / 2 || reg[iB].up != iB % 2)
+      return fail(c, SAC_ERR_UNSUPPORTED,
+                  "regions 2*idim-1 and 2*idim must be the lower and upper boundaries of dimension idim");
   c->h_type.assign((size_t)g.nw * nB, 0);
   c->h_fixed.assign((size_t)g.nw * nB, 0);
   std::vector<std::string> t((size_t)g.nw * nB);
@@ -836,18 +946,36 @@ sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* 
       if (!ok) return fail(c, SAC_ERR_UNSUPPORTED, "boundary type '" + s + "' is not implemented");
       t[iw + (long)g.nw * iB] = s;
     }
-  // periodic pairing (src/vacgrid.t:109-120) and source offsets
-  int pair[6] = {-1, -1, -1, -1, -1, -1};
+  // periodic pairing (src/vacgrid.t:103-120): direction, orientation and extent
+  int pair[SAC_NHIB];
   for (int iB = 0; iB < nB; ++iB) pair[iB] = ipairB ? ipairB[iB] - 1 : -1;
+  auto same_extent = [&](int iB, int jB) {
+    for (int e = 0; e < g.ndim; ++e)
+      if (reg[iB].hi[e] - reg[iB].lo[e] != reg[jB].hi[e] - reg[jB].lo[e]) return false;
+    return true;
+  };
   for (int iB = 0; iB < nB; ++iB)
     if (t[(long)g.nw * iB] == "periodic" && pair[iB] < 0) {
       for (int jB = iB + 1; jB < nB; ++jB)
-        if (t[(long)g.nw * jB] == "periodic" && pair[jB] < 0 && jB / 2 == iB / 2 && (jB % 2) != (iB % 2)) {
+        if (t[(long)g.nw * jB] == "periodic" && pair[jB] < 0 && reg[jB].d == reg[iB].d &&
+            reg[jB].up != reg[iB].up && same_extent(iB, jB)) {
           pair[iB] = jB;
           pair[jB] = iB;
         }
       if (pair[iB] < 0) return fail(c, SAC_ERR_ARG, "Error in BoundSetup: No periodic pair");
     }
+  for (int iB = 0; iB < nB; ++iB) {
+    if (pair[iB] < 0 || pair[iB] >= nB) continue;
+    // source of region iB: its pair moved by dixB along idim (src/vacgrid.t:236-246)
+    const sac_ctx::Region& q = reg[pair[iB]];
+    long sh = 0;
+    for (int e = 0; e < g.ndim; ++e) {
+      int se = q.lo[e] - reg[iB].lo[e];
+      if (e == reg[iB].d) se += reg[iB].up ? 2 : -2;
+      sh += (long)se * g.st[e];
+    }
+    reg[iB].shift = sh;
+  }
   for (int d = 0; d < g.ndim; ++d) {
     const int nm = g.hi[d] - g.lo[d] + 1;
     c->pairshift[d][0] = nm;   // lower ghosts copy ixMmax-1..ixMmax
@@ -857,22 +985,34 @@ sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* 
       c->zero1[d][s] = (t1 != "periodic" && t1 != "mpi") ? 1 : 0;
     }
   }
-  // fixB slabs for every region that holds a fixed-type variable
+  // fixB slabs for every region that holds a fixed-type variable: the default
+  // regions' slabs are the dixB layers times the full grid across (k_bound), a user
+  // region's slab is its own cells
   long off = 0;
   for (int iB = 0; iB < nB; ++iB) {
-    const int d = iB / 2;
-    long sl = 2;  // dixB layers
-    for (int e = 0; e < g.ndim; ++e)
-      if (e != d) sl *= g.n[e];
-    c->slab[iB] = sl;
-    c->fixoff[iB] = off;
+    long sl;
+    if (is_default) {
+      const int d = iB / 2;
+      sl = 2;  // dixB layers
+      for (int e = 0; e < g.ndim; ++e)
+        if (e != d) sl *= g.n[e];
+      if (iB < 6) c->slab[iB] = sl;
+    } else {
+      sl = reg[iB].cells;
+    }
+    if (iB < 6) c->fixoff[iB] = off;
+    reg[iB].fixoff = off;
     bool any = false;
     for (int iw = 0; iw < g.nw; ++iw) {
       int8_t ty = c->h_type[iw * nB + iB];
       any = any || ty == BT_FIXED || ty == BT_FIXED1 || ty == BT_GRAD1;
     }
+    reg[iB].anyfix = any;
     if (any) off += sl * g.nw;
   }
+  c->nB = nB;
+  c->reg = reg;
+  c->regions = !is_default;
   if (c->fixB) cudaFree(c->fixB), c->fixB = nullptr;
   if (c->d_type) cudaFree(c->d_type), c->d_type = nullptr;
   if (c->d_fixed) cudaFree(c->d_fixed), c->d_fixed = nullptr;
@@ -943,13 +1083,25 @@ sac_status sac_getboundary(sac_ctx* c, double t) {
   else
     launch_bound<double>(c, b, g.nw);
   if (!c->bc_init_done) {
-    const int nB = 2 * g.ndim;
+    const int nB = c->nB;
     for (int iB = 0; iB < nB; ++iB)
       for (int iw = 0; iw < g.nw; ++iw) {
         const int8_t ty = c->h_type[iw * nB + iB];
         if ((ty == BT_FIXED || ty == BT_FIXED1 || ty == BT_GRAD1) && !c->h_fixed[iw * nB + iB]) {
           const int bs = 256;
           Prof pr(c, SAC_K_OTHER);
+          if (c->regions) {
+            RegionArgs a = region_args(c, c->P[0], iB);
+            const unsigned nb = (unsigned)((a.cells + bs - 1) / bs);
+            if (c->prec == SAC_PREC_FP32)
+              k_fixcapture_region<float><<<nb, bs, 0, c->stream>>>(a, c->fixB + c->reg[iB].fixoff, iw,
+                                                                   ty == BT_GRAD1 ? 1 : 0);
+            else
+              k_fixcapture_region<double><<<nb, bs, 0, c->stream>>>(a, c->fixB + c->reg[iB].fixoff, iw,
+                                                                    ty == BT_GRAD1 ? 1 : 0);
+            c->h_fixed[iw * nB + iB] = 1;
+            continue;
+          }
           const unsigned nb = (unsigned)((c->slab[iB] + bs - 1) / bs);
           if (c->prec == SAC_PREC_FP32)
             k_fixcapture<float><<<nb, bs, 0, c->stream>>>(g, (const float*)c->P[0], c->BG, c->fixB, c->fixoff[iB],
@@ -1097,9 +1249,10 @@ sac_status sac_advect(sac_ctx* c, const char* method, const int* iws, int idimmi
     st = (x);                     \
     if (st != SAC_OK) return st;  \
   } while (0)
-  if (ta == "fourstep" && c->par.smallfix) {
+  if (ta == "fourstep" && (c->par.smallfix || c->regions)) {
     // keeppositive changes the mesh of w3 and of w at their fills, before the
-    // combinations read them: the combinations run as passes of their own
+    // combinations read them, and user regions fill region by region: the
+    // combinations run as passes of their own, as src/vac.t:450,454 write them
     const long n = (long)g.np * g.ncell;
     RUN(advect1(c, m, dt / 2, dmin, dmax, t, w, w, w1, mask));
     RUN(advect1(c, m, dt / 2, dmin, dmax, t, w1, w, w2, mask));

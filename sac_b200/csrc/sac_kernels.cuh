@@ -450,6 +450,133 @@ __global__ void k_fixcapture(Geom g, const S* __restrict__ A, const double* __re
   fixB[off + (long)iw * slab + t] = v;
 }
 
+// ---------------------------------------------------------------------------
+// user boundary regions (&boundlist ixB^LIM, idimB, upperB; src/vacgrid.t:71-99):
+// getboundary fills region iB = 1..nB in order (src/vacgrid.t:227-471), one
+// launch per region.  Every source a region reads lies outside it along idimB (the
+// edge, the inner edge, the mirror image, the periodic pair or fixB), so the cells
+// of one region are independent and one parallel pass per region, in region
+// order, is the sequential result; corners that several regions cover take the
+// value of the last one, as in the reference.
+// ---------------------------------------------------------------------------
+struct RegionArgs {
+  Geom g;
+  void* A;                          // advanced block (np variables, storage type), field stride g.ncell
+  double* bgA;                      // background block (nw-np variables)
+  const int8_t* __restrict__ type;  // [iw*nB + iB]
+  const int* __restrict__ fixed;    // [iw*nB + iB] 1 once fixB holds values
+  const double* __restrict__ fixB;  // this region's slab: nw blocks of `cells` values
+  int lo[3], hi[3];                 // the region (0-based, inclusive; 0..0 beyond ndim)
+  long shift;                       // periodic: cell offset of the source (the pair moved by dixB)
+  long cells;
+  int d, up, iB, nB;
+  int fullgridini;  // a fixed-type variable not yet in fixB keeps the values read
+};
+
+__device__ __forceinline__ void region_cell(const RegionArgs& a, long t, int p[3]) {
+  const unsigned e0 = a.hi[0] - a.lo[0] + 1, e1 = a.hi[1] - a.lo[1] + 1;
+  const unsigned ut = (unsigned)t, q = ut / e0;
+  p[0] = a.lo[0] + (int)(ut - q * e0);
+  p[1] = a.lo[1] + (int)(q % e1);
+  p[2] = a.lo[2] + (int)(q / e1);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_bound_region(const __grid_constant__ RegionArgs a, int nvar) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= a.cells) return;
+  const Geom& g = a.g;
+  int p[3];
+  region_cell(a, t, p);
+  const long N = g.ncell, sd = g.st[a.d];
+  const long c = p[0] + g.st[1] * p[1] + g.st[2] * p[2];
+  const int pd = p[a.d];
+  auto rd = [&](int iw, long cc) {
+    return iw < g.np ? (double)((const S*)a.A)[(long)iw * N + cc] : a.bgA[(long)(iw - g.np) * N + cc];
+  };
+  const int ixe = a.up ? a.lo[a.d] - 1 : a.hi[a.d] + 1;  // the edge the region copies from
+  for (int iw = 0; iw < nvar; ++iw) {
+    const int ty = a.type[iw * a.nB + a.iB];
+    const bool isfixed = a.fixed[iw * a.nB + a.iB] != 0;
+    double v;
+    bool store = true;
+    switch (ty) {
+      case BT_CONT:
+      case BT_FIXED:  // src/vacgrid.t:343-368
+        if (isfixed)
+          v = a.fixB[(long)iw * a.cells + t];
+        else if (ty == BT_CONT || !a.fullgridini)
+          v = rd(iw, c + (long)(ixe - pd) * sd);
+        else
+          store = false;
+        break;
+      case BT_PERIODIC:  // :411-413
+        v = rd(iw, c + a.shift);
+        break;
+      case BT_SYMM:
+      case BT_SYMM0:
+      case BT_ASYMM: {  // :414-446
+        const int m = a.up ? 2 * a.lo[a.d] - 1 : 2 * a.hi[a.d] + 1;
+        v = rd(iw, c + (long)(m - 2 * pd) * sd);
+        if (ty == BT_ASYMM) v = -v;
+        break;
+      }
+      case BT_CONTCD4: {  // :261-293: the plane ixmin, then the plane ixmax
+        const int se = a.up ? a.lo[a.d] - 2 : a.hi[a.d] + 3, see = a.up ? a.lo[a.d] - 3 : a.hi[a.d] + 2;
+        if (pd == a.hi[a.d])
+          v = rd(iw, c + (long)(see - pd) * sd);
+        else if (pd == a.lo[a.d])
+          v = rd(iw, c + (long)(se - pd) * sd);
+        else
+          store = false;
+        break;
+      }
+      default: {  // cont1, fixed1, grad1, :369-409
+        if (isfixed) {
+          v = a.fixB[(long)iw * a.cells + t];
+          if (ty == BT_GRAD1) v = v + rd(iw, c + (long)(ixe - pd) * sd);
+        } else if (ty == BT_CONT1 || !a.fullgridini) {
+          const int ixf = a.up ? ixe - 1 : ixe + 1;
+          const int n = abs(pd - ixe);
+          v = sub_rn(mul_rn((double)(n + 1), rd(iw, c + (long)(ixe - pd) * sd)),
+                     mul_rn((double)n, rd(iw, c + (long)(ixf - pd) * sd)));
+        } else {
+          store = false;
+        }
+        break;
+      }
+    }
+    if (!store) continue;
+    if (iw < g.np)
+      ((S*)a.A)[(long)iw * N + c] = (S)v;
+    else
+      a.bgA[(long)(iw - g.np) * N + c] = v;
+  }
+}
+
+// fixB of a user region for variable iw after the first fill (src/vacgrid.t:476-507):
+// the values, or for grad1 their differences to the region's edge
+template <typename S>
+__global__ void __launch_bounds__(256) k_fixcapture_region(const __grid_constant__ RegionArgs a, double* fixB,
+                                                           int iw, int grad) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= a.cells) return;
+  const Geom& g = a.g;
+  int p[3];
+  region_cell(a, t, p);
+  const long N = g.ncell;
+  const long c = p[0] + g.st[1] * p[1] + g.st[2] * p[2];
+  auto rd = [&](long cc) {
+    return iw < g.np ? (double)((const S*)a.A)[(long)iw * N + cc] : a.bgA[(long)(iw - g.np) * N + cc];
+  };
+  double v = rd(c);
+  if (grad) {
+    const int ixe = a.up ? a.lo[a.d] - 1 : a.hi[a.d] + 1;
+    v = v - rd(c + (long)(ixe - p[a.d]) * g.st[a.d]);
+  }
+  fixB[(long)iw * a.cells + t] = v;
+}
+
 // storage conversions for the FP32 path
 template <typename D, typename S>
 __global__ void k_convert(D* __restrict__ dst, const S* __restrict__ src, long n) {

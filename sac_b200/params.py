@@ -279,3 +279,50 @@ def typeB_from_par(pf: ParFile, nw: int, nB: int) -> list[list[str]]:
     for n, t in enumerate(flat[: nw * nB]):
         types[n // nw][n % nw] = str(t).strip()
     return types
+
+
+def _namelist_array(pf: ParFile, group: str, name: str, shape: tuple, default):
+    """A NAMELIST array of `shape` (Fortran order) from a whole-array list
+    (name = v1, v2, ...) and/or element keys (name(i,j) = v, ...), a list after an
+    element key continuing in column-major order, as NAMELIST input fills it."""
+    n = 1
+    for e in shape:
+        n *= e
+    flat = [default] * n
+    grp = pf.groups.get(group, {})
+
+    def put(start, vals):
+        vals = vals if isinstance(vals, list) else [vals]
+        for k, v in enumerate(vals):
+            if start + k < n:
+                flat[start + k] = v
+
+    name = name.lower()
+    if name in grp:
+        put(0, grp[name])
+    for k, v in grp.items():
+        if k.startswith(name + "(") and k.endswith(")"):
+            idx = [int(x) - 1 for x in k[len(name) + 1:-1].split(",")]
+            lin, mul = 0, 1
+            for i, e in zip(idx, shape):
+                lin += i * mul
+                mul *= e
+            put(lin, v)
+    return flat
+
+
+def boundary_regions_from_par(pf: ParFile, ndim: int):
+    """&boundlist's nB and, when the user gave regions (ixBmax(1,1) /= 0,
+    src/vacio.t:117 and src/vacgrid.t:53), (ixBmin, ixBmax, idimB, upperB) as
+    Context.set_boundaries takes them, with ipairB (0 = automatic); else None."""
+    nB = int(pf.get("boundlist", "nb", 2 * ndim))
+    lo = _namelist_array(pf, "boundlist", "ixbmin", (ndim, 10), 0)
+    hi = _namelist_array(pf, "boundlist", "ixbmax", (ndim, 10), 0)
+    ipair = [int(v) for v in _namelist_array(pf, "boundlist", "ipairb", (10,), 0)][:nB]
+    if int(hi[0]) == 0:
+        return nB, None, ipair
+    idim = [int(v) for v in _namelist_array(pf, "boundlist", "idimb", (10,), 0)][:nB]
+    upper = [bool(v) for v in _namelist_array(pf, "boundlist", "upperb", (10,), False)][:nB]
+    ixlo = [[int(lo[d + ndim * iB]) for d in range(ndim)] for iB in range(nB)]
+    ixhi = [[int(hi[d + ndim * iB]) for d in range(ndim)] for iB in range(nB)]
+    return nB, (ixlo, ixhi, idim, upper), ipair

@@ -37,6 +37,9 @@ class Problem:
     tmax: float = 1e99
     nsteps: int = 0
     meta: dict = field(default_factory=dict)
+    # user boundary regions (ixBmin, ixBmax, idimB, upperB) for Context.set_boundaries,
+    # one per entry of typeB; None: the 2*ndim default regions
+    regions: tuple = None
 
     @property
     def nw(self):
@@ -59,7 +62,7 @@ class Problem:
 
     @property
     def nB(self):
-        return 2 * self.ndim
+        return len(self.typeB) if self.regions is not None else 2 * self.ndim
 
     @property
     def ncells(self):

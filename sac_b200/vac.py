@@ -180,7 +180,7 @@ class Run:
             raise ValueError("divbfix=T requires unsplitsource=T or splitsource=T !")
         # options that change the run but are not built: say so rather than ignore them
         for grp, key, off, what in (("methodlist", "divbconstrain", False, "divbconstrain=T (the CT module)"),
-                                    ("boundlist", "extraB", False, "extraB=T (user boundary regions)")):
+                                    ("boundlist", "extraB", False, "extraB=T (a user specialbound before every fill)")):
             if bool(g(grp, key, off)) != off:
                 raise NotImplementedError(what + " is outside the implemented path")
         if str(g("filelist", "typefilelog", "default")).strip() != "default":
@@ -218,7 +218,9 @@ class Run:
             # src/vac.t:76 resets dtpar after the first step; the context's
             # parameters are fixed at its creation
             raise NotImplementedError("slowsteps=1 with dtpar>0 is outside the implemented path")
-        self.types = params.typeB_from_par(pf, nw, 2 * ndim)
+        # &boundlist regions: the default 2*ndim, or the user's ixB^LIM/idimB/upperB
+        self.nB, self.regions, self.ipairB = params.boundary_regions_from_par(pf, ndim)
+        self.types = params.typeB_from_par(pf, nw, self.nB)
         self.wnames = g("methodlist", "wnames", snap.varnames)
         self.fileheadout, self.varnames = header_strings(str(g("methodlist", "fileheadout", snap.header)),
                                                          snap.varnames, ndim, ndir, user)
@@ -232,7 +234,7 @@ class Run:
         self.dt = 0.0
         self.ctx = (context or abi.Context)(self.params)
         self.ctx.set_grid(ndim, ndir, self.ixGhi, self.ixM, self.x, self.fullgridini)
-        self.ctx.set_boundaries(params.pack_typeB(self.types), 2 * ndim)
+        self.ctx.set_boundaries(params.pack_typeB(self.types), self.nB, ipairB=self.ipairB, regions=self.regions)
         self.ctx.upload(self.w)
         self.ctx.getboundary(self.t)
 

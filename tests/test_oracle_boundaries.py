@@ -159,3 +159,91 @@ def test_fills_match_for_random_shapes_and_types():
         o.close()
 
     check()
+
+
+def _fill_regions(w, nd, lo, hi, idim, up, types, pair):
+    """The first fill with user regions (src/vacgrid.t:227-471): region by region
+    in order, each over its own limits (1-based lo/hi), reading the edge, inner
+    edge, mirror or periodic pair outside it."""
+    w = w.copy()
+    for iB in range(len(types)):
+        d = idim[iB] - 1
+        box = tuple(slice(lo[iB][e] - 1, hi[iB][e]) for e in range(nd))
+        a0, a1 = lo[iB][d] - 1, hi[iB][d] - 1
+
+        def plane(i):
+            return tuple(i if e == d else box[e] for e in range(nd))
+
+        for iw in range(w.shape[-1]):
+            t = types[iB][iw]
+            a = w[..., iw]
+            ixe = a0 - 1 if up[iB] else a1 + 1
+            if t in ("cont", "fixed"):
+                for i in range(a0, a1 + 1):
+                    a[plane(i)] = a[plane(ixe)]
+            elif t in ("cont1", "fixed1", "grad1"):
+                ixf = ixe - 1 if up[iB] else ixe + 1
+                for i in range(a0, a1 + 1):
+                    n = abs(i - ixe)
+                    a[plane(i)] = float(n + 1) * a[plane(ixe)] - float(n) * a[plane(ixf)]
+            elif t == "periodic":
+                j = pair[iB]
+                src = tuple(slice(lo[j][e] - 1 + (2 if (e == d and up[iB]) else -2 if e == d else 0),
+                                  hi[j][e] + (2 if (e == d and up[iB]) else -2 if e == d else 0))
+                            for e in range(nd))
+                a[box] = a[src]
+            elif t in ("symm", "asymm"):
+                m = 2 * a0 - 1 if up[iB] else 2 * a1 + 1
+                for i in range(a0, a1 + 1):
+                    a[plane(i)] = (-1.0 if t == "asymm" else 1.0) * a[plane(m - i)]
+            else:
+                raise ValueError(t)
+    return w
+
+
+def test_user_regions_first_fill():
+    """Six regions in 2D: the defaults given explicitly (the x2 pair matched by
+    direction, orientation and extent) plus a 'cont1' and a 'symm'/'asymm'
+    sub-region of the lower x1 boundary that overwrite parts of the first region
+    and of each other, in order."""
+    P = problems.random_problem((10, 8), seed=31, types=["cont", "cont", "periodic", "periodic"])
+    nw = 3 * P.ndir + 4
+    G = [n + 4 for n in P.nx]
+    lo = [[1, 1], [G[0] - 1, 1], [1, 1], [1, G[1] - 1], [1, 2], [1, 5]]
+    hi = [[2, G[1]], [G[0], G[1]], [G[0], 2], [G[0], G[1]], [2, 6], [2, 9]]
+    idim = [1, 1, 2, 2, 1, 1]
+    up = [False, True, False, True, False, False]
+    types = [["cont"] * nw, ["cont"] * nw, ["periodic"] * nw, ["periodic"] * nw, ["cont1"] * nw, ["symm"] * nw]
+    types[5][1] = "asymm"
+    from sac_b200 import params
+    o = Oracle(P.params)
+    o.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
+    o.set_boundaries(params.pack_typeB(types), len(types), regions=(lo, hi, idim, up))
+    o.upload(P.w)
+    o.getboundary(0.0)
+    ref = _fill_regions(P.w, 2, lo, hi, idim, up, types, pair={2: 3, 3: 2})
+    np.testing.assert_array_equal(o.download(), ref)
+
+
+def test_explicit_default_regions_are_the_default_fill():
+    P = problems.random_problem((9, 7, 6), seed=32, types=["cont1", "fixed", "periodic", "periodic", "symm", "cont"])
+    G = [n + 4 for n in P.nx]
+    lo, hi, idim, up = [], [], [], []
+    for iB in range(6):
+        d, u = iB // 2, iB % 2
+        a, b = [1, 1, 1], list(G)
+        if u:
+            a[d] = G[d] - 1
+        else:
+            b[d] = 2
+        lo.append(a), hi.append(b), idim.append(d + 1), up.append(bool(u))
+    a = _util.start(Oracle, P)
+    o = Oracle(P.params)
+    o.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
+    o.set_boundaries(P.typeB_packed, P.nB, regions=(lo, hi, idim, up))
+    o.upload(P.w)
+    o.getboundary(0.0)
+    np.testing.assert_array_equal(o.download(), a.download())
+    _util.run(a, 2)
+    _util.run(o, 2)
+    np.testing.assert_array_equal(o.download(), a.download())
