@@ -42,6 +42,11 @@ typedef struct sac_fno_gemm_desc {
   int* err;
   long b_n1;    /* B rows split like A's: (n / b_nsplit)*b_n1 + (n % b_nsplit)*b_n */
   int b_nsplit;
+  int wait_tries; /* bound of the tensor-core pipeline waits, in tries of at most ~5 ms:
+                   * 0 = default (400), > 0 = that many, -1 = none: the first wait gives
+                   * up at once, sets bit 0 of *err and the kernel returns (a test of the
+                   * time-out path; MMAs already issued are still drained with the default
+                   * bound before the accumulator is released) */
 } sac_fno_gemm_desc;
 
 /* 0 on success; 1 on an argument that breaks the requirements (message in
@@ -105,6 +110,9 @@ int sac_fno_features(sac_fno* n, const void* state, int state_bf16, const float*
 int sac_fno_apply(sac_fno* n, float* state, const float* y, const float* scale, int B, int nst);
 /* synchronises; 7 when a tensor-core wait timed out since the last reset */
 int sac_fno_check(sac_fno* n, int reset);
+/* wait_tries of every GEMM the network launches (see sac_fno_gemm_desc; 0 =
+ * default, -1 = give up at once, for testing the time-out report) */
+int sac_fno_set_wait_tries(sac_fno* n, int tries);
 
 #ifdef __cplusplus
 }

@@ -13,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -73,13 +74,17 @@ def _build_lib(out, force=False, verbose=False, extra=()):
     src, units, _ = LIBS[out]
     objdir = os.path.join(HERE, "_build", os.path.basename(out).replace(".so", ""))
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for unit, flags in units:
         obj = os.path.join(objdir, unit.replace(".cu", ".o"))
-        _run([nvcc_path(), "-O3", "-std=c++17", *ARCH, "-lineinfo", *flags, "-Xcompiler", "-fPIC",
-              "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-c", "-o", obj, os.path.join(src, unit), *extra],
-             verbose)
+        cmds.append([nvcc_path(), "-O3", "-std=c++17", *ARCH, "-lineinfo", *flags, "-Xcompiler", "-fPIC",
+                     "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-c", "-o", obj, os.path.join(src, unit),
+                     *extra])
         objs.append(obj)
+    # the translation units compile independently: one nvcc each, side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, c, verbose) for c in cmds]:
+            f.result()
     _run([nvcc_path(), *ARCH, "-shared", "-o", out + ".tmp", *objs], verbose)
     os.replace(out + ".tmp", out)
     return out

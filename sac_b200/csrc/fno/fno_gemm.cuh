@@ -55,6 +55,11 @@ struct GemmDesc {
   // B rows split like A's: n = (n / b_nsplit, n % b_nsplit) -> (n / b_nsplit)*b_n1 + (n % b_nsplit)*b_n
   long b_n1;
   int b_nsplit;
+  // bound of the pipeline's mbarrier waits in tries of at most ~5 ms each:
+  // 0 = the default kWaitTries, > 0 = that many, < 0 = none (the first wait gives
+  // up at once; a test of the time-out path).  The wait that drains the MMAs in
+  // flight before the accumulator is released always keeps the default bound.
+  int wait_tries;
 };
 
 constexpr int kBM = 128, kBK = 64, kThreads = 128;
@@ -118,10 +123,12 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
 
+constexpr int kWaitTries = 400;  // ~2 s
+
 // bounded wait for the phase with the given parity; false on time-out
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int tries = kWaitTries) {
   const uint32_t a = smem_u32(bar);
-  for (int it = 0; it < 400; ++it) {  // each try suspends for at most ~5 ms
+  for (int it = 0; it < tries; ++it) {  // each try suspends for at most ~5 ms
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred P1;\n mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n selp.b32 %0, 1, 0, P1;\n}"
@@ -239,6 +246,7 @@ __global__ void __launch_bounds__(kThreads, BN <= 64 ? 4 : BN <= 128 ? 3 : 1) k_
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_sh;
   const uint32_t idesc = umma_idesc(BN, d.a_mn_major, d.b_mn_major);
+  const int tries = d.wait_tries == 0 ? kWaitTries : (d.wait_tries < 0 ? 0 : d.wait_tries);
 
   Tile16<kBM> ta;
   Tile16<BN> tb;
@@ -250,7 +258,7 @@ __global__ void __launch_bounds__(kThreads, BN <= 64 ? 4 : BN <= 128 ? 3 : 1) k_
     uint8_t* sb = sa + A_BYTES;
     load_tile<kBM>(ta, A, d.a_m0, d.a_m1, d.a_msplit, d.a_k, d.a_mn_major, m0, d.M, k0, kend);
     load_tile<BN>(tb, B, d.b_n, d.b_n1, d.b_nsplit, d.b_k, d.b_mn_major, n0, d.N, k0, kend);
-    if (kt >= 2 && !mbar_wait(&bar[s], ((kt - 2) >> 1) & 1)) ok = false;  // stage s free again
+    if (kt >= 2 && !mbar_wait(&bar[s], ((kt - 2) >> 1) & 1, tries)) ok = false;  // stage s free again
     if (__syncthreads_or(!ok)) {
       ok = false;
       break;
@@ -278,7 +286,7 @@ __global__ void __launch_bounds__(kThreads, BN <= 64 ? 4 : BN <= 128 ? 3 : 1) k_
     }
     issued = kt + 1;
   }
-  if (ok && issued > 0 && !mbar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1)) ok = false;
+  if (ok && issued > 0 && !mbar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1, tries)) ok = false;
   if (__syncthreads_or(!ok)) {
     if (tid == 0 && d.err) atomicOr(d.err, 1);
     // let the MMAs in flight drain (bounded) before the accumulator is released

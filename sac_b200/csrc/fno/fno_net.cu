@@ -282,6 +282,7 @@ struct sac_fno {
        *dtp = nullptr, *dhpre = nullptr, *dyb = nullptr;
   float *spec = nullptr, *dvacc = nullptr, *dpt = nullptr, *scal = nullptr;
   int* errw = nullptr;
+  int wait_tries = 0;  // GemmDesc::wait_tries of every launch (0: default bound)
 };
 
 namespace {
@@ -304,7 +305,9 @@ int fail(sac_fno* n, const std::string& m) {
 
 #define GK(desc)                      \
   do {                                \
-    int rc_ = gemm((desc), n->st);    \
+    GemmDesc d_ = (desc);             \
+    d_.wait_tries = n->wait_tries;    \
+    int rc_ = gemm(d_, n->st);        \
     if (rc_) return rc_;              \
   } while (0)
 
@@ -1022,6 +1025,12 @@ int sac_fno_check(sac_fno* n, int reset) {
   FK(cudaStreamSynchronize(n->st));
   if (reset) FK(cudaMemsetAsync(n->errw, 0, sizeof(int), n->st));
   if (e) return fail(n, "a tensor-core wait timed out (error word " + std::to_string(e) + ")") + 6;
+  return 0;
+}
+
+int sac_fno_set_wait_tries(sac_fno* n, int tries) {
+  if (!n) return 1;
+  n->wait_tries = tries < 0 ? -1 : tries;
   return 0;
 }
 

@@ -22,7 +22,7 @@ class GemmDesc(ctypes.Structure):
         ("c", VP), ("c_m0", ctypes.c_long), ("c_m1", ctypes.c_long), ("c_n", ctypes.c_long),
         ("c_b", ctypes.c_long), ("c_msplit", ctypes.c_int), ("c_bf16", ctypes.c_int), ("c_mode", ctypes.c_int),
         ("alpha", ctypes.c_float), ("bias_n", VP), ("add", VP), ("act", ctypes.c_int), ("pre", VP),
-        ("err", VP), ("b_n1", ctypes.c_long), ("b_nsplit", ctypes.c_int),
+        ("err", VP), ("b_n1", ctypes.c_long), ("b_nsplit", ctypes.c_int), ("wait_tries", ctypes.c_int),
     ]
 
 
@@ -57,7 +57,8 @@ def check(rc, lib=None):
 def gemm(M, N, K, a, b, c, *, batch=1, ksplit=1, a_m0=None, a_m1=0, a_k=1, a_b=0, a_msplit=None,
          a_mn_major=False, b_n=None, b_k=1, b_b=0, b_mn_major=False, b_n1=0, b_nsplit=None,
          c_m0=None, c_m1=0, c_n=1, c_b=0,
-         c_msplit=None, c_bf16=False, c_mode=0, alpha=1.0, bias_n=0, add=0, act=0, pre=0, err=0, stream=0):
+         c_msplit=None, c_bf16=False, c_mode=0, alpha=1.0, bias_n=0, add=0, act=0, pre=0, err=0, stream=0,
+         wait_tries=0):
     """Thin call of sac_fno_gemm with integer device pointers (0 = none)."""
     lib = load()
     d = GemmDesc()
@@ -78,6 +79,7 @@ def gemm(M, N, K, a, b, c, *, batch=1, ksplit=1, a_m0=None, a_m1=0, a_k=1, a_b=0
     d.c_msplit = (1 << 30) if c_msplit is None else c_msplit
     d.c_bf16, d.c_mode, d.alpha = int(bool(c_bf16)), c_mode, alpha
     d.bias_n, d.add, d.act, d.pre, d.err = bias_n or None, add or None, act, pre or None, err or None
+    d.wait_tries = wait_tries
     check(lib.sac_fno_gemm(ctypes.byref(d), VP(stream) if stream else None), lib)
 
 
@@ -117,9 +119,10 @@ def _bind_net(lib):
     lib.sac_fno_features.argtypes = [VP, VP, ctypes.c_int, VP, VP, ctypes.c_int, VP, ctypes.c_int, ctypes.c_int]
     lib.sac_fno_apply.argtypes = [VP, VP, VP, VP, ctypes.c_int, ctypes.c_int]
     lib.sac_fno_check.argtypes = [VP, ctypes.c_int]
+    lib.sac_fno_set_wait_tries.argtypes = [VP, ctypes.c_int]
     for f in ("sac_fno_create", "sac_fno_param_layout", "sac_fno_init", "sac_fno_set_params", "sac_fno_get_params",
               "sac_fno_get_grads", "sac_fno_zero_grad", "sac_fno_forward", "sac_fno_infer", "sac_fno_backward", "sac_fno_mse",
-              "sac_fno_adam", "sac_fno_features", "sac_fno_apply", "sac_fno_check"):
+              "sac_fno_adam", "sac_fno_features", "sac_fno_apply", "sac_fno_check", "sac_fno_set_wait_tries"):
         getattr(lib, f).restype = ctypes.c_int
     lib._net_bound = True
     return lib
@@ -207,6 +210,10 @@ class Net:
 
     def check(self, reset=True):
         self._c(self.lib.sac_fno_check(self.h, int(bool(reset))))
+
+    def set_wait_tries(self, tries):
+        """Bound of the tensor-core waits of every GEMM (0: default; -1: give up at once)."""
+        self._c(self.lib.sac_fno_set_wait_tries(self.h, int(tries)))
 
     def close(self):
         if self.h:

@@ -2,9 +2,11 @@
 initial-data scripts (inipar/briowu-test12.py, inipar/riemann-test11.py,
 inipar/strongshock-test11.py of drewleonard42/SAC).
 
-Run in a container where the reference tree is mounted (default /root/reference);
-each script is executed unmodified in a scratch directory and the .ini file it
-writes is copied here.  The tests read only the copies.
+Run with the reference tree's root in the environment variable SAC_REFERENCE
+(required); each script is executed unmodified in a scratch directory and the
+.ini file it writes is copied here.  The tests read only the copies.
+
+    SAC_REFERENCE=<path to the SAC tree> python tests/golden/make_golden.py
 
 The scripts were written for Python 2, whose list comprehensions leak their loop
 variable: line 37 of each uses `p`, the last entry of `nprocs` (1 for the `_np01`
@@ -16,7 +18,6 @@ import runpy
 import shutil
 import tempfile
 
-REF = os.environ.get("SAC_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 SCRIPTS = {
     "briowu-test12.py": "data/briowu-test12_np01_000.ini",
@@ -26,8 +27,11 @@ SCRIPTS = {
 
 
 def main():
+    ref = os.environ.get("SAC_REFERENCE")
+    if not ref or not os.path.isdir(os.path.join(ref, "inipar")):
+        raise SystemExit("set SAC_REFERENCE to the root of the SAC tree (the directory holding inipar/)")
     for script, out in SCRIPTS.items():
-        src = os.path.join(REF, "inipar", script)
+        src = os.path.join(ref, "inipar", script)
         with tempfile.TemporaryDirectory() as tmp:
             os.makedirs(os.path.join(tmp, "data"))
             cwd = os.getcwd()

@@ -126,3 +126,40 @@ def test_b_rows_split_mn_major():
     Bm = b.permute(0, 2, 1).reshape(G * S, K)
     ref = _ref(a, Bm).T.reshape(G, S, M)
     _close(c, ref, _scale(a, Bm).T.reshape(G, S, M))
+
+
+def test_wait_time_out_sets_the_error_word_and_returns():
+    """wait_tries = -1: the first pipeline wait gives up at once.  The kernel
+    raises bit 0 of the error word, drains the MMAs it issued, releases its TMEM
+    and returns; the next call with the default bound computes normally."""
+    M, N, K = 256, 64, 512  # 8 k tiles: the wait for a free stage comes at k tile 2
+    a, b = _bf((M, K), 11), _bf((N, K), 12)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    c = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), c.data_ptr(), err=err.data_ptr(), wait_tries=-1)
+    torch.cuda.synchronize()
+    assert int(err.item()) & 1
+    err.zero_()
+    fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), c.data_ptr(), err=err.data_ptr())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    _close(c, _ref(a, b), _scale(a, b))
+
+
+def test_network_reports_the_time_out():
+    """The network's GEMMs with the test bound: sac_fno_check returns 7 (a
+    tensor-core wait timed out) and the network still runs once the default
+    bound is back."""
+    net = fno_abi.Net(S=64, F=64, width=32, layers=2, hidden=32, cin=16, cout=6, max_batch=2, seed=1)
+    x = torch.randn(2, 16, 64, 64).to(torch.bfloat16).cuda()
+    y = torch.zeros(2, 6, 64, 64, dtype=torch.float32, device="cuda")
+    net.set_wait_tries(-1)
+    net.infer(x.data_ptr(), y.data_ptr(), 2)
+    with pytest.raises(fno_abi.FnoError) as e:
+        net.check(reset=True)
+    assert "status 7" in str(e.value)
+    net.set_wait_tries(0)
+    net.infer(x.data_ptr(), y.data_ptr(), 2)
+    net.check(reset=True)
+    assert torch.isfinite(y).all()
+    net.close()
