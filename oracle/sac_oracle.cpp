@@ -961,6 +961,31 @@ void keeppositive(Oracle& o, Arr& w) {
     });
 }
 
+// primitive and conserve over the whole grid, src/vacphys0.t.mhd:5-52: p into the
+// e slot (getpthermal) and v = m/(rho'+rhob) into the m slots; then back, e from
+// p, v and b (e = p/(gamma-1) + (rho'+rhob) v^2/2 + b^2/2 + b.bg) and m = (rho'+rhob) v
+void primitive(Oracle& o, Arr& w) {
+  Arr p(o.ncell);
+  getpthermal(o, w, o.ixG, p);
+  forR(o, o.ixG, [&](long c) {
+    o.V(w, o.e_)[c] = p[c];
+    for (int C = 1; C <= o.ndir; ++C)
+      o.V(w, o.m0_ + C)[c] = o.V(w, o.m0_ + C)[c] / (o.V(w, o.rho_)[c] + o.V(w, o.rhob_)[c]);
+  });
+}
+void conserve(Oracle& o, Arr& w) {
+  const double g = o.par.gamma;
+  forR(o, o.ixG, [&](long c) {
+    const double rt = o.V(w, o.rho_)[c] + o.V(w, o.rhob_)[c];
+    double v2 = 0, b2 = 0, bb = 0;
+    for (int C = 1; C <= o.ndir; ++C) v2 += o.V(w, o.m0_ + C)[c] * o.V(w, o.m0_ + C)[c];
+    for (int C = 1; C <= o.ndir; ++C) b2 += o.V(w, o.b0_ + C)[c] * o.V(w, o.b0_ + C)[c];
+    for (int C = 1; C <= o.ndir; ++C) bb += o.V(w, o.b0_ + C)[c] * o.V(w, o.bg0_ + C)[c];
+    o.V(w, o.e_)[c] = o.V(w, o.e_)[c] / (g - 1.0) + 0.5 * (rt * v2 + b2) + bb;
+    for (int C = 1; C <= o.ndir; ++C) o.V(w, o.m0_ + C)[c] = rt * o.V(w, o.m0_ + C)[c];
+  });
+}
+
 // ---------------------------------------------------------------------------
 // boundaries, src/vacgrid.t:9-512
 // ---------------------------------------------------------------------------
@@ -1028,6 +1053,13 @@ void getboundary(Oracle& o, Arr& w) {
         int se = up ? r.lo[d] - 2 : r.hi[d] + 3, see = up ? r.lo[d] - 3 : r.hi[d] + 2;
         forR(o, plane(q1), [&](long c) { a[c] = a[c + (long)(se - q1) * s]; });
         forR(o, plane(q2), [&](long c) { a[c] = a[c + (long)(see - q2) * s]; });
+      } else if (t == "zero") {  // src/vacgrid.t:295-346: contCD4's copy in primitive variables
+        primitive(o, w);
+        int q1 = r.lo[d], q2 = r.hi[d];
+        int se = up ? r.lo[d] - 2 : r.hi[d] + 3, see = up ? r.lo[d] - 3 : r.hi[d] + 2;
+        forR(o, plane(q1), [&](long c) { a[c] = a[c + (long)(se - q1) * s]; });
+        forR(o, plane(q2), [&](long c) { a[c] = a[c + (long)(see - q2) * s]; });
+        conserve(o, w);
       }
     }
   }
@@ -1425,7 +1457,7 @@ int oracle_set_boundaries(oracle_ctx* cx, int nB, const char* typeB, const int* 
     for (int iw = 0; iw < o.nw; ++iw) {
       const std::string& t = o.typeB[iw + (long)o.nw * iB];
       if (!(t == "cont" || t == "fixed" || t == "cont1" || t == "fixed1" || t == "grad1" || t == "periodic" ||
-            t == "symm" || t == "symm0" || t == "asymm" || t == "contCD4")) {
+            t == "symm" || t == "symm0" || t == "asymm" || t == "contCD4" || t == "zero")) {
         o.err = "boundary type '" + t + "' is not implemented";
         return SAC_ERR_UNSUPPORTED;
       }

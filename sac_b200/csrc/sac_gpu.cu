@@ -171,6 +171,7 @@ int8_t btype(const std::string& t, bool* ok) {
   if (t == "symm0") return BT_SYMM0;
   if (t == "asymm") return BT_ASYMM;
   if (t == "contCD4") return BT_CONTCD4;
+  if (t == "zero") return BT_ZERO;
   *ok = false;
   return BT_CONT;
 }
@@ -247,11 +248,51 @@ template <typename S>
 void launch_bound(sac_ctx* c, const BcArgs& b, int nvar) {
   const Geom& g = c->g;
   if (c->regions) {  // user regions: one pass per region, in the reference's order
+    // every variable, background included: a 'zero' variable of any kind converts
+    // the whole grid to primitive variables and back around its copy
+    const int nv = g.nw;
+    auto zero_pass = [&](auto ND) {
+      constexpr int NDIR = decltype(ND)::value;
+      const unsigned nb = (unsigned)std::min<long>((g.ncell + 255) / 256, 148L * 16);
+      Prof pr(c, SAC_K_BOUND);
+      k_primitive<NDIR, S><<<nb, 256, 0, c->stream>>>(g, (S*)b.A, c->BG, c->par.gamma);
+      return nb;
+    };
+    auto conserve_pass = [&](auto ND, unsigned nb) {
+      constexpr int NDIR = decltype(ND)::value;
+      Prof pr(c, SAC_K_BOUND);
+      k_conserve<NDIR, S><<<nb, 256, 0, c->stream>>>(g, (S*)b.A, c->BG, c->par.gamma);
+    };
     for (int iB = 0; iB < c->nB; ++iB) {
       const RegionArgs a = region_args(c, b.A, iB);
-      Prof pr(c, SAC_K_BOUND);
-      k_bound_region<S><<<(unsigned)((a.cells + 255) / 256), 256, 0, c->stream>>>(a, nvar);
+      const unsigned rb = (unsigned)((a.cells + 255) / 256);
+      int iw = 0;
+      while (iw < nv) {
+        int z = iw;  // the next 'zero' variable of this region
+        while (z < nv && c->h_type[z * c->nB + iB] != BT_ZERO) ++z;
+        if (z > iw) {
+          Prof pr(c, SAC_K_BOUND);
+          k_bound_region<S><<<rb, 256, 0, c->stream>>>(a, iw, z);
+        }
+        if (z >= nv) break;
+        auto around = [&](auto ND) {
+          const unsigned nb = zero_pass(ND);
+          {
+            Prof pr(c, SAC_K_BOUND);
+            k_bound_region<S><<<rb, 256, 0, c->stream>>>(a, z, z + 1);
+          }
+          conserve_pass(ND, nb);
+        };
+        if (g.ndir == 1)
+          around(std::integral_constant<int, 1>{});
+        else if (g.ndir == 2)
+          around(std::integral_constant<int, 2>{});
+        else
+          around(std::integral_constant<int, 3>{});
+        iw = z + 1;
+      }
     }
+    (void)nvar;
     return;
   }
   long ns[3];
@@ -985,13 +1026,18 @@ sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* 
       c->zero1[d][s] = (t1 != "periodic" && t1 != "mpi") ? 1 : 0;
     }
   }
+  // 'zero' converts the whole grid around its copy, which the one-pass resolver
+  // cannot express: it takes the region-by-region fill
+  bool any_zero = false;
+  for (int8_t ty : c->h_type) any_zero = any_zero || ty == BT_ZERO;
+  const bool region_mode = !is_default || any_zero;
   // fixB slabs for every region that holds a fixed-type variable: the default
   // regions' slabs are the dixB layers times the full grid across (k_bound), a user
   // region's slab is its own cells
   long off = 0;
   for (int iB = 0; iB < nB; ++iB) {
     long sl;
-    if (is_default) {
+    if (!region_mode) {
       const int d = iB / 2;
       sl = 2;  // dixB layers
       for (int e = 0; e < g.ndim; ++e)
@@ -1012,7 +1058,7 @@ sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* 
   }
   c->nB = nB;
   c->reg = reg;
-  c->regions = !is_default;
+  c->regions = region_mode;
   if (c->fixB) cudaFree(c->fixB), c->fixB = nullptr;
   if (c->d_type) cudaFree(c->d_type), c->d_type = nullptr;
   if (c->d_fixed) cudaFree(c->d_fixed), c->d_fixed = nullptr;

@@ -13,7 +13,7 @@ constexpr int kMaxDim = 3;
 // Boundary codes (typeB strings of src/vacgrid.t:257-470)
 enum BType : int8_t {
   BT_CONT = 0, BT_FIXED, BT_CONT1, BT_FIXED1, BT_GRAD1, BT_PERIODIC, BT_SYMM, BT_SYMM0, BT_ASYMM,
-  BT_CONTCD4
+  BT_CONTCD4, BT_ZERO
 };
 
 // Driver codes
@@ -482,7 +482,7 @@ __device__ __forceinline__ void region_cell(const RegionArgs& a, long t, int p[3
 }
 
 template <typename S>
-__global__ void __launch_bounds__(256) k_bound_region(const __grid_constant__ RegionArgs a, int nvar) {
+__global__ void __launch_bounds__(256) k_bound_region(const __grid_constant__ RegionArgs a, int iw0, int nvar) {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t >= a.cells) return;
   const Geom& g = a.g;
@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(256) k_bound_region(const __grid_constant__ Re
     return iw < g.np ? (double)((const S*)a.A)[(long)iw * N + cc] : a.bgA[(long)(iw - g.np) * N + cc];
   };
   const int ixe = a.up ? a.lo[a.d] - 1 : a.hi[a.d] + 1;  // the edge the region copies from
-  for (int iw = 0; iw < nvar; ++iw) {
+  for (int iw = iw0; iw < nvar; ++iw) {
     const int ty = a.type[iw * a.nB + a.iB];
     const bool isfixed = a.fixed[iw * a.nB + a.iB] != 0;
     double v;
@@ -521,6 +521,7 @@ __global__ void __launch_bounds__(256) k_bound_region(const __grid_constant__ Re
         if (ty == BT_ASYMM) v = -v;
         break;
       }
+      case BT_ZERO:     // :295-346: contCD4's copy, on the primitive variables (k_primitive before)
       case BT_CONTCD4: {  // :261-293: the plane ixmin, then the plane ixmax
         const int se = a.up ? a.lo[a.d] - 2 : a.hi[a.d] + 3, see = a.up ? a.lo[a.d] - 3 : a.hi[a.d] + 2;
         if (pd == a.hi[a.d])
@@ -551,6 +552,64 @@ __global__ void __launch_bounds__(256) k_bound_region(const __grid_constant__ Re
       ((S*)a.A)[(long)iw * N + c] = (S)v;
     else
       a.bgA[(long)(iw - g.np) * N + c] = v;
+  }
+}
+
+// primitive and conserve over the whole grid (src/vacphys0.t.mhd:5-52), around the
+// copy of a 'zero' variable: p = getpthermal into the e slot and v = m/(rho'+rhob)
+// into the m slots; then e = p/(gamma-1) + ((rho'+rhob) v^2 + b^2)/2 + b.bg and
+// m = (rho'+rhob) v, in the reference's order of operations
+template <int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_primitive(const __grid_constant__ Geom g, S* __restrict__ A,
+                                                   const double* __restrict__ bg, double gamma) {
+  const long N = g.ncell;
+  constexpr int E = NDIR + 1;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < N; c += (long)gridDim.x * blockDim.x) {
+    const double rho = (double)A[c], rhob = bg[N + c];
+    double m2 = 0.0, b2 = 0.0, bb = 0.0, m[NDIR];
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) {
+      m[C] = (double)A[(1 + C) * N + c];
+      m2 = m2 + m[C] * m[C];
+    }
+    double q = 0.5 * m2 / (rho + rhob);
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) {
+      const double b = (double)A[(E + 1 + C) * N + c];
+      b2 = b2 + b * b;
+    }
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) bb = bb + (double)A[(E + 1 + C) * N + c] * bg[(2 + C) * N + c];
+    q = q + 0.5 * b2 + bb;
+    A[E * N + c] = (S)((gamma - 1.0) * ((double)A[E * N + c] - q));
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) A[(1 + C) * N + c] = (S)(m[C] / (rho + rhob));
+  }
+}
+
+template <int NDIR, typename S>
+__global__ void __launch_bounds__(256) k_conserve(const __grid_constant__ Geom g, S* __restrict__ A,
+                                                  const double* __restrict__ bg, double gamma) {
+  const long N = g.ncell;
+  constexpr int E = NDIR + 1;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < N; c += (long)gridDim.x * blockDim.x) {
+    const double rt = (double)A[c] + bg[N + c];
+    double v2 = 0.0, b2 = 0.0, bb = 0.0, v[NDIR];
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) {
+      v[C] = (double)A[(1 + C) * N + c];
+      v2 = v2 + v[C] * v[C];
+    }
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) {
+      const double b = (double)A[(E + 1 + C) * N + c];
+      b2 = b2 + b * b;
+    }
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) bb = bb + (double)A[(E + 1 + C) * N + c] * bg[(2 + C) * N + c];
+    A[E * N + c] = (S)((double)A[E * N + c] / (gamma - 1.0) + 0.5 * (rt * v2 + b2) + bb);
+#pragma unroll
+    for (int C = 0; C < NDIR; ++C) A[(1 + C) * N + c] = (S)(rt * v[C]);
   }
 }
 

@@ -194,13 +194,29 @@ def test_resistive_source_method():
     _compare(P, o, g)
 
 
-@pytest.mark.parametrize("kind", ["zero", "special"])
-def test_unbuilt_boundary_types_are_errors(kind):
-    P = problems.random_problem((12, 10), seed=48, types=[kind, "cont", "periodic", "periodic"])
+def test_special_boundary_is_an_error():
+    """'special' calls the user's specialbound, which the reference's user files
+    define as die('not defined') (src/vacusr.f:1387-1399): an error here too."""
+    P = problems.random_problem((12, 10), seed=48, types=["special", "cont", "periodic", "periodic"])
     g = abi.Context(P.params)
     g.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
     with pytest.raises(abi.SacError):
         g.set_boundaries(P.typeB_packed, P.nB)
+
+
+@pytest.mark.parametrize("where", ["lower", "upper", "both"])
+def test_zero_boundary(where):
+    """'zero' (src/vacgrid.t:295-346): the whole grid to primitive variables, the
+    contCD4 copy, and back to conservative ones, once per variable that has it, so
+    every fill re-rounds e and m everywhere; both paths do it in the same order."""
+    types = {"lower": ["zero", "cont"], "upper": ["cont1", "zero"], "both": ["zero", "zero"]}[where]
+    P = problems.random_problem((14, 12), seed=49, types=types + ["periodic", "periodic"])
+    o, g = _pair(P)
+    np.testing.assert_array_equal(g.download(), o.download())
+    d_o = _util.run(o, 10)
+    d_g = _util.run(g, 10)
+    np.testing.assert_allclose(d_g, d_o, rtol=RTOL, atol=0)
+    _compare(P, o, g)
 
 
 def test_negative_eta_is_an_error():

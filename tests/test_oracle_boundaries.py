@@ -247,3 +247,79 @@ def test_explicit_default_regions_are_the_default_fill():
     _util.run(a, 2)
     _util.run(o, 2)
     np.testing.assert_array_equal(o.download(), a.download())
+
+
+def _primitive(w, ndir, gamma):
+    """src/vacphys0.t.mhd:31-52 on the whole grid: p (getpthermal) into e, v = m/rho_t into m."""
+    w = w.copy()
+    rho, rhob = w[..., 0], w[..., 3 * ndir + 4 - ndir - 1]
+    rt = rho + rhob
+    m = [w[..., 1 + C].copy() for C in range(ndir)]
+    b = [w[..., ndir + 2 + C] for C in range(ndir)]
+    bg = [w[..., 2 * ndir + 4 + C] for C in range(ndir)]
+    m2 = sum_ordered([mc * mc for mc in m])
+    q = 0.5 * m2 / rt
+    q = q + 0.5 * sum_ordered([bc * bc for bc in b]) + sum_ordered([bc * gc for bc, gc in zip(b, bg)])
+    w[..., ndir + 1] = (gamma - 1.0) * (w[..., ndir + 1] - q)
+    for C in range(ndir):
+        w[..., 1 + C] = m[C] / rt
+    return w
+
+
+def _conserve(w, ndir, gamma):
+    """src/vacphys0.t.mhd:5-28: e from p, v and b; m = rho_t v."""
+    w = w.copy()
+    rt = w[..., 0] + w[..., 3 * ndir + 4 - ndir - 1]
+    v = [w[..., 1 + C].copy() for C in range(ndir)]
+    b = [w[..., ndir + 2 + C] for C in range(ndir)]
+    bg = [w[..., 2 * ndir + 4 + C] for C in range(ndir)]
+    w[..., ndir + 1] = (w[..., ndir + 1] / (gamma - 1.0) + 0.5 * (rt * sum_ordered([x * x for x in v])
+                                                                  + sum_ordered([x * x for x in b]))
+                        + sum_ordered([x * y for x, y in zip(b, bg)]))
+    for C in range(ndir):
+        w[..., 1 + C] = rt * v[C]
+    return w
+
+
+def sum_ordered(terms):
+    s = terms[0].copy()
+    for t in terms[1:]:
+        s = s + t
+    return s
+
+
+def test_zero_boundary_first_fill():
+    """'zero' on the lower x1 boundary of a 2D state (src/vacgrid.t:295-346): per
+    variable in order, primitive over the whole grid, contCD4's copy of that
+    variable, conserve; then the other regions."""
+    P = problems.random_problem((10, 8), seed=33, types=["zero", "cont", "periodic", "periodic"])
+    nd, ndir = P.ndim, P.ndir
+    nw = 3 * ndir + 4
+    gamma = P.params.gamma
+    o = _util.start(Oracle, P)
+    w = P.w.copy()
+    lo = 2
+    for iw in range(nw):
+        w = _primitive(w, ndir, gamma)
+        # the lower region is x1 = 0..1 (0-based): its plane ixmin copies ixmax+3,
+        # its plane ixmax copies ixmax+2
+        w[0, :, iw] = w[lo + 2, :, iw]
+        w[1, :, iw] = w[lo + 1, :, iw]
+        w = _conserve(w, ndir, gamma)
+    ref = _fill_regions_default_rest(P, w)
+    np.testing.assert_array_equal(o.download(), ref)
+
+
+def _fill_regions_default_rest(P, w):
+    """Regions 2..4 of the default set after a 'zero' region 1 (cont upper x1,
+    periodic x2)."""
+    w = w.copy()
+    lo, hi = 2, 2 + P.nx[0] - 1
+    for i in (hi + 1, hi + 2):
+        w[i] = w[hi]
+    n2 = P.nx[1]
+    w[:, 0] = w[:, n2]
+    w[:, 1] = w[:, n2 + 1]
+    w[:, n2 + 2] = w[:, 2]
+    w[:, n2 + 3] = w[:, 3]
+    return w
