@@ -1,20 +1,24 @@
 #!/usr/bin/env python
 """Benchmark of the perturbation-MHD hot path on B200.
 
-Workload: the 3D gravitationally stratified atmosphere, 128x128x128 mesh cells,
-FP64, RK4 (typeadvance='fourstep'), hyperdiffusion, gravity, bottom velocity
-driver, fixed/open x1 boundaries and periodic x2/x3 (sac_b200.problems.stratified).
-One step = one time step of the reference's main loop: getdt + advect (four RK
-stages with their boundary fills) on the resident state.  Metric: cell-updates
-per second (one mesh cell advanced by one full RK4 step).
+Headline workload: the 3D gravitationally stratified atmosphere at 512x512x512
+mesh cells (the precision-comparison configuration), FP64, RK4
+(typeadvance='fourstep'), hyperdiffusion, gravity, bottom velocity driver,
+fixed/open x1 boundaries and periodic x2/x3 (sac_b200.problems.stratified).  The
+same workload at 128^3 (the stratified-atmosphere configuration) is measured
+beside it.  One step = one time step of the reference's main loop: getdt + advect
+(four RK stages with their boundary fills) on the resident state.  Metric:
+cell-updates per second (one mesh cell advanced by one full RK4 step), for the
+FP64 path and the FP32-perturbation path.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 512]
 
 For N>1 the script runs under torch.distributed.run, one process per GPU, each
 advancing its own replica (the path does not shard); timing is the max over
 ranks, value is the whole-job rate.  `--impl reference` times the CPU
-restatement of the reference (oracle/, C++, all host threads) on the same
-workload; rank 0 alone runs it.
+restatement of the reference (oracle/, C++, all host threads) on a bounded
+sample of the same workload: the full 128^3 cube (a whole step of the 512^3
+grid takes minutes on the host); rank 0 alone runs it.
 """
 from __future__ import annotations
 
@@ -39,7 +43,7 @@ METRIC = "3D MHD cell-updates/s"
 UNIT = "cell-updates/s"
 BYTES_PER_CELL_UPDATE = {"fp64": 1056, "fp32": 608}  # 14*n_p*s_p + 4*n_b*s_b, n_p=8, n_b=5
 STAGES_PER_STEP = 4
-REF_SAMPLE = (128, 128, 32)  # bounded CPU sample: one RK4 step on an x3 slab of the workload
+CPU_SAMPLE_N = 128  # the CPU legs time whole RK4 steps of the stratified workload on this cube
 
 
 def workload(n=128, precision="fp64"):
@@ -121,34 +125,58 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # the CPU legs (oracle = C++ restatement of the reference)
 # ---------------------------------------------------------------------------
-def cpu_sample(seconds=12.0, max_steps=64):
-    """Cell-updates/s of the oracle on the host cores: one untimed RK4 step, then
-    timed steps until `seconds` elapse, on a REF_SAMPLE slab of the workload."""
+def cpu_steps(n=CPU_SAMPLE_N, threads=None, seconds=12.0, max_steps=64, min_steps=1, warmup=1):
+    """Cell-updates/s of the oracle on the host cores: `warmup` untimed RK4 steps
+    (getdt + advect), then timed steps until `seconds` elapse (at least
+    min_steps), on the n^3 stratified cube.  Both CPU legs use this."""
     from oracle import oracle
 
-    P = problems.stratified(n=REF_SAMPLE)
+    oracle.build()
+    if threads is not None:
+        oracle.set_threads(threads)
+    P = problems.stratified(n=(n, n, n))
     o = oracle.Oracle(P.params)
     o.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
     o.set_boundaries(P.typeB_packed, P.nB)
     o.upload(P.w)
     o.getboundary(0.0)
     t, it = 0.0, 0
-    dt = o.getdt(it)
-    o.advect(dt, t, it)
-    t += dt
-    it += 1
-    n, t0 = 0, time.perf_counter()
-    while n < max_steps:
+    for _ in range(warmup):
         dt = o.getdt(it)
         o.advect(dt, t, it)
         t += dt
         it += 1
-        n += 1
-        if time.perf_counter() - t0 > seconds:
+    k, t0 = 0, time.perf_counter()
+    while k < max_steps:
+        dt = o.getdt(it)
+        o.advect(dt, t, it)
+        t += dt
+        it += 1
+        k += 1
+        el = time.perf_counter() - t0
+        if k >= min_steps and el > seconds:
             break
     el = time.perf_counter() - t0
     o.close()
-    return P.ncells * n / el, n, el, oracle.max_threads()
+    used = threads if threads is not None else oracle.max_threads()
+    if threads is not None:
+        oracle.set_threads(oracle.max_threads())
+    return {"value": P.ncells * k / el, "steps": k, "seconds": el, "threads": used, "cells": P.ncells, "n": n}
+
+
+def cpu_sample_text(r):
+    return (f"{r['steps']} RK4 steps (getdt+advect) in {r['seconds']:.1f} s on the full {r['n']}^3 stratified "
+            f"cube, C++ FP64 restatement of the reference (the Fortran reference cannot be built: no Fortran "
+            f"compiler), {r['threads']} OpenMP thread(s); a whole RK4 step of the 512^3 grid would take minutes on "
+            f"the host, so the cube is the bounded sample of the workload, per cell")
+
+
+def headline_config(n, world):
+    return {"workload": f"stratified atmosphere {n}^3, FP64 and FP32-perturbation paths, RK4, hyperdiffusion, "
+                        f"gravity, driver",
+            "cells_per_step": n ** 3, "parallelism": f"replicas{world}",
+            "l2": f"no flush: resident state ~{n ** 3 * 13 * 8 * 1.2 / 1e9:.0f} GB per replica, larger than L2",
+            "step": "getdt + advect (4 RK stages + boundary fills)"}
 
 
 def reference_arm(args, rank, world):
@@ -157,37 +185,14 @@ def reference_arm(args, rank, world):
     from oracle import oracle
 
     oracle.build()
-    P = problems.stratified(n=REF_SAMPLE)
-    o = oracle.Oracle(P.params)
-    o.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
-    o.set_boundaries(P.typeB_packed, P.nB)
-    o.upload(P.w)
-    o.getboundary(0.0)
-    t, it = 0.0, 0
-    for _ in range(args.warmup):
-        dt = o.getdt(it)
-        o.advect(dt, t, it)
-        t += dt
-        it += 1
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        dt = o.getdt(it)
-        o.advect(dt, t, it)
-        t += dt
-        it += 1
-    el = time.perf_counter() - t0
-    v = P.ncells * args.steps / el
-    cores = oracle.max_threads()
-    sample = (f"one RK4 step (getdt+advect) per step on a {REF_SAMPLE[0]}x{REF_SAMPLE[1]}x{REF_SAMPLE[2]} "
-              f"x3-slab of the 128^3 stratified workload, C++ FP64 restatement of the reference "
-              f"(the Fortran reference cannot be built: no Fortran compiler), OpenMP {cores} threads")
+    r = cpu_steps(warmup=args.warmup, seconds=0.0, min_steps=args.steps, max_steps=args.steps)
+    v = r["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "stratified atmosphere 128^3, FP64, RK4, hyperdiffusion, gravity, driver",
-                   "cells_per_step": P.ncells, "parallelism": "cpu"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": headline_config(args.n, world),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["threads"], "kind": "port", "sample": cpu_sample_text(r)},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -307,30 +312,27 @@ def roofline(b_cell_update, cells, kern, peak, peak_kind, tr_name, label):
             "kernel": label, "bytes_per_launch": b_launch, "avg_launch_ms": upd_ms / upd_n if upd_n else None}
 
 
-def ours(args, rank, world, local_rank):
+def measure(args, n, local_rank, world, legs, clocks=True):
+    """The FP64 and FP32 legs (and e2e) of the stratified workload at n^3: each a
+    context of its own on the rank's GPU, created, timed and released in turn."""
     import torch
     import torch.distributed as dist
 
-    from sac_b200 import build as sbuild
-
-    sbuild.build()
-    torch.cuda.set_device(local_rank)
-    legs = set(args.legs.split(","))
-    P = workload(args.n)
+    P = workload(n)
     cells = P.ncells
     nbytes = P.nw * int(np.prod(P.ixGhi)) * 8
-    r64 = r32 = None
-    value = e2e = v32 = None
+    out = {"cells": cells, "nbytes": nbytes}
     if legs & {"fp64", "e2e"}:
         ctx, lib = make_ctx(P, local_rank, "fp64")
-        r64 = timed_steps(args, P, ctx, lib, local_rank, world)
-        value = job_rate(cells, args.steps, world, r64["ms"] / 1e3)
+        r64 = timed_steps(args, P, ctx, lib, local_rank, world, clocks=clocks)
+        out["r64"] = r64
+        out["v64"] = job_rate(cells, args.steps, world, r64["ms"] / 1e3)
         if "e2e" in legs:
             # end to end through the C-ABI with host buffers: per step upload(w),
             # getdt, advect, download(w) from/to pinned host memory
             pin = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
             hw = pin.numpy().reshape(P.ixGhi + (P.nw,), order="F")
-            hw[...] = ctx.download()
+            ctx.download(hw)
             t, it = r64["t"], r64["it"]
             e2e_steps = max(3, min(args.steps, 10))
             if world > 1:
@@ -345,52 +347,86 @@ def ours(args, rank, world, local_rank):
                 it += 1
                 ctx.download(hw)
             e2e_s = max_over_ranks(time.perf_counter() - t0, world, device=f"cuda:{local_rank}")
-            e2e = job_rate(cells, e2e_steps, world, e2e_s)
+            out["e2e"] = job_rate(cells, e2e_steps, world, e2e_s)
+            del hw, pin
         ctx.close()
-
+        torch.cuda.empty_cache()
     if "fp32" in legs:
         # the FP32-perturbation path on the same workload
-        P32 = workload(args.n)
-        ctx32, lib32 = make_ctx(P32, local_rank, "fp32")
-        r32 = timed_steps(args, P32, ctx32, lib32, local_rank, world, clocks=r64 is None)
+        ctx32, lib32 = make_ctx(P, local_rank, "fp32")
+        r32 = timed_steps(args, P, ctx32, lib32, local_rank, world, clocks=clocks and "r64" not in out)
         ctx32.close()
-        v32 = job_rate(cells, args.steps, world, r32["ms"] / 1e3)
+        torch.cuda.empty_cache()
+        out["r32"] = r32
+        out["v32"] = job_rate(cells, args.steps, world, r32["ms"] / 1e3)
+    return out
 
+
+def leg_summary(m, args, peak, peak_kind):
+    """Per-path numbers of one workload size for the JSON line."""
+    cells = m["cells"]
+    d = {"cells_per_step": cells}
+    if "r64" in m:
+        r = m["r64"]
+        d["fp64"] = {"value": m["v64"], "ms_per_step": r["ms"] / args.steps, "gpu_launches": r["launches"],
+                     "kernels_ms_per_step": {k: v[0] / args.steps for k, v in r["kern"].items()},
+                     "roofline": roofline(BYTES_PER_CELL_UPDATE["fp64"], cells, r["kern"], peak, peak_kind,
+                                          "update_fp64_traffic.json", "k_update<3,3,double>")}
+    if "r32" in m:
+        r = m["r32"]
+        d["fp32"] = {"value": m["v32"], "ms_per_step": r["ms"] / args.steps, "gpu_launches": r["launches"],
+                     "speedup_vs_fp64": (m["v32"] / m["v64"]) if "v64" in m else None,
+                     "kernels_ms_per_step": {k: v[0] / args.steps for k, v in r["kern"].items()},
+                     "roofline": roofline(BYTES_PER_CELL_UPDATE["fp32"], cells, r["kern"], peak, peak_kind,
+                                          "update_fp32_traffic.json", "k_update<3,3,float>")}
+    return d
+
+
+def ours(args, rank, world, local_rank):
+    import torch
+
+    from sac_b200 import build as sbuild
+
+    sbuild.build()
+    torch.cuda.set_device(local_rank)
+    legs = set(args.legs.split(","))
+    main = measure(args, args.n, local_rank, world, legs)
+    small = None
+    if args.n != 128 and "small" in legs:
+        small = measure(args, 128, local_rank, world, legs & {"fp64", "fp32"}, clocks=False)
     if rank != 0:
         return 0
     peak, peak_kind = load_peaks()
-    lead = r64 or r32
+    summ = leg_summary(main, args, peak, peak_kind)
+    lead = main.get("r64") or main.get("r32")
+    value = main.get("v64", main.get("v32"))
     line = {
-        "metric": METRIC, "value": value if value is not None else v32, "unit": UNIT, "n_gpus": world,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": lead["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if r64 else "f32", "data": "synthetic",
-        "config": {"workload": f"stratified atmosphere {args.n}^3, FP64, RK4, hyperdiffusion, gravity, driver",
-                   "cells_per_step": cells, "parallelism": f"replicas{world}",
-                   "l2": "no flush: resident state ~1.6 GB per replica at 128^3, larger than L2",
-                   "step": "getdt + advect (4 RK stages + boundary fills)"},
+        "vs_baseline": None, "dtype": "f64" if "r64" in main else "f32", "data": "synthetic",
+        "config": headline_config(args.n, world),
         "gpu_launches": lead["launches"],
         "clocks": lead["clocks"],
     }
-    if r64:
-        line["roofline"] = roofline(BYTES_PER_CELL_UPDATE["fp64"], cells, r64["kern"], peak, peak_kind,
-                                    "update_fp64_traffic.json", "k_update<3,3,double>")
-        line["kernels_ms_per_step"] = {k: v[0] / args.steps for k, v in r64["kern"].items()}
-    if e2e is not None:
-        line["e2e"] = {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+    if "fp64" in summ:
+        line["roofline"] = summ["fp64"]["roofline"]
+        line["kernels_ms_per_step"] = summ["fp64"]["kernels_ms_per_step"]
+    if "e2e" in main:
+        line["e2e"] = {"value": main["e2e"], "unit": UNIT, "h2d_bytes_per_step": main["nbytes"],
+                       "d2h_bytes_per_step": main["nbytes"],
                        "path": "sac_upload + sac_getdt + sac_advect + sac_download per step, pinned host w"}
-    if r32:
-        line["fp32"] = {"value": v32, "ms_per_step": r32["ms"] / args.steps,
-                        "speedup_vs_fp64": (v32 / value) if value else None,
-                        "gpu_launches": r32["launches"],
-                        "kernels_ms_per_step": {k: v[0] / args.steps for k, v in r32["kern"].items()},
-                        "roofline": roofline(BYTES_PER_CELL_UPDATE["fp32"], cells, r32["kern"], peak, peak_kind,
-                                             "update_fp32_traffic.json", "k_update<3,3,float>")}
+    if "fp32" in summ:
+        line["fp32"] = summ["fp32"]
+    if small is not None:
+        line["stratified_128"] = leg_summary(small, args, peak, peak_kind)
     if world == 1 and not args.no_cpu and "cpu" in legs:
-        v, n, el, cores = cpu_sample()
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                                "sample": f"{n} RK4 steps in {el:.1f} s on a {REF_SAMPLE[0]}x{REF_SAMPLE[1]}x"
-                                          f"{REF_SAMPLE[2]} x3-slab of the workload, C++ oracle, OpenMP"}
+        r = cpu_steps()
+        line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "port",
+                                "sample": cpu_sample_text(r)}
+        r1 = cpu_steps(n=64, threads=1, seconds=8.0, max_steps=8)
+        line["cpu_baseline_1core"] = {"value": r1["value"], "unit": UNIT, "cores": 1, "kind": "port",
+                                      "sample": cpu_sample_text(r1)}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -487,21 +523,41 @@ def batch_cpu_workload(steps=5):
             "steps": steps, "s": el, "cell_updates_per_s": Q.ncells * steps / el, "threads": nthreads}
 
 
+def batch_workload(args):
+    """The batched configuration: 4096 uneven Orszag-Tang vortices (nx, ny from
+    {64, 96, ..., 512}), every instance with its own dt, FP64 and FP32, each a
+    CUDA-graph replay per RK4 step (sac_b200.batch_bench)."""
+    import torch
+
+    from sac_b200 import batch_bench, build, params
+
+    build.build()
+    torch.cuda.init()
+    out = {"workload": "4096 uneven Orszag-Tang vortices, RK4, hyperdiffusion, own dt per instance"}
+    for name, prec in (("fp64", params.PREC_FP64), ("fp32", params.PREC_FP32)):
+        out[name] = batch_bench.run(4096, max(args.steps, 3), max(args.warmup, 1), prec)
+        torch.cuda.empty_cache()
+    out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=128, help="mesh cells per dimension (default 128)")
+    ap.add_argument("--n", type=int, default=512, help="mesh cells per dimension of the headline line (default 512)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--legs", default="fp64,e2e,fp32,cpu",
-                    help="comma list of fp64, e2e, fp32, cpu (profiling runs select one kernel family)")
-    ap.add_argument("--workload", default="stratified", choices=["stratified", "briowu", "batch-cpu"],
-                    help="stratified: the headline line; briowu / batch-cpu: the small configurations' legs")
+    ap.add_argument("--legs", default="fp64,e2e,fp32,small,cpu",
+                    help="comma list of fp64, e2e, fp32, small (the 128^3 legs beside a larger --n), cpu "
+                         "(profiling runs select one kernel family)")
+    ap.add_argument("--workload", default="stratified", choices=["stratified", "briowu", "batch", "batch-cpu"],
+                    help="stratified: the headline line; briowu / batch / batch-cpu: the other configurations' legs")
     args = ap.parse_args()
     if args.workload != "stratified":
-        res = briowu_workload() if args.workload == "briowu" else batch_cpu_workload()
+        res = {"briowu": briowu_workload, "batch-cpu": batch_cpu_workload,
+               "batch": lambda: batch_workload(args)}[args.workload]()
         print(json.dumps(res), flush=True)
         return 0
     rank = int(os.environ.get("RANK", "0"))
