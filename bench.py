@@ -301,6 +301,28 @@ def timed_steps(args, P, ctx, lib, local_rank, world, clocks=True):
     return dict(ms=ms, launches=launches, kern=kern, clocks=clk.summary() if clk else None, t=t, it=it)
 
 
+SM_COUNT, SCHEDULERS_PER_SM = 148, 4
+
+
+def issue_ceiling(path, value, sm_mhz):
+    """The instruction-issue wall of a path: the warp instructions one RK4 step
+    issues per mesh cell (all kernels of the step, ncu instruction counts at 128^3,
+    profiles/stage_instructions_stratified128.json) against the SM issue peak of
+    one warp instruction per scheduler and clock, at the sampled SM clock."""
+    p = os.path.join(ROOT, "profiles", "stage_instructions_stratified128.json")
+    if not os.path.exists(p) or not sm_mhz:
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    if path not in d.get("warp_instr_per_step", {}):
+        return None
+    per_cell = d["warp_instr_per_step"][path] / d["cells"]
+    peak = SM_COUNT * SCHEDULERS_PER_SM * sm_mhz * 1e6
+    ceiling = peak / per_cell
+    return {"warp_instr_per_cell_update": per_cell, "peak_warp_instr_per_s": peak, "unit": "cell-updates/s",
+            "ceiling": ceiling, "frac": value / ceiling}
+
+
 def roofline(b_cell_update, cells, kern, peak, peak_kind, tr_name, label):
     upd_ms, upd_n = kern["update"]
     b_launch = b_cell_update / STAGES_PER_STEP * cells
@@ -409,9 +431,13 @@ def ours(args, rank, world, local_rank):
         "gpu_launches": lead["launches"],
         "clocks": lead["clocks"],
     }
+    sm_mhz = (lead["clocks"] or {}).get("sm_mhz")
     if "fp64" in summ:
         line["roofline"] = summ["fp64"]["roofline"]
+        line["roofline"]["issue"] = issue_ceiling("fp64", summ["fp64"]["value"] / world, sm_mhz)
         line["kernels_ms_per_step"] = summ["fp64"]["kernels_ms_per_step"]
+    if "fp32" in summ:
+        summ["fp32"]["roofline"]["issue"] = issue_ceiling("fp32", summ["fp32"]["value"] / world, sm_mhz)
     if "e2e" in main:
         line["e2e"] = {"value": main["e2e"], "unit": UNIT, "h2d_bytes_per_step": main["nbytes"],
                        "d2h_bytes_per_step": main["nbytes"],
@@ -541,6 +567,43 @@ def batch_workload(args):
     return out
 
 
+def smallfix_workload(args):
+    """keeppositive on the device: the Orszag-Tang vortex at 512^2 with the floors
+    of its initial state (smallp 0.5, smallrho = vacuumrho = 2.75), FP64, RK4 with
+    hyperdiffusion, K steps after W untimed ones (each fill runs keeppositive)."""
+    from sac_b200 import build
+
+    build.build()
+    P = problems.orszag_tang((512, 512))
+    P.params.smallfix = 1
+    P.params.smallp = 0.5
+    P.params.smallrho = 2.75
+    P.params.vacuumrho = 2.75
+    c = abi.Context(P.params)
+    c.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
+    c.set_boundaries(P.typeB_packed, P.nB)
+    c.upload(P.w)
+    c.getboundary(0.0)
+    t, it = 0.0, 0
+    for _ in range(max(args.warmup, 1)):
+        dt = c.getdt(it)
+        c.advect(dt, t, it)
+        t, it = t + dt, it + 1
+    c.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        dt = c.getdt(it)
+        c.advect(dt, t, it)
+        t, it = t + dt, it + 1
+    c.synchronize()
+    el = time.perf_counter() - t0
+    d = c.diag()
+    c.close()
+    return {"workload": "Orszag-Tang 512^2 with keeppositive floors, FP64, RK4, hyperdiffusion",
+            "steps": args.steps, "s": el, "cell_updates_per_s": P.ncells * args.steps / el,
+            "nerror_toosmallp": d.nerror_toosmallp}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -552,12 +615,14 @@ def main():
     ap.add_argument("--legs", default="fp64,e2e,fp32,small,cpu",
                     help="comma list of fp64, e2e, fp32, small (the 128^3 legs beside a larger --n), cpu "
                          "(profiling runs select one kernel family)")
-    ap.add_argument("--workload", default="stratified", choices=["stratified", "briowu", "batch", "batch-cpu"],
-                    help="stratified: the headline line; briowu / batch / batch-cpu: the other configurations' legs")
+    ap.add_argument("--workload", default="stratified",
+                    choices=["stratified", "briowu", "batch", "batch-cpu", "smallfix"],
+                    help="stratified: the headline line; briowu / batch / batch-cpu: the other configurations' legs; "
+                         "smallfix: keeppositive on a 2D vortex (profiling)")
     args = ap.parse_args()
     if args.workload != "stratified":
         res = {"briowu": briowu_workload, "batch-cpu": batch_cpu_workload,
-               "batch": lambda: batch_workload(args)}[args.workload]()
+               "batch": lambda: batch_workload(args), "smallfix": lambda: smallfix_workload(args)}[args.workload]()
         print(json.dumps(res), flush=True)
         return 0
     rank = int(os.environ.get("RANK", "0"))
