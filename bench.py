@@ -175,7 +175,8 @@ def headline_config(n, world):
     return {"workload": f"stratified atmosphere {n}^3, FP64 and FP32-perturbation paths, RK4, hyperdiffusion, "
                         f"gravity, driver",
             "cells_per_step": n ** 3, "parallelism": f"replicas{world}",
-            "l2": f"no flush: resident state ~{n ** 3 * 13 * 8 * 1.2 / 1e9:.0f} GB per replica, larger than L2",
+            "l2": f"no flush: the FP64 context holds ~{(n + 4) ** 3 * 800 / 1e9:.1f} GB per replica (state, RK "
+                  f"arrays and per-stage intermediates), far larger than the 126 MB L2",
             "step": "getdt + advect (4 RK stages + boundary fills)"}
 
 

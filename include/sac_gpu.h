@@ -275,8 +275,20 @@ sac_status sac_batch_state(sac_batch* b, double* t, double* dt, int* it);
 sac_status sac_batch_synchronize(sac_batch* b);
 void* sac_batch_get_stream(const sac_batch* b);
 /* time the update pass for each candidate tile shape on this batch and keep the
- * fastest; tile_xy[2] and ms (per update pass) receive the choice (may be NULL) */
+ * fastest; tile_xy[2] and ms (per update pass) receive the choice (may be NULL);
+ * then time one whole stage in both stage forms (below) and keep the faster */
 sac_status sac_batch_tune(sac_batch* b, int* tile_xy, double* ms);
+/* Stage form.  By default each RK stage is three passes (face, setnu, update)
+ * through device-wide intermediates.  For 2D instances with the default sources
+ * (no Powell or resistive term) it can instead be one fused kernel per tile of
+ * TX x TY mesh cells that computes the fluxes, setnu's quotients and the update
+ * in shared memory (shapes: 0 = 32 x 8, 1 = 16 x 8); the results are the same
+ * bit for bit.  sac_batch_tune times both forms on the batch and keeps the
+ * faster; sac_batch_set_stage chooses one (SAC_ERR_UNSUPPORTED where the fused
+ * form does not apply); sac_batch_get_stage reports the form and the tuner's
+ * times of one stage (ms). */
+sac_status sac_batch_set_stage(sac_batch* b, int fused, int shape);
+sac_status sac_batch_get_stage(const sac_batch* b, int* fused, int* shape, double* ms_three, double* ms_fused);
 /* per-instance driver amplitude and angular frequency of the Gaussian velocity
  * drivers (users SAC_USR_STRAT and SAC_USR_TUBE, tdep = sin(omega t)); the
  * defaults are userpar[0] and userpar[1].  Either array may be NULL. */

@@ -43,6 +43,8 @@ def _bind(lib):
     f("set_driver").argtypes = [P, DP, DP]
     f("set_time").argtypes = [P, DP, IP]
     f("set_tmax").argtypes = [P, DP]
+    f("set_stage").argtypes = [P, ctypes.c_int, ctypes.c_int]
+    f("get_stage").argtypes = [P, IP, IP, DP, DP]
     f("mesh_cells").argtypes = [P]
     f("mesh_cells").restype = ctypes.c_long
     f("gather").argtypes = [P, ctypes.c_void_p, ctypes.c_int]
@@ -53,7 +55,7 @@ def _bind(lib):
     f("destroy").restype = None
     for n in ("create", "set_grid", "set_boundaries", "upload", "download", "upload_range", "download_range",
               "getboundary", "advance", "state", "synchronize", "tune", "set_driver", "set_time", "set_tmax", "gather",
-              "scatter"):
+              "scatter", "set_stage", "get_stage"):
         f(n).restype = ctypes.c_int
     lib._sac_batch_bound = True
     return lib
@@ -189,6 +191,19 @@ class Batch:
         ms = ctypes.c_double(0.0)
         self._call("tune", tile.ctypes.data_as(IP), ctypes.byref(ms))
         return (int(tile[0]), int(tile[1])), ms.value
+
+    def set_stage(self, fused, shape=0):
+        """Each RK stage as the fused per-tile kernel (2D, default sources) in tile
+        shape `shape` (0: 32x8, 1: 16x8), or as the face / setnu / update passes."""
+        self._call("set_stage", int(bool(fused)), int(shape))
+
+    def stage(self):
+        """(fused, shape, ms of one three-pass stage, ms of one fused stage) as the
+        tuner measured them (0 before tune)."""
+        f, sh = ctypes.c_int(0), ctypes.c_int(0)
+        a, b = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self._call("get_stage", ctypes.byref(f), ctypes.byref(sh), ctypes.byref(a), ctypes.byref(b))
+        return bool(f.value), sh.value, a.value, b.value
 
     def close(self):
         if self.h:

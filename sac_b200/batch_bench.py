@@ -21,7 +21,7 @@ from . import batch, params
 
 
 def run(ninst, steps, warmup, precision, seed=0, group_cells=0, tune=True, sizes=batch.OT_SIZES,
-        verbose=False):
+        verbose=False, stage=None):
     import torch
 
     gen = batch.OTBatch(ninst, seed=seed, sizes=sizes)
@@ -32,6 +32,9 @@ def run(ninst, steps, warmup, precision, seed=0, group_cells=0, tune=True, sizes
     setup_s = time.time() - t0
     held = free0 - torch.cuda.mem_get_info()[0]
     tile, tune_ms = b.tune() if tune else ((32, 8), 0.0)
+    if stage is not None:
+        b.set_stage(*stage)
+    fused, shape, ms3, msf = b.stage()
     stream = torch.cuda.ExternalStream(b.stream())
     b.advance(warmup)
     b.synchronize()
@@ -55,6 +58,8 @@ def run(ninst, steps, warmup, precision, seed=0, group_cells=0, tune=True, sizes
         "ms_per_step": ms / steps,
         "tile": list(tile),
         "tune_update_ms": tune_ms,
+        "stage": {"fused": fused, "fused_tile": [[32, 8], [16, 8]][shape], "tune_ms_three_pass": ms3,
+                  "tune_ms_fused": msf},
         "device_bytes": int(held),
         "setup_s": setup_s,
         "t_min": float(t.min()), "t_max": float(t.max()),
@@ -76,12 +81,16 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--group-cells", type=int, default=0)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--stage", choices=["tuned", "three", "fused0", "fused1"], default="tuned",
+                    help="the stage form: the tuner's choice, the three passes, or the fused kernel in tile shape 0/1")
     a = ap.parse_args(argv)
     precs = {"fp64": [params.PREC_FP64], "fp32": [params.PREC_FP32],
              "both": [params.PREC_FP64, params.PREC_FP32]}[a.precision]
     res = []
     for p in precs:
-        r = run(a.ninst, a.steps, a.warmup, p, seed=a.seed, group_cells=a.group_cells, tune=not a.no_tune)
+        stage = {"tuned": None, "three": (False, 0), "fused0": (True, 0), "fused1": (True, 1)}[a.stage]
+        r = run(a.ninst, a.steps, a.warmup, p, seed=a.seed, group_cells=a.group_cells, tune=not a.no_tune,
+                stage=stage)
         print(json.dumps(r), flush=True)
         res.append(r)
     if len(res) == 2:

@@ -73,6 +73,13 @@ struct sac_batch {
   int pairshift[3][2] = {};
   int zero1[3][2] = {};
   dim3 upd_blk = dim3(32, 8, 1);
+  // the stage as one fused kernel per tile (2D, default sources; sac_stage2d.cuh)
+  // instead of the face / setnu / update passes, with its tile shape
+  bool fused = false;
+  int fused_shape = 0;
+  Tile* d_fused = nullptr;
+  int n_fused = 0;
+  double tune_three_ms = 0, tune_fused_ms = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool grid_set = false, bc_set = false, state_set = false, bc_init = false;
@@ -99,6 +106,15 @@ bool visc_on_b(const sac_batch* b) {
   return std::fabs(b->par.nu) > kSmallD;
 }
 bool grav_mod(int u) { return u == SAC_USR_SLOG || u == SAC_USR_GRAVVISC || u == SAC_USR_STRAT || u == SAC_USR_TUBE; }
+
+// the fused stage covers 2D instances with the default sources (gravity,
+// hyperdiffusion, the Gaussian drivers); Powell's and the resistive terms take the
+// three passes
+bool fused_ok(const sac_batch* b) {
+  const bool divb = b->par.sourceunsplit && b->par.divbfix && b->ndim > 1;
+  const bool res = b->par.sourceunsplit && std::fabs(b->par.eta) > kSmallD;
+  return b->ndim == 2 && !divb && !res;
+}
 
 template <typename T>
 sac_status upload_vec(sac_batch* b, T** dptr, const std::vector<T>& v) {
@@ -312,6 +328,38 @@ void enqueue_step(sac_batch* b) {
   const bool visc = visc_on_b(b);
   for (int s = 0; s < 4; ++s) {
     kb_zero<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst, 0);
+    if (b->fused) {
+      // c_tot of the stage input, then face, setnu and update in one kernel per tile
+      BatchStageArgs sa{};
+      sa.a = stage_base(b);
+      sa.a.wct = wct[s];
+      sa.a.base = w;
+      sa.a.out = out[s];
+      sa.a.aux1 = w1;
+      sa.a.aux2 = w2;
+      sa.a.epi = epi[s];
+      sa.inst = b->d_inst;
+      sa.dyn = b->d_dyn;
+      sa.stage = s;
+      sa.tiles = b->d_cour;
+      sa.ntiles = b->n_cour;
+      if (visc) launch_batch_ctot<S>(sa, b->stream);
+      sa.tiles = b->d_fused;
+      sa.ntiles = b->n_fused;
+      launch_batch_stage2d<S>(sa, b->fused_shape, b->stream);
+      BcArgs ba = bc_proto(b, out[s]);
+      if (epi[s] == EPI_RK4_S3) {
+        ba.mode = 1;
+        ba.aux1 = w1;
+        ba.aux2 = w2;
+        ba.basep = w;
+      } else if (epi[s] == EPI_RK4_S4) {
+        ba.mode = 2;
+        ba.aux1 = w1;
+      }
+      launch_bound_b<S>(b, ba, b->np, b->d_gh_all, b->n_gh_all, b->d_dyn);
+      continue;
+    }
     for (Group& gr : b->groups) {
       BatchStageArgs sa{};
       sa.a = stage_base(b);
@@ -377,6 +425,12 @@ sac_status build_lists(sac_batch* b) {
   if ((st = upload_vec(b, &b->d_gh_all, gh)) != SAC_OK) return st;
   b->n_cour = (int)cour.size();
   b->n_gh_all = (int)gh.size();
+  if (fused_ok(b)) {
+    const dim3 ft((unsigned)stage2d_shape_tx(b->fused_shape), (unsigned)stage2d_shape_ty(b->fused_shape), 1);
+    std::vector<Tile> fu = make_tiles(b->h_inst, 0, b->ninst, 2, ft);
+    if ((st = upload_vec(b, &b->d_fused, fu)) != SAC_OK) return st;
+    b->n_fused = (int)fu.size();
+  }
   for (Group& gr : b->groups) {
     std::vector<Tile> f = make_tiles(b->h_inst, gr.i0, gr.i1, 0, dim3(32, 8, 1));
     std::vector<Tile> n = make_tiles(b->h_inst, gr.i0, gr.i1, 1, dim3(32, 8, 1));
@@ -404,6 +458,7 @@ void free_all(sac_batch* b) {
     p = nullptr;
   };
   fr(b->BG), fr(b->dx), fr(b->drv), fr(b->stg), fr(b->d_dyn), fr(b->d_inst), fr(b->d_cour), fr(b->d_gh_all), fr(b->d_meshoff);
+  fr(b->d_fused);
   fr(b->D), fr(b->F), fr(b->R), fr(b->d_type), fr(b->d_fixed), fr(b->d_fixB);
   for (Group& gr : b->groups) fr(gr.d_inst), fr(gr.d_face), fr(gr.d_nu), fr(gr.d_upd), fr(gr.d_gh);
 }
@@ -830,14 +885,122 @@ sac_status sac_batch_tune(sac_batch* b, int* tile_out, double* ms_out) {
   // the timing runs wrote w1 (scratch) and the running max nu: restore the table
   BK(cudaMemcpy(b->d_dyn, saved.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice));
   b->upd_blk = bestb;
+  b->fused = false;
   sac_status st = build_lists(b);
   if (st != SAC_OK) return st;
+  // the whole stage: the three passes with the chosen update tile against the
+  // fused kernel in each of its tile shapes (2D, default sources)
+  if (fused_ok(b) && visc_on_b(b)) {
+    BK(cudaMemcpy(b->d_dyn, tmp.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice));
+    BK(cudaEventCreate(&e0));
+    BK(cudaEventCreate(&e1));
+    auto stage_ms = [&](auto&& run) -> double {
+      run();
+      cudaEventRecord(e0, b->stream);
+      for (int r = 0; r < 3; ++r) run();
+      cudaEventRecord(e1, b->stream);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      return ms / 3;
+    };
+    auto proto = [&]() {
+      BatchStageArgs sa{};
+      sa.a = stage_base(b);
+      sa.a.wct = b->P[0];
+      sa.a.base = b->P[0];
+      sa.a.out = b->P[1];
+      sa.a.epi = EPI_PLAIN;
+      sa.dyn = b->d_dyn;
+      sa.stage = 0;
+      return sa;
+    };
+    double three = stage_ms([&]() {
+      for (Group& gr : b->groups) {
+        BatchStageArgs sa = proto();
+        sa.inst = gr.d_inst;
+        sa.tiles = gr.d_face;
+        sa.ntiles = gr.n_face;
+        if (b->prec == SAC_PREC_FP32) launch_batch_face<float>(sa, b->par.gamma, b->stream);
+        else launch_batch_face<double>(sa, b->par.gamma, b->stream);
+        sa.tiles = gr.d_nu;
+        sa.ntiles = gr.n_nu;
+        if (b->prec == SAC_PREC_FP32) launch_batch_nu<float>(sa, b->stream);
+        else launch_batch_nu<double>(sa, b->stream);
+        sa.tiles = gr.d_upd;
+        sa.ntiles = gr.n_upd;
+        if (b->prec == SAC_PREC_FP32) launch_batch_update<float>(sa, b->upd_blk, b->stream);
+        else launch_batch_update<double>(sa, b->upd_blk, b->stream);
+      }
+    });
+    double bestf = 1e300;
+    int bests = 0;
+    for (int sh = 0; sh < kStage2dShapeCount; ++sh) {
+      b->fused_shape = sh;
+      if ((st = build_lists(b)) != SAC_OK) return st;
+      const double ms = stage_ms([&]() {
+        BatchStageArgs sa = proto();
+        sa.inst = b->d_inst;
+        sa.tiles = b->d_cour;
+        sa.ntiles = b->n_cour;
+        if (b->prec == SAC_PREC_FP32) launch_batch_ctot<float>(sa, b->stream);
+        else launch_batch_ctot<double>(sa, b->stream);
+        sa.tiles = b->d_fused;
+        sa.ntiles = b->n_fused;
+        if (b->prec == SAC_PREC_FP32) launch_batch_stage2d<float>(sa, sh, b->stream);
+        else launch_batch_stage2d<double>(sa, sh, b->stream);
+      });
+      if (ms < bestf) {
+        bestf = ms;
+        bests = sh;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    BK(cudaGetLastError());
+    BK(cudaMemcpy(b->d_dyn, saved.data(), sizeof(InstDyn) * b->ninst, cudaMemcpyHostToDevice));
+    b->fused_shape = bests;
+    b->fused = bestf < three;
+    b->tune_three_ms = three;
+    b->tune_fused_ms = bestf;
+    if ((st = build_lists(b)) != SAC_OK) return st;
+  }
   drop_graph(b);
   if (tile_out) {
     tile_out[0] = (int)bestb.x;
     tile_out[1] = (int)bestb.y;
   }
   if (ms_out) *ms_out = best;
+  return SAC_OK;
+}
+
+// stage form: fused != 0 runs each stage as the fused per-tile kernel in tile
+// shape `shape` (2D instances with the default sources only), 0 as the face /
+// setnu / update passes
+sac_status sac_batch_set_stage(sac_batch* b, int fused, int shape) {
+  if (!b) return SAC_ERR_ARG;
+  if (fused && !fused_ok(b))
+    return bfail(b, SAC_ERR_UNSUPPORTED, "the fused stage covers 2D instances without Powell's or the resistive term");
+  if (shape < 0 || shape >= kStage2dShapeCount) return bfail(b, SAC_ERR_ARG, "no such tile shape");
+  BK(cudaSetDevice(b->dev));
+  b->fused = fused != 0;
+  b->fused_shape = shape;
+  if (b->grid_set) {
+    sac_status st = build_lists(b);
+    if (st != SAC_OK) return st;
+  }
+  drop_graph(b);
+  return SAC_OK;
+}
+
+// the stage form in use: fused (0/1), its tile shape, and the tuner's timings of
+// one stage (three passes, fused; 0 before sac_batch_tune)
+sac_status sac_batch_get_stage(const sac_batch* b, int* fused, int* shape, double* ms_three, double* ms_fused) {
+  if (!b) return SAC_ERR_ARG;
+  if (fused) *fused = b->fused ? 1 : 0;
+  if (shape) *shape = b->fused_shape;
+  if (ms_three) *ms_three = b->tune_three_ms;
+  if (ms_fused) *ms_fused = b->tune_fused_ms;
   return SAC_OK;
 }
 

@@ -85,6 +85,27 @@ __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, 
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 
+// Division that skips the divide for a zero numerator, bit-identical to n / d:
+// for a finite nonzero d, n / d is a zero exactly when n is one, with the sign of
+// n times the sign of d, which n * d gives.  The shortcut is taken only where d
+// is finite and nonzero.  An FP64 division whose numerator is zero leaves the
+// fast path of the divide (measured on B200: 3.6x the time of one with a normal
+// numerator); k_face divides the momenta, which are exactly zero over most of a
+// run that starts from rest, by rho'+rhob.  FP32 storage keeps its plain
+// (approximate) division.
+template <typename T>
+__device__ __forceinline__ T dvs(T n, T d) {
+  if constexpr (sizeof(T) == 8) {
+    if (n == T(0) && d != T(0) && fabs(d) <= 1.7976931348623157e308) return n * d;
+  }
+  return n / d;
+}
+__device__ __forceinline__ double dvs_rn(double n, double d) {
+  if (n == 0.0 && d != 0.0 && fabs(d) <= 1.7976931348623157e308) return __dmul_rn(n, d);
+  return __ddiv_rn(n, d);
+}
+__device__ __forceinline__ float dvs_rn(float n, float d) { return __fdiv_rn(n, d); }
+
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* a, double v) {
   // non-negative doubles order like their bit patterns; NaN maps above +Inf
   unsigned long long b = __double_as_longlong(v);

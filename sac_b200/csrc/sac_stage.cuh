@@ -36,18 +36,27 @@ __device__ __forceinline__ float fmaxT(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double fabsT(double a) { return fabs(a); }
 __device__ __forceinline__ float fabsT(float a) { return fabsf(a); }
 
+// a load of a stencil field: from global memory through the read-only path, or
+// from a shared-memory tile
+template <bool TILE, typename S, typename I>
+__device__ __forceinline__ S ldt(const S* p, I i) {
+  if constexpr (TILE) return p[i];
+  else return __ldg(p + i);
+}
+
+
 // ---------------------------------------------------------------------------
 // per-cell bodies (one grid, located by the offsets o)
 // ---------------------------------------------------------------------------
-// k_face body at local cell c; mesh tells whether the getcmax maxima apply there
-template <int NDIM, int NDIR, typename S>
-__device__ __forceinline__ void face_cell(const Stage2Args& a, const Offs& o, int c, bool mesh, double gamma,
-                                          double* cm) {
+// the k_face arithmetic of the cell whose fields are read at c: dout(i, v) takes
+// the derived field i, fout(d, iw, v) the flux of iw along d for the dimensions in
+// the bit mask fdims; mesh tells whether the getcmax maxima apply there
+template <int NDIM, int NDIR, typename S, class DOut, class FOut>
+__device__ __forceinline__ void face_eval(const Stage2Args& a, const Offs& o, long c, bool mesh, double gamma,
+                                          double* cm, unsigned fdims, DOut&& dout, FOut&& fout) {
   constexpr int E = NDIR + 1;
   auto W = [&](int iw) { return (const S*)a.fW[iw] + o.P; };
   auto BG = [&](int i) { return a.fBG[i] + o.B; };
-  auto Dw = [&](int i) { return (S*)a.fD[i] + o.I; };
-  auto Fw = [&](int d, int iw) { return (S*)a.fF[d][iw] + o.I; };
   {
     const double rho = (double)W(0)[c];
     const double eb = BG(0)[c];
@@ -62,7 +71,7 @@ __device__ __forceinline__ void face_cell(const Stage2Args& a, const Offs& o, in
     }
     const double e = (double)W(E)[c];
 #pragma unroll
-    for (int C = 0; C < NDIR; ++C) v[C] = div_rn(m[C], rt);  // getv / tmp_nu for m
+    for (int C = 0; C < NDIR; ++C) v[C] = dvs_rn(m[C], rt);  // getv / tmp_nu for m
     double b2 = 0.0, m2 = 0.0, bb = 0.0;
 #pragma unroll
     for (int C = 0; C < NDIR; ++C) {
@@ -70,15 +79,15 @@ __device__ __forceinline__ void face_cell(const Stage2Args& a, const Offs& o, in
       m2 = add_rn(m2, mul_rn(m[C], m[C]));
       bb = add_rn(bb, mul_rn(b[C], bg[C]));
     }
-    Dw(0)[c] = (S)rt;
+    dout(0, (S)rt);
 #pragma unroll
-    for (int C = 0; C < NDIR; ++C) Dw(1 + C)[c] = (S)v[C];
+    for (int C = 0; C < NDIR; ++C) dout(1 + C, (S)v[C]);
     // tmp_nu for iw=173, src/vacusr.viscosity.t:301
-    Dw(NDIR + 1)[c] = (S)sub_rn(e, mul_rn(0.5, add_rn(b2, div_rn(m2, rt))));
+    dout(NDIR + 1, (S)sub_rn(e, mul_rn(0.5, add_rn(b2, dvs_rn(m2, rt)))));
     // getptotal, src/vacphys0.t.mhd:199-201
     const double pp = (gamma - 2.0) * (bb + 0.5 * b2);
-    const double ptot = (gamma - 1.0) * (e - 0.5 * m2 / rt) - pp;
-    Dw(NDIR + 2)[c] = (S)ptot;
+    const double ptot = (gamma - 1.0) * (e - dvs(0.5 * m2, rt)) - pp;
+    dout(NDIR + 2, (S)ptot);
     // fluxes in the storage precision's arithmetic (FP64 for the FP64 path; FP32
     // for the FP32 path, whose pressure/energy recovery above stays FP64)
     using C_ = S;
@@ -98,8 +107,9 @@ __device__ __forceinline__ void face_cell(const Stage2Args& a, const Offs& o, in
     for (int C = 0; C < NDIR; ++C) s2 = s2 + bC[C] * mC[C];
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
+      if (!((fdims >> d) & 1u)) continue;
       const C_ vd = vC[d], bd = bC[d], bgd = bgC[d], md = mC[d];
-      Fw(d, 0)[c] = (S)(rhobC * md / rtC + vd * rhoC);
+      fout(d, 0, (S)(dvs(rhobC * md, rtC) + vd * rhoC));
 #pragma unroll
       for (int C = 0; C < NDIR; ++C) {
         C_ f;
@@ -107,15 +117,15 @@ __device__ __forceinline__ void face_cell(const Stage2Args& a, const Offs& o, in
           f = (ptC + C_(0)) - (bC[C] * bgd + bd * bgC[C]) - bC[C] * bd;
         else
           f = -(bC[C] * bgd + bd * bgC[C]) - bC[C] * bd;
-        Fw(d, 1 + C)[c] = (S)(f + vd * mC[C]);
+        fout(d, 1 + C, (S)(f + vd * mC[C]));
       }
-      const C_ fe = (md * (ptC + C_(0)) - bd * s1 - bgd * s2) / rtC + ebC * md / rtC - bd * s2 / rtC;
-      Fw(d, E)[c] = (S)(fe + vd * eC);
+      const C_ fe = dvs(md * (ptC + C_(0)) - bd * s1 - bgd * s2, rtC) + dvs(ebC * md, rtC) - dvs(bd * s2, rtC);
+      fout(d, E, (S)(fe + vd * eC));
       // b_d has no flux along d (getflux sets transport=.false., src/vacphys.mhd0.t:204-206), and
       // k_update never reads that slot, so it is not written
 #pragma unroll
       for (int C = 0; C < NDIR; ++C)
-        if (C != d) Fw(d, E + 1 + C)[c] = (S)(-(vC[C] * (bd + bgd)) + vd * bgC[C] + vd * bC[C]);
+        if (C != d) fout(d, E + 1 + C, (S)(-(vC[C] * (bd + bgd)) + vd * bgC[C] + vd * bC[C]));
     }
     if (mesh) {
         // getpthermal, getcsound2, getcmax: src/vacphys0.t.mhd:95-183
@@ -141,8 +151,18 @@ __device__ __forceinline__ void face_cell(const Stage2Args& a, const Offs& o, in
   }
 }
 
+// k_face body at local cell c: the derived fields and every flux into D and F
+template <int NDIM, int NDIR, typename S>
+__device__ __forceinline__ void face_cell(const Stage2Args& a, const Offs& o, int c, bool mesh, double gamma,
+                                          double* cm) {
+  face_eval<NDIM, NDIR, S>(
+      a, o, c, mesh, gamma, cm, (1u << NDIM) - 1u, [&](int i, S v) { ((S*)a.fD[i] + o.I)[c] = v; },
+      [&](int d, int iw, S v) { ((S*)a.fF[d][iw] + o.I)[c] = v; });
+}
+
 // setnu's face quotient from a window of six values of q along one dimension
-template <typename S>
+// (TILE: q is a shared-memory tile)
+template <bool TILE = false, typename S>
 __device__ __forceinline__ S face_quotient(const S* __restrict__ q, int c, int s, int pos, int lo, int hi, S pre) {
   // q(c-2..c+3) along s; the layer beyond the two ghosts is the mirror image
   // about the first/last mesh cell (tmp_nuI, src/vacusr.viscosity.t:378-400)
@@ -152,7 +172,7 @@ __device__ __forceinline__ S face_quotient(const S* __restrict__ q, int c, int s
     int p = pos + o;
     if (p <= lo - 3) p = lo + 3;
     if (p >= hi + 3) p = hi - 3;
-    a[o + 2] = ld(q, c + (p - pos) * s);
+    a[o + 2] = ldt<TILE>(q, c + (p - pos) * s);
   }
   S d1[5], d3[3];
 #pragma unroll
@@ -193,6 +213,19 @@ __device__ __forceinline__ void nu_cell(const Stage2Args& a, const Geom& g, cons
   }
 }
 
+// The fused 2D stage's view of one cell for update_cell: the stencil fields in
+// shared-memory tiles of row stride st1 (each pointer offset so that [c] is the
+// cell), the cell's box index c and its index cg in the instance's global blocks.
+template <typename S>
+struct TileView {
+  const S* W[8];
+  const S* D[6];
+  const S* F[3][8];
+  const S* Q[21];
+  int st1, c;
+  long cg;
+};
+
 // optional source terms of the update, compiled in per instantiation so that the
 // default stage carries none of their registers
 // OPT_PRE: the cross-derivative half-sums come precomputed from k_cross (the
@@ -220,19 +253,38 @@ __host__ __device__ constexpr int res_idirmin(int ndim, int ndir) {
 }
 
 // k_update body at the mesh cell pos
-template <int NDIM, int NDIR, typename S, int OPT>
+template <int NDIM, int NDIR, typename S, int OPT, bool TILE = false>
 __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, const Offs& o, const int pos[3],
                                             double qdt_d, double qdt2_d, double tdep, double drvA,
-                                            double& numax_out) {
+                                            double& numax_out, const TileView<S>* tv = nullptr) {
+  static_assert(!TILE || (OPT & (OPT_DIVB | OPT_RES | OPT_RES1 | OPT_PRE | OPT_PART_A | OPT_PART_B)) == 0,
+                "the tile form computes the default sources with inline cross terms");
   using PR = Pairs<NDIM>;
   using T = S;
   constexpr int NP = 2 * NDIR + 2, E = NDIR + 1, B0 = NDIR + 1;
   T numax = T(0);
   {
-    const int st[3] = {1, (int)g.st[1], (int)g.st[2]};
-    const int c = pos[0] + st[1] * pos[1] + st[2] * pos[2];
-    auto W = [&](int iw) { return (const S*)a.fW[iw] + o.P; };
-    auto Df = [&](int i) { return (const S*)a.fD[i] + o.I; };
+    // stencil fields at c and its neighbours (st); the cell's own global fields at cg
+    const int st[3] = {1, TILE ? tv->st1 : (int)g.st[1], TILE ? 0 : (int)g.st[2]};
+    const int c = TILE ? tv->c : pos[0] + st[1] * pos[1] + st[2] * pos[2];
+    const long cg = TILE ? tv->cg : (long)c;
+    const long stg[3] = {1, g.st[1], g.st[2]};
+    auto W = [&](int iw) {
+      if constexpr (TILE) return tv->W[iw];
+      else return (const S*)a.fW[iw] + o.P;
+    };
+    auto Df = [&](int i) {
+      if constexpr (TILE) return tv->D[i];
+      else return (const S*)a.fD[i] + o.I;
+    };
+    auto FF = [&](int d, int iw) {
+      if constexpr (TILE) return tv->F[d][iw];
+      else return (const S*)a.fF[d][iw] + o.I;
+    };
+    auto QQ = [&](int ip) {
+      if constexpr (TILE) return tv->Q[ip];
+      else return (const S*)a.fQ[ip] + o.I;
+    };
     auto BG = [&](int i) { return a.fBG[i] + o.B; };
     const S* base = (const S*)a.base + o.P;
     const long sP = a.sP;
@@ -240,21 +292,21 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
     if constexpr ((OPT & OPT_PART_B) != 0) {
       const S* part = (const S*)a.out + o.P;  // part A's sums after centdiff4 and gravity
 #pragma unroll
-      for (int iw = 0; iw < NP; ++iw) acc[iw] = part[iw * sP + c];
+      for (int iw = 0; iw < NP; ++iw) acc[iw] = part[iw * sP + cg];
     } else {
 #pragma unroll
-      for (int iw = 0; iw < NP; ++iw) acc[iw] = base[iw * sP + c];
+      for (int iw = 0; iw < NP; ++iw) acc[iw] = base[iw * sP + cg];
     }
     T dxv[NDIM];
 #pragma unroll
-    for (int d = 0; d < NDIM; ++d) dxv[d] = (T)__ldg(a.fDX[d] + o.X + c);
+    for (int d = 0; d < NDIM; ++d) dxv[d] = (T)__ldg(a.fDX[d] + o.X + cg);
     // gradient4 (src/vacgrid.t:684): -(q(+2) - 8(q(+1)-q(-1)) - q(-2))/dx/12, zero on
     // the first and last two mesh cells along its dimension (:690-709)
     bool z4[NDIM];
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) z4[d] = pos[d] <= g.lo[d] + 1 || pos[d] >= g.hi[d] - 1;
     auto g4 = [&](const S* q, int s, T dxd) {
-      return -(ld(q, c + 2 * s) - T(8) * (ld(q, c + s) - ld(q, c - s)) - ld(q, c - 2 * s)) / dxd / T(12);
+      return -(ldt<TILE>(q, c + 2 * s) - T(8) * (ldt<TILE>(q, c + s) - ldt<TILE>(q, c - s)) - ldt<TILE>(q, c - 2 * s)) / dxd / T(12);
     };
     const T qdt = (T)qdt_d;
 
@@ -269,7 +321,7 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
         for (int iw = 0; iw < NP; ++iw) {
           if (iw == B0 + 1 + d) continue;  // no flux of b_d along d
           if (!((a.iwmask >> iw) & 1u)) continue;
-          acc[iw] = acc[iw] - qdt * g4((const S*)a.fF[d][iw] + o.I, st[d], dxv[d]);
+          acc[iw] = acc[iw] - qdt * g4(FF(d, iw), st[d], dxv[d]);
         }
       }
       if ((a.iwmask >> E) & 1u) {
@@ -278,37 +330,37 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
           // getptotal_bg, src/vacphys0.t.mhd:221
           double bgs = 0.0;
 #pragma unroll
-          for (int C = 0; C < NDIR; ++C) bgs = bgs + __ldg(BG(2 + C) + c) * __ldg(BG(2 + C) + c);
-          const T fb = (T)((a.gamma - 1.0) * __ldg(BG(0) + c) - 0.5 * (a.gamma - 2.0) * bgs);
+          for (int C = 0; C < NDIR; ++C) bgs = bgs + __ldg(BG(2 + C) + cg) * __ldg(BG(2 + C) + cg);
+          const T fb = (T)((a.gamma - 1.0) * __ldg(BG(0) + cg) - 0.5 * (a.gamma - 2.0) * bgs);
           acc[E] = acc[E] - qdt * g4(vd, st[d], dxv[d]) * fb;
         }
 #pragma unroll
         for (int di = 0; di < NDIM; ++di) {
           if (di < a.dmin || di > a.dmax || z4[di]) continue;
-          acc[E] = acc[E] + qdt * (T)__ldg(BG(2 + di) + c) * (T)__ldg(BG(2 + d) + c) * g4(vd, st[di], dxv[di]);
+          acc[E] = acc[E] + qdt * (T)__ldg(BG(2 + di) + cg) * (T)__ldg(BG(2 + d) + cg) * g4(vd, st[di], dxv[di]);
         }
       }
     }
 
     // --- gravity, src/vacusr.gravity.t:46-78 ---------------------------------------
     if (a.grav_on) {
-      const T rho = ld(W(0), c);
+      const T rho = ldt<TILE>(W(0), c);
 #pragma unroll
       for (int d = 0; d < NDIM; ++d)
         if (((a.iwmask >> (1 + d)) & 1u) && fabs(a.grav[d]) > kSmall)
           acc[1 + d] = acc[1 + d] + q2 * (T)a.grav[d] * rho;
       if ((a.iwmask >> E) & 1u) {
-        const T rt = ld(Df(0), c);
+        const T rt = ldt<TILE>(Df(0), c);
 #pragma unroll
         for (int d = 0; d < NDIM; ++d)
-          if (fabs(a.grav[d]) > kSmall) acc[E] = acc[E] + q2 * (T)a.grav[d] * rho * ld(W(1 + d), c) / rt;
+          if (fabs(a.grav[d]) > kSmall) acc[E] = acc[E] + q2 * (T)a.grav[d] * rho * ldt<TILE>(W(1 + d), c) / rt;
       }
     }
     }  // centdiff4 and gravity
     if constexpr ((OPT & OPT_PART_A) != 0) {
       S* part = (S*)a.out + o.P;
 #pragma unroll
-      for (int iw = 0; iw < NP; ++iw) part[iw * sP + c] = acc[iw];
+      for (int iw = 0; iw < NP; ++iw) part[iw * sP + cg] = acc[iw];
     } else {
 
     // --- hyperdiffusion, src/vacusr.viscosity.t:2-221 --------------------------------
@@ -319,9 +371,9 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
       for (int d = 0; d < NDIM; ++d)
         z1[d] = (a.zero1[d][0] && pos[d] == g.lo[d]) || (a.zero1[d][1] && pos[d] == g.hi[d]);
       auto nus = [&](int ip, int k, int j, T dxk, T& nl, T& nr) {
-        const S* Qp = (const S*)a.fQ[ip] + o.I;
-        nr = ld(Qp, j) * dxk;
-        nl = ld(Qp, j - st[k]) * dxk;
+        const S* Qp = QQ(ip);
+        nr = ldt<TILE>(Qp, j) * dxk;
+        nl = ldt<TILE>(Qp, j - st[k]) * dxk;
       };
       // density and the "173" energy, :45-64
 #pragma unroll
@@ -333,9 +385,9 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
           T nl, nr;
           nus(pass == 0 ? PR::rho(k) : PR::e(k), k, c, dxv[k], nl, nr);
           numax = fmaxT(numax, fmaxT(nr, nl));
-          const T qc = ld(q, c);
-          const T gL = z1[k] ? T(0) : (qc - ld(q, c - st[k])) / dxv[k];
-          const T gR = z1[k] ? T(0) : (ld(q, c + st[k]) - qc) / dxv[k];
+          const T qc = ldt<TILE>(q, c);
+          const T gL = z1[k] ? T(0) : (qc - ldt<TILE>(q, c - st[k])) / dxv[k];
+          const T gR = z1[k] ? T(0) : (ldt<TILE>(q, c + st[k]) - qc) / dxv[k];
           const T tL = (nl + T(0)) * gL, tR = (nr + T(0)) * gR;
           acc[tgt] = acc[tgt] + (tR - tL) / dxv[k] * q2;
         }
@@ -346,21 +398,21 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
       for (int k = 0; k < NDIM; ++k) {
         const int sk = st[k];
         const T dxk = dxv[k];
-        const T rC = ld(rtf, c);
-        const T rL = (rC + ld(rtf, c - sk)) / T(2), rR = (ld(rtf, c + sk) + rC) / T(2);
+        const T rC = ldt<TILE>(rtf, c);
+        const T rL = (rC + ldt<TILE>(rtf, c - sk)) / T(2), rR = (ldt<TILE>(rtf, c + sk) + rC) / T(2);
 #pragma unroll
         for (int l = 0; l < NDIM; ++l) {
           const S* q = Df(1 + l);  // v_l
           T nl, nr;
           nus(PR::v(l, k), k, c, dxk, nl, nr);
           numax = fmaxT(numax, fmaxT(nr, nl));
-          const T qc = ld(q, c);
-          const T gL = z1[k] ? T(0) : (qc - ld(q, c - sk)) / dxk;
-          const T gR = z1[k] ? T(0) : (ld(q, c + sk) - qc) / dxk;
+          const T qc = ldt<TILE>(q, c);
+          const T gL = z1[k] ? T(0) : (qc - ldt<TILE>(q, c - sk)) / dxk;
+          const T gR = z1[k] ? T(0) : (ldt<TILE>(q, c + sk) - qc) / dxk;
           const T tL = (nl + T(0)) * gL, tR = (nr + T(0)) * gR;
           const S* ml = W(1 + l);
-          const T mc = ld(ml, c);
-          const T VL = (mc + ld(ml, c - sk)) / T(2), VR = (ld(ml, c + sk) + mc) / T(2);
+          const T mc = ldt<TILE>(ml, c);
+          const T VL = (mc + ldt<TILE>(ml, c - sk)) / T(2), VR = (ldt<TILE>(ml, c + sk) + mc) / T(2);
           const T t2m = (rR * tR - rL * tL) / dxk / T(2);
           const T t2e = (VR * tR - VL * tL) / dxk / T(2);
           // ii1=0: i=k, ii0=l
@@ -377,21 +429,22 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
 #pragma unroll
             for (int sg = 0; sg < 2; ++sg) {
               const int j = sg ? c + sl : c - sl;
+              const long jg = sg ? cg + stg[l] : cg - stg[l];
               const int pl = pos[l] + (sg ? 1 : -1);
               T H = T(0);
               if (pl >= g.lo[l] && pl <= g.hi[l]) {  // nu vanishes outside the mesh
                 if constexpr ((OPT & OPT_PRE) != 0) {
-                  H = ld((const S*)a.fX[Cross<NDIM>::m(l, k)] + o.I, j);
+                  H = ldt<TILE>((const S*)a.fX[Cross<NDIM>::m(l, k)] + o.I, j);
                 } else {
-                  const T dxkj = (T)__ldg(a.fDX[k] + o.X + j);
+                  const T dxkj = (T)__ldg(a.fDX[k] + o.X + jg);
                   T njl, njr;
                   nus(PR::v(l, k), k, j, dxkj, njl, njr);
-                  const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
+                  const T gC = z1[k] ? T(0) : (ldt<TILE>(q, j + sk) - ldt<TILE>(q, j - sk)) / dxkj / T(2);
                   H = gC * (njl + njr + T(2) * T(0)) / T(2) / T(2);
                 }
               }
-              Tm[sg] = ld(rtf, j) * H;
-              Te[sg] = ld(W(1 + k), j) * H;
+              Tm[sg] = ldt<TILE>(rtf, j) * H;
+              Te[sg] = ldt<TILE>(W(1 + k), j) * H;
             }
             const T dxl = dxv[l];
             const T tCm = z1[l] ? T(0) : (Tm[1] - Tm[0]) / dxl / T(2);
@@ -419,21 +472,22 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
 #pragma unroll
             for (int sg = 0; sg < 2; ++sg) {
               const int j = sg ? c + sl : c - sl;
+              const long jg = sg ? cg + stg[l] : cg - stg[l];
               const int pl = pos[l] + (sg ? 1 : -1);
               T Kv = T(0);
               if (pl >= g.lo[l] && pl <= g.hi[l]) {
                 if constexpr ((OPT & OPT_PRE) != 0) {
-                  Kv = ld((const S*)a.fX[Cross<NDIM>::b(l, k)] + o.I, j);
+                  Kv = ldt<TILE>((const S*)a.fX[Cross<NDIM>::b(l, k)] + o.I, j);
                 } else {
-                  const T dxkj = (T)__ldg(a.fDX[k] + o.X + j);
+                  const T dxkj = (T)__ldg(a.fDX[k] + o.X + jg);
                   T njl, njr;
                   nus(PR::b(l, k), k, j, dxkj, njl, njr);
-                  const T gC = z1[k] ? T(0) : (ld(q, j + sk) - ld(q, j - sk)) / dxkj / T(2);
+                  const T gC = z1[k] ? T(0) : (ldt<TILE>(q, j + sk) - ldt<TILE>(q, j - sk)) / dxkj / T(2);
                   Kv = gC * (njl + njr) / T(2);
                 }
               }
               K[sg] = Kv;
-              Ke[sg] = Kv * ld(W(B0 + 1 + k), j);
+              Ke[sg] = Kv * ldt<TILE>(W(B0 + 1 + k), j);
             }
             const T dxl = dxv[l];
             const T tC = z1[l] ? T(0) : (K[1] - K[0]) / dxl / T(2);
@@ -443,7 +497,7 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
           }
           // ii1=1: ii0=l, m=k, sB=+1, j=l (m == k branch)
           {
-            const T qc = ld(q, c), qm = ld(q, c - sk), qp = ld(q, c + sk);
+            const T qc = ldt<TILE>(q, c), qm = ldt<TILE>(q, c - sk), qp = ldt<TILE>(q, c + sk);
             const T BL = (qc + qm) / T(2), BR = (qp + qc) / T(2);
             const T gL = z1[k] ? T(0) : (qc - qm) / dxk;
             const T gR = z1[k] ? T(0) : (qp - qc) / dxk;
@@ -456,18 +510,18 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
 
     // --- user driver: tdep from the host, spatial profiles precomputed there -----------
     if (a.driver != DRV_NONE) {
-      const T rtn = (T)((double)acc[0] + __ldg(BG(1) + c));
+      const T rtn = (T)((double)acc[0] + __ldg(BG(1) + cg));
       if (a.driver == DRV_SLOG) {
         // src/vacusr.f:1355-1375 (x1 vertical; m2, m3 driven)
-        const T vvx = (T)(__ldg(a.drv + o.X + c) * tdep * drvA);
-        const T vvy = (T)(__ldg(a.drv + a.sX + o.X + c) * tdep * drvA);
+        const T vvx = (T)(__ldg(a.drv + o.X + cg) * tdep * drvA);
+        const T vvy = (T)(__ldg(a.drv + a.sX + o.X + cg) * tdep * drvA);
         if (NDIR >= 3) {
           acc[2] = acc[2] + rtn * vvx * q2;
           acc[3 % NP] = acc[3 % NP] + rtn * vvy * q2;
         }
         acc[E] = acc[E] + rtn * (vvx * vvx + vvy * vvy + T(0) * T(0)) * q2 / T(2);
       } else {
-        const T v = (T)(drvA * tdep * __ldg(a.drv + o.X + c) * __ldg(a.drv + a.sX + o.X + c));
+        const T v = (T)(drvA * tdep * __ldg(a.drv + o.X + cg) * __ldg(a.drv + a.sX + o.X + cg));
         const int comp = (a.driver == DRV_STRAT) ? 1 : 2;
         acc[comp] = acc[comp] + rtn * v * q2;
         acc[E] = acc[E] + rtn * (v * v) * q2 / T(2);
@@ -478,7 +532,7 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
     // orders them (src/vac.t:569-571): the resistive term, then Powell's; both
     // read wCT only
     // b + bg at cell n, summed in FP64
-    auto Bat = [&](int C, int n) { return (T)((double)ld(W(B0 + 1 + C), n) + __ldg(BG(2 + C) + n)); };
+    auto Bat = [&](int C, int n) { return (T)((double)ldt<TILE>(W(B0 + 1 + C), n) + __ldg(BG(2 + C) + n)); };
 
     // --- resistivity, addsource_res2 (src/vacphys.mhdres.t:231-301), constant eta ------
     // J = curl(b+bg) by getcurrent (:48-95) at the 2*ndim face neighbours, with the
@@ -588,11 +642,11 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
         divb = divb + gd;
       }
       divb = q2 * divb;
-      const T rt = ld(Df(0), c);
+      const T rt = ldt<TILE>(Df(0), c);
       T sm = T(0);
 #pragma unroll
       for (int C = 0; C < NDIR; ++C) {
-        const T mC = ld(W(1 + C), c);
+        const T mC = ldt<TILE>(W(1 + C), c);
         const T BC = Bat(C, c);
         if ((a.iwmask >> (1 + C)) & 1u) acc[1 + C] = acc[1 + C] - BC * divb;
         if ((a.iwmask >> (B0 + 1 + C)) & 1u) acc[B0 + 1 + C] = acc[B0 + 1 + C] - mC / rt * divb;
@@ -605,21 +659,22 @@ __device__ __forceinline__ void update_cell(const Stage2Args& a, const Geom& g, 
     S* out = (S*)a.out + o.P;
     if (a.epi == EPI_PLAIN) {
 #pragma unroll
-      for (int iw = 0; iw < NP; ++iw) out[iw * sP + c] = acc[iw];
+      for (int iw = 0; iw < NP; ++iw) out[iw * sP + cg] = acc[iw];
     } else if (a.epi == EPI_RK4_S3) {
       S* w1 = (S*)a.aux1 + o.P;
       const S* w2 = (const S*)a.aux2 + o.P;
 #pragma unroll
       for (int iw = 0; iw < NP; ++iw) {
         const T w3 = acc[iw];
-        out[iw * sP + c] = w3;
-        w1[iw * sP + c] = (w1[iw * sP + c] + T(2) * w2[iw * sP + c] + w3 - T(4) * base[iw * sP + c]) / T(3);
+        out[iw * sP + cg] = w3;
+        w1[iw * sP + cg] = (w1[iw * sP + cg] + T(2) * w2[iw * sP + cg] + w3 - T(4) * base[iw * sP + cg]) / T(3);
       }
     } else {
       const S* w1 = (const S*)a.aux1 + o.P;
 #pragma unroll
-      for (int iw = 0; iw < NP; ++iw) out[iw * sP + c] = acc[iw] + w1[iw * sP + c];
+      for (int iw = 0; iw < NP; ++iw) out[iw * sP + cg] = acc[iw] + w1[iw * sP + cg];
     }
+
     }  // part B
     }
   numax_out = fmax(numax_out, (double)numax);
@@ -964,32 +1019,12 @@ void dispatch_nd(const Geom& g, Fn&& f) {
   else f(std::integral_constant<int, 3>{}, std::integral_constant<int, 3>{});
 }
 
-// The stage kernels read their stencil neighbours through L1 and use almost no
-// shared memory: with SAC_PREFER_L1 they ask for the largest L1 share of the
-// unified L1/shared storage (set once per kernel).
-#ifndef SAC_PREFER_L1
-#define SAC_PREFER_L1 0
-#endif
-template <typename K>
-inline void prefer_l1(K* kernel) {
-  if constexpr (SAC_PREFER_L1 != 0) {
-    static bool done = false;  // per kernel instantiation
-    if (!done) {
-      cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-      done = true;
-    }
-  } else {
-    (void)kernel;
-  }
-}
-
 template <typename S>
 void launch_face(const Stage2Args& a0, int do_ctot, cudaStream_t st) {
   Stage2Args a = a0;
   fill_field_ptrs(a, sizeof(S));
   const int N = (int)a.g.ncell;
   dispatch_nd(a.g, [&](auto ND, auto NR) {
-    prefer_l1(k_face<decltype(ND)::value, decltype(NR)::value, S>);
     k_face<decltype(ND)::value, decltype(NR)::value, S><<<(unsigned)((N + 255) / 256), 256, 0, st>>>(a, do_ctot);
   });
 }
@@ -1001,7 +1036,6 @@ void launch_nu(const Stage2Args& a0, cudaStream_t st) {
   long nb = 1;
   for (int d = 0; d < a.g.ndim; ++d) nb *= (a.g.hi[d] - a.g.lo[d] + 2);
   dispatch_nd(a.g, [&](auto ND, auto NR) {
-    prefer_l1(k_nu<decltype(ND)::value, decltype(NR)::value, S>);
     k_nu<decltype(ND)::value, decltype(NR)::value, S><<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(a);
   });
 }
@@ -1056,13 +1090,10 @@ void launch_update(const Stage2Args& a0, cudaStream_t st) {
     }
     // SAC_UPDATE_SPLIT bit 0: the FP64 3D update in two parts; bit 1: the FP32 one
     if constexpr (NDIM == 3 && (SAC_UPDATE_SPLIT & (sizeof(S) == 8 ? 1 : 2)) != 0) {
-      prefer_l1(k_update<NDIM, NDIR, S, P | OPT_PART_A>);
-      prefer_l1(k_update<NDIM, NDIR, S, P | OPT_PART_B>);
       k_update<NDIM, NDIR, S, P | OPT_PART_A><<<grd, blk, 0, st>>>(a);
       k_update<NDIM, NDIR, S, P | OPT_PART_B><<<grd, blk, 0, st>>>(a);
       return;
     }
-    prefer_l1(k_update<NDIM, NDIR, S, P>);
     k_update<NDIM, NDIR, S, P><<<grd, blk, 0, st>>>(a);
   });
 }
@@ -1079,7 +1110,6 @@ void launch_cross(const Stage2Args& a0, cudaStream_t st) {
       const dim3 blk = NDIM == 2 ? dim3(32, 8, 1) : dim3(32, 4, 2);
       const int n0 = g.hi[0] - g.lo[0] + 1, n1 = g.hi[1] - g.lo[1] + 1, n2 = g.hi[2] - g.lo[2] + 1;
       const dim3 grd((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, (n2 + blk.z - 1) / blk.z);
-      prefer_l1(k_cross<NDIM, decltype(NR)::value, S>);
       k_cross<NDIM, decltype(NR)::value, S><<<grd, blk, 0, st>>>(a);
     }
   });

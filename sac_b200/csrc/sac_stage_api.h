@@ -124,6 +124,20 @@ void launch_batch_update(const BatchStageArgs& b, dim3 blk, cudaStream_t st);
 template <typename S>
 void launch_batch_courant(const BatchStageArgs& b, double gamma, cudaStream_t st);
 
+// the fused 2D stage (sac_stage2d.cuh): c_tot of the stage input, then one kernel
+// per tile for face, setnu and update; shape indexes the tile shapes
+template <typename S>
+void launch_batch_ctot(const BatchStageArgs& b, cudaStream_t st);
+template <typename S>
+cudaError_t launch_batch_stage2d(const BatchStageArgs& b, int shape, cudaStream_t st);
+constexpr int kStage2dShapeCount = 2;
+inline int stage2d_shape_tx(int i) { return i == 0 ? 32 : 16; }
+inline int stage2d_shape_ty(int i) { return i == 0 ? 8 : 8; }
+extern template void launch_batch_ctot<double>(const BatchStageArgs&, cudaStream_t);
+extern template void launch_batch_ctot<float>(const BatchStageArgs&, cudaStream_t);
+extern template cudaError_t launch_batch_stage2d<double>(const BatchStageArgs&, int, cudaStream_t);
+extern template cudaError_t launch_batch_stage2d<float>(const BatchStageArgs&, int, cudaStream_t);
+
 extern template void launch_batch_face<double>(const BatchStageArgs&, double, cudaStream_t);
 extern template void launch_batch_face<float>(const BatchStageArgs&, double, cudaStream_t);
 extern template void launch_batch_nu<double>(const BatchStageArgs&, cudaStream_t);
