@@ -394,7 +394,8 @@ def leg_summary(m, args, peak, peak_kind):
         d["fp64"] = {"value": m["v64"], "ms_per_step": r["ms"] / args.steps, "gpu_launches": r["launches"],
                      "kernels_ms_per_step": {k: v[0] / args.steps for k, v in r["kern"].items()},
                      "roofline": roofline(BYTES_PER_CELL_UPDATE["fp64"], cells, r["kern"], peak, peak_kind,
-                                          "update_fp64_traffic.json", "k_update<3,3,double>")}
+                                          "update_fp64_traffic.json",
+                                          "k_update<3,3,double> parts A+B (one RK stage)")}
     if "r32" in m:
         r = m["r32"]
         d["fp32"] = {"value": m["v32"], "ms_per_step": r["ms"] / args.steps, "gpu_launches": r["launches"],

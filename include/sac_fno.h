@@ -47,6 +47,18 @@ typedef struct sac_fno_gemm_desc {
                    * up at once, sets bit 0 of *err and the kernel returns (a test of the
                    * time-out path; MMAs already issued are still drained with the default
                    * bound before the accumulator is released) */
+  /* a second product accumulated into the same tile when K2 > 0:
+   *   C = epilogue(alpha * (sum_k A(m,k) B(n,k) + sum_k2 A2(m,k2) B2(n,k2)))
+   * A2 is addressed like A; B2 like B without a row split, its base moved by
+   * (m0 / b2_mdiv) * b2_m for the 128-row tile whose first row is m0 (b2_mdiv a
+   * multiple of 128).  Needs ksplit = 1. */
+  int K2;
+  int a2_msplit, a2_mn_major;
+  const void* a2;
+  long a2_m0, a2_m1, a2_k, a2_b;
+  const void* b2;
+  long b2_n, b2_k, b2_b, b2_m;
+  int b2_mn_major, b2_mdiv;
 } sac_fno_gemm_desc;
 
 /* 0 on success; 1 on an argument that breaks the requirements (message in

@@ -171,6 +171,10 @@ sac_status sac_set_grid(sac_ctx* c, int ndim, int ndir, const int ixGhi[3], cons
 sac_status sac_set_boundaries(sac_ctx* c, int nB, const char* typeB, const int* ixB, const int* idimB,
                               const int* upperB, const int* ipairB);
 
+/* w is always the host's FP64 w(ixG^T,nw).  There is no per-call storage mode:
+ * the precision of the resident perturbed variables is the context's
+ * sac_params.precision, fixed at sac_create because the FP32 path's arrays and
+ * kernels are chosen then; upload rounds to it and download widens from it. */
 sac_status sac_upload(sac_ctx* c, const double* w);
 sac_status sac_download(sac_ctx* c, double* w);
 sac_status sac_getboundary(sac_ctx* c, double t);
@@ -289,6 +293,34 @@ sac_status sac_batch_tune(sac_batch* b, int* tile_xy, double* ms);
  * times of one stage (ms). */
 sac_status sac_batch_set_stage(sac_batch* b, int fused, int shape);
 sac_status sac_batch_get_stage(const sac_batch* b, int* fused, int* shape, double* ms_three, double* ms_fused);
+/* FP64 and FP32-perturbation instances advanced together.  After
+ * sac_batch_join(lead, partner), sac_batch_advance(lead, n) advances the
+ * instances of both batches in one CUDA graph per step, each instance with its
+ * own dt.  lead holds FP64 instances, partner FP32 ones, with the same parameters
+ * (all but the precision), ndim = 2, ndir and device; both must have had their
+ * first boundary fill; both take the fused stage in the lead's tile shape.  The
+ * graph has one of two forms:
+ *   0  joint kernels: every kernel of the RK4 step (getdt_courant, the dt block,
+ *      c_tot, the fused stage, the boundary fill) is one persistent launch over
+ *      the tiles of both batches;
+ *   1  two branches: each batch's own kernels, the partner's on its own stream
+ *      beside the lead's.
+ * sac_batch_join times one RK stage in each form and keeps the faster;
+ * sac_batch_set_join_form overrides it and sac_batch_get_join reports the form
+ * (-1 when b leads no pair) and the two times (ms).  The FP64 instances advance
+ * bit for bit as in a batch of their own in both forms.  In form 0 the FP32
+ * instances compute without FMA contraction (the FP64 units' rounding rules), so
+ * they may differ in the last bits from an FP32 batch advanced alone.  While
+ * joined, the partner's work runs on the lead's stream (sac_batch_get_stream
+ * returns it), and sac_batch_advance, sac_batch_tune, sac_batch_set_stage,
+ * sac_batch_set_grid and sac_batch_set_boundaries of either batch are
+ * SAC_ERR_STATE, except advancing the lead; uploads, downloads, the state,
+ * drivers, times and packing work on each batch as before.
+ * sac_batch_unjoin(lead), or destroying either batch, ends the join. */
+sac_status sac_batch_join(sac_batch* lead, sac_batch* partner);
+sac_status sac_batch_unjoin(sac_batch* lead);
+sac_status sac_batch_set_join_form(sac_batch* lead, int form);
+sac_status sac_batch_get_join(const sac_batch* lead, int* form, double* ms_joint, double* ms_forked);
 /* per-instance driver amplitude and angular frequency of the Gaussian velocity
  * drivers (users SAC_USR_STRAT and SAC_USR_TUBE, tdep = sin(omega t)); the
  * defaults are userpar[0] and userpar[1].  Either array may be NULL. */

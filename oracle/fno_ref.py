@@ -20,19 +20,19 @@ import math
 import numpy as np
 
 
-try:
-    from scipy.special import erf as _erf
-except ImportError:  # pragma: no cover
-    def _erf(x):
-        return np.vectorize(math.erf, otypes=[np.float64])(x)
+# GELU in its tanh form (Hendrycks and Gimpel, "Gaussian Error Linear Units"):
+# 0.5 x (1 + tanh(c0 (x + c1 x^3))), c0 = sqrt(2/pi), c1 = 0.044715
+GELU_C0 = math.sqrt(2.0 / math.pi)
+GELU_C1 = 0.044715
 
 
 def gelu(x):
-    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
+    return 0.5 * x * (1.0 + np.tanh(GELU_C0 * (x + GELU_C1 * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + _erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(GELU_C0 * (x + GELU_C1 * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * GELU_C0 * (1.0 + 3.0 * GELU_C1 * x * x)
 
 
 class Layout:

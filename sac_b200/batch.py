@@ -45,6 +45,10 @@ def _bind(lib):
     f("set_tmax").argtypes = [P, DP]
     f("set_stage").argtypes = [P, ctypes.c_int, ctypes.c_int]
     f("get_stage").argtypes = [P, IP, IP, DP, DP]
+    f("join").argtypes = [P, P]
+    f("unjoin").argtypes = [P]
+    f("set_join_form").argtypes = [P, ctypes.c_int]
+    f("get_join").argtypes = [P, IP, DP, DP]
     f("mesh_cells").argtypes = [P]
     f("mesh_cells").restype = ctypes.c_long
     f("gather").argtypes = [P, ctypes.c_void_p, ctypes.c_int]
@@ -55,7 +59,8 @@ def _bind(lib):
     f("destroy").restype = None
     for n in ("create", "set_grid", "set_boundaries", "upload", "download", "upload_range", "download_range",
               "getboundary", "advance", "state", "synchronize", "tune", "set_driver", "set_time", "set_tmax", "gather",
-              "scatter", "set_stage", "get_stage"):
+              "scatter", "set_stage", "get_stage", "join", "unjoin", "set_join_form",
+              "get_join"):
         f(n).restype = ctypes.c_int
     lib._sac_batch_bound = True
     return lib
@@ -204,6 +209,27 @@ class Batch:
         a, b = ctypes.c_double(0.0), ctypes.c_double(0.0)
         self._call("get_stage", ctypes.byref(f), ctypes.byref(sh), ctypes.byref(a), ctypes.byref(b))
         return bool(f.value), sh.value, a.value, b.value
+
+    def join(self, partner):
+        """Advance `partner` (FP32 instances, the same parameters) with this FP64
+        batch: from now on advance() steps both in one graph, in the faster of
+        the two join forms (0: joint kernels over the tiles of both batches, 1:
+        each batch's kernels on a branch of its own)."""
+        self._call("join", self.h, partner.h, own=False)
+
+    def set_join_form(self, form):
+        self._call("set_join_form", int(form))
+
+    def join_info(self):
+        """(form, ms of one joint-kernel stage, ms of one two-branch stage)."""
+        f = ctypes.c_int(0)
+        a, b = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self._call("get_join", ctypes.byref(f), ctypes.byref(a), ctypes.byref(b))
+        return f.value, a.value, b.value
+
+    def unjoin(self):
+        """End join(): each batch advances alone again."""
+        self._call("unjoin")
 
     def close(self):
         if self.h:

@@ -29,6 +29,7 @@ LIBS = {
         ("stage_f64.cu", ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
         ("stage_f32.cu", ["--fmad=true", "-prec-div=false", "-ftz=true"]),
         ("sac_batch.cu", ["--fmad=false"]),
+        ("stage_joint.cu", ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ], "sac_gpu.h"),
     FNO_OUT: (os.path.join(CSRC, "fno"), [
         ("fno_gemm.cu", []),

@@ -95,6 +95,29 @@ int gemm(const GemmDesc& d, cudaStream_t st) {
     if (d.b_k != 1) return bad("K-major B needs b_k == 1");
     if (d.b_n % 8 || d.b_n1 % 8 || d.b_b % 8) return bad("K-major B alignment");
   }
+  if (d.K2 < 0) return bad("negative K2");
+  if (d.K2 > 0) {
+    if (d.K2 % 8) return bad("K2 must be a multiple of 8");
+    if (d.ksplit != 1) return bad("a second product needs ksplit == 1");
+    if (!d.a2 || !d.b2) return bad("null second operand");
+    if (!aligned16(d.a2) || !aligned16(d.b2)) return bad("second operands must be 16-byte aligned");
+    if (d.a2_msplit <= 0) return bad("a2_msplit must be positive");
+    if (d.b2_mdiv <= 0 || d.b2_mdiv % kBM) return bad("b2_mdiv must be a positive multiple of 128");
+    if (d.a2_mn_major) {
+      if (d.a2_m0 != 1) return bad("MN-major A2 needs a2_m0 == 1");
+      if (d.M % 8 || d.a2_msplit % 8 || d.a2_k % 8 || d.a2_m1 % 8 || d.a2_b % 8) return bad("MN-major A2 alignment");
+    } else {
+      if (d.a2_k != 1) return bad("K-major A2 needs a2_k == 1");
+      if (d.a2_m0 % 8 || d.a2_m1 % 8 || d.a2_b % 8) return bad("K-major A2 alignment");
+    }
+    if (d.b2_mn_major) {
+      if (d.b2_n != 1) return bad("MN-major B2 needs b2_n == 1");
+      if (d.N % 8 || d.b2_k % 8 || d.b2_b % 8 || d.b2_m % 8) return bad("MN-major B2 alignment");
+    } else {
+      if (d.b2_k != 1) return bad("K-major B2 needs b2_k == 1");
+      if (d.b2_n % 8 || d.b2_b % 8 || d.b2_m % 8) return bad("K-major B2 alignment");
+    }
+  }
   if (d.c_mode == C_ATOMIC && d.c_bf16) return bad("atomic accumulation needs a float C");
   if (d.ksplit > 1 && d.c_mode != C_ATOMIC) return bad("ksplit > 1 needs c_mode atomic");
   if (d.act == ACT_GELU_GRAD && !d.pre) return bad("GELU' needs the pre-activation");

@@ -60,6 +60,18 @@ struct GemmDesc {
   // up at once; a test of the time-out path).  The wait that drains the MMAs in
   // flight before the accumulator is released always keeps the default bound.
   int wait_tries;
+  // a second product accumulated into the same tile when K2 > 0:
+  //   C = epilogue(alpha * (sum_k A(m,k) B(n,k) + sum_k2 A2(m,k2) B2(n,k2)))
+  // A2 is addressed like A; B2 like B without a row split, its base moved by
+  // (m0 / b2_mdiv) * b2_m for the tile whose first row is m0 (b2_mdiv a multiple of
+  // the tile height, so that all rows of a tile read the same B2 block)
+  int K2;
+  int a2_msplit, a2_mn_major;
+  const bf16* a2;
+  long a2_m0, a2_m1, a2_k, a2_b;
+  const bf16* b2;
+  long b2_n, b2_k, b2_b, b2_m;
+  int b2_mn_major, b2_mdiv;
 };
 
 constexpr int kBM = 128, kBK = 64, kThreads = 128;
@@ -140,9 +152,23 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int tr
   return false;
 }
 
-__device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks and Gimpel): 0.5 x (1 + tanh(u)),
+// u = c0 (x + c1 x^3), c0 = sqrt(2/pi), c1 = 0.044715, with the SFU's tanh
+// (tanh.approx.f32, relative error near 2^-11, below the BF16 rounding of the
+// activations it feeds); its derivative 0.5 (1 + t) + 0.5 x (1 - t^2) c0 (1 + 3 c1 x^2)
+__device__ __forceinline__ float tanh_sfu(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float gelu_f(float x) {
+  const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+  return 0.5f * x * (1.0f + tanh_sfu(u));
+}
 __device__ __forceinline__ float gelu_grad_f(float x) {
-  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float x2 = x * x;
+  const float t = tanh_sfu(0.7978845608028654f * fmaf(0.044715f * x, x2, x));
+  return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * (0.7978845608028654f * fmaf(0.134145f, x2, 1.0f));
 }
 
 // the 16-byte chunks one thread moves for a ROWS x 64 operand tile
@@ -227,9 +253,12 @@ __global__ void __launch_bounds__(kThreads, BN <= 64 ? 4 : BN <= 128 ? 3 : 1) k_
   const int zb = blockIdx.z / d.ksplit, zk = blockIdx.z % d.ksplit;
   const int kper = ((d.K + d.ksplit - 1) / d.ksplit + kBK - 1) / kBK * kBK;
   const int kbeg = zk * kper, kend = min(d.K, kbeg + kper);
-  const int nk = kend > kbeg ? (kend - kbeg + kBK - 1) / kBK : 0;
+  const int nk1 = kend > kbeg ? (kend - kbeg + kBK - 1) / kBK : 0;
+  const int nk = nk1 + (d.K2 > 0 ? (d.K2 + kBK - 1) / kBK : 0);  // k tiles of both products
   const bf16* A = d.a + (long)zb * d.a_b;
   const bf16* B = d.b + (long)zb * d.b_b;
+  const bf16* A2 = d.K2 > 0 ? d.a2 + (long)zb * d.a2_b : nullptr;
+  const bf16* B2 = d.K2 > 0 ? d.b2 + (long)zb * d.b2_b + (long)(m0 / d.b2_mdiv) * d.b2_m : nullptr;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
@@ -245,7 +274,8 @@ __global__ void __launch_bounds__(kThreads, BN <= 64 ? 4 : BN <= 128 ? 3 : 1) k_
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_sh;
-  const uint32_t idesc = umma_idesc(BN, d.a_mn_major, d.b_mn_major);
+  const uint32_t idesc1 = umma_idesc(BN, d.a_mn_major, d.b_mn_major);
+  const uint32_t idesc2 = umma_idesc(BN, d.a2_mn_major, d.b2_mn_major);
   const int tries = d.wait_tries == 0 ? kWaitTries : (d.wait_tries < 0 ? 0 : d.wait_tries);
 
   Tile16<kBM> ta;
@@ -253,18 +283,27 @@ __global__ void __launch_bounds__(kThreads, BN <= 64 ? 4 : BN <= 128 ? 3 : 1) k_
   bool ok = true;
   int issued = 0;  // k tiles whose MMAs were issued and committed
   for (int kt = 0; kt < nk; ++kt) {
-    const int s = kt & 1, k0 = kbeg + kt * kBK;
+    const int s = kt & 1;
+    const bool first = kt < nk1;  // uniform: a k tile of the first product or of the second
+    const int a_mn = first ? d.a_mn_major : d.a2_mn_major, b_mn = first ? d.b_mn_major : d.b2_mn_major;
     uint8_t* sa = smem + s * STAGE;
     uint8_t* sb = sa + A_BYTES;
-    load_tile<kBM>(ta, A, d.a_m0, d.a_m1, d.a_msplit, d.a_k, d.a_mn_major, m0, d.M, k0, kend);
-    load_tile<BN>(tb, B, d.b_n, d.b_n1, d.b_nsplit, d.b_k, d.b_mn_major, n0, d.N, k0, kend);
+    if (first) {
+      const int k0 = kbeg + kt * kBK;
+      load_tile<kBM>(ta, A, d.a_m0, d.a_m1, d.a_msplit, d.a_k, d.a_mn_major, m0, d.M, k0, kend);
+      load_tile<BN>(tb, B, d.b_n, d.b_n1, d.b_nsplit, d.b_k, d.b_mn_major, n0, d.N, k0, kend);
+    } else {
+      const int k0 = (kt - nk1) * kBK;
+      load_tile<kBM>(ta, A2, d.a2_m0, d.a2_m1, d.a2_msplit, d.a2_k, d.a2_mn_major, m0, d.M, k0, d.K2);
+      load_tile<BN>(tb, B2, d.b2_n, 0, 1 << 30, d.b2_k, d.b2_mn_major, n0, d.N, k0, d.K2);
+    }
     if (kt >= 2 && !mbar_wait(&bar[s], ((kt - 2) >> 1) & 1, tries)) ok = false;  // stage s free again
     if (__syncthreads_or(!ok)) {
       ok = false;
       break;
     }
-    store_tile<kBM>(ta, sa, d.a_mn_major);
-    store_tile<BN>(tb, sb, d.b_mn_major);
+    store_tile<kBM>(ta, sa, a_mn);
+    store_tile<BN>(tb, sb, b_mn);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
@@ -272,13 +311,13 @@ __global__ void __launch_bounds__(kThreads, BN <= 64 ? 4 : BN <= 128 ? 3 : 1) k_
       const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
 #pragma unroll
       for (int kk = 0; kk < kBK / 16; ++kk) {
-        const uint64_t da = tile_desc<kBM>(a0, d.a_mn_major, kk);
-        const uint64_t db = tile_desc<BN>(b0, d.b_mn_major, kk);
+        const uint64_t da = tile_desc<kBM>(a0, a_mn, kk);
+        const uint64_t db = tile_desc<BN>(b0, b_mn, kk);
         const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
-            "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            "l"(da), "l"(db), "r"(first ? idesc1 : idesc2), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        smem_u32(&bar[s]))

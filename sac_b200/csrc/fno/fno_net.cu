@@ -20,6 +20,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -28,6 +29,7 @@
 
 #include "fno_gemm.cuh"
 #include "fno_host.h"
+#include "fno_proj.cuh"
 #include "sac_fno.h"
 
 using namespace fno;
@@ -422,6 +424,38 @@ int forward(sac_fno* n, const bf16* x, float* y, int B, bool train) {
       d.err = n->errw;
       GK(d);
     }
+    // F5 and F6 in one GEMM where a 128-row tile of pixels lies in one row s (F a
+    // multiple of 128): z[b][o][p] = sum_i W[o][i] v[b][i][p] + sum_j' Hy[f][j'] Y[(b,o),s][j']
+    // + b[o] accumulates both products in the tile's TMEM accumulator, so the
+    // spectral term never goes to memory
+    const bool fused56 = F % kBM == 0;
+    if (fused56) {
+      GemmDesc d = gd((int)P, W, W, B);
+      a_chanfirst(d, v, W, P);
+      d.b = n->wb + n->sW[l].off;
+      d.b_n = W;
+      d.b_k = 1;
+      d.K2 = kJ;
+      d.a2 = n->Hy;  // A2(p, j') = Hy[p % F][j']
+      d.a2_msplit = F;
+      d.a2_m0 = kJ;
+      d.a2_k = 1;
+      d.b2 = n->yb;  // B2(o, j') = Y[(b,o)][s][j'], s = p0 / F for the tile at p0
+      d.b2_n = (long)S * kJ;
+      d.b2_k = 1;
+      d.b2_b = (long)W * S * kJ;
+      d.b2_m = kJ;
+      d.b2_mdiv = F;
+      c_chanfirst(d, n->act[l + 1], W, P, 1);
+      d.bias_n = n->w + n->sWb[l].off;
+      if (l < n->L - 1) {
+        d.act = ACT_GELU;
+        d.pre = train ? n->pre[l] : nullptr;
+      }
+      d.err = n->errw;
+      GK(d);
+      continue;
+    }
     // F5: spec[(b,o,s)][f] = sum_j' Y[(b,o,s)][j'] Hy[f][j']  (rows f)
     {
       GemmDesc d = gd(F, B * W * S, kJ);
@@ -455,7 +489,38 @@ int forward(sac_fno* n, const bf16* x, float* y, int B, bool train) {
       GK(d);
     }
   }
-  // projection: h = GELU(Q1 v_L + q1b), y = Q2 h + q2b
+  // projection: h = GELU(Q1 v_L + q1b), y = Q2 h + q2b; for inference in one
+  // kernel that keeps h on chip (fno_proj.cuh)
+  if (!train && H == kProjH && W <= kBK && W % 8 == 0 && n->cpad <= kProjN2 && P % 8 == 0) {
+    ProjArgs pa{};
+    pa.v = n->act[n->L];
+    pa.q1 = n->wb + n->sQ1.off;
+    pa.q1b = n->w + n->sQ1b.off;
+    pa.q2 = n->wb + n->sQ2.off;
+    pa.q2b = n->w + n->sQ2b.off;
+    pa.y = y;
+    pa.P = P;
+    pa.B = B;
+    pa.W = W;
+    pa.cout = n->cout;
+    pa.cpad = n->cpad;
+    pa.err = n->errw;
+    pa.wait_tries = n->wait_tries;
+    static int per_sm = 0;
+    if (!per_sm) {
+      FK(cudaFuncSetAttribute(k_proj_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kProjSmem));
+      FK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_proj_infer, kThreads, kProjSmem));
+      if (per_sm < 1) per_sm = 1;
+    }
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long ntiles = (P + kBM - 1) / kBM * B;
+    const unsigned grid = (unsigned)std::min<long>(ntiles, (long)nsm * per_sm);
+    k_proj_infer<<<grid, kThreads, kProjSmem, n->st>>>(pa);
+    FK(cudaGetLastError());
+    return 0;
+  }
   {
     GemmDesc d = gd((int)P, H, W, B);
     a_chanfirst(d, n->act[n->L], W, P);

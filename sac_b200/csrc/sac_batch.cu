@@ -82,6 +82,17 @@ struct sac_batch {
   double tune_three_ms = 0, tune_fused_ms = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // sac_batch_join: the lead (FP64) steps its partner (FP32) in the same launches;
+  // while joined the partner's work runs on the lead's stream (own_stream kept)
+  sac_batch* partner = nullptr;
+  sac_batch* lead = nullptr;
+  cudaStream_t own_stream = nullptr;
+  // the lead's join form: 0 = joint kernels (one launch per kernel over both
+  // batches), 1 = the two batches' own kernels on two branches of the graph;
+  // sac_batch_join times one stage in each and keeps the faster
+  int join_form = 0;
+  double join_ms[2] = {0.0, 0.0};
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool grid_set = false, bc_set = false, state_set = false, bc_init = false;
   std::vector<double> mindx2, dtgrav;
 };
@@ -163,24 +174,35 @@ std::vector<GhostChunk> make_ghosts(const std::vector<InstInfo>& in, int i0, int
   return out;
 }
 
-__global__ void kb_zero(InstDyn* dyn, int n, int what) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// the instance tables a per-instance kernel covers: a batch's own, or a joined
+// pair's (the lead's instances first)
+struct DynPair {
+  InstDyn* d[2];
+  int n[2];
+  __device__ __forceinline__ InstDyn* at(int i) const {
+    return i < n[0] ? d[0] + i : (i < n[0] + n[1] ? d[1] + (i - n[0]) : nullptr);
+  }
+  int total() const { return n[0] + n[1]; }
+};
+
+__global__ void kb_zero(DynPair dp, int what) {
+  InstDyn* D = dp.at(blockIdx.x * blockDim.x + threadIdx.x);
+  if (!D) return;
   if (what == 0) {
-    dyn[i].ctot[0] = dyn[i].ctot[1] = dyn[i].ctot[2] = 0ull;
+    D->ctot[0] = D->ctot[1] = D->ctot[2] = 0ull;
   } else {
-    dyn[i].courant = 0ull;
+    D->courant = 0ull;
   }
 }
 
 // the dt block of program vac per instance (src/vac.t:61-70): getdt_courant,
 // getdt_res (src/vacphys.mhdres.t:5-45), getdt_visc (src/vacusr.viscosity.t:509-542),
 // getdt_grav (fixed at itmin)
-__global__ void kb_dt(InstDyn* dyn, int n, int ndim, double courantpar, double dtpar, int visc, int grav,
-                      int cantgrow, double eta, double dtdiffpar) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  InstDyn& D = dyn[i];
+__global__ void kb_dt(DynPair dp, int ndim, double courantpar, double dtpar, int visc, int grav, int cantgrow,
+                      double eta, double dtdiffpar) {
+  InstDyn* Dp = dp.at(blockIdx.x * blockDim.x + threadIdx.x);
+  if (!Dp) return;
+  InstDyn& D = *Dp;
   double dt;
   if (dtpar > 0.0) {
     dt = dtpar;
@@ -211,12 +233,12 @@ __global__ void kb_dt(InstDyn* dyn, int n, int ndim, double courantpar, double d
   D.dt = dt;
 }
 
-__global__ void kb_time(InstDyn* dyn, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (dyn[i].dt == 0.0) return;  // finished at tmax
-  dyn[i].t += dyn[i].dt;
-  dyn[i].it += 1;
+__global__ void kb_time(DynPair dp) {
+  InstDyn* D = dp.at(blockIdx.x * blockDim.x + threadIdx.x);
+  if (!D) return;
+  if (D->dt == 0.0) return;  // finished at tmax
+  D->t += D->dt;
+  D->it += 1;
 }
 
 template <typename D>
@@ -304,12 +326,28 @@ Stage2Args stage_base(sac_batch* b) {
   return a;
 }
 
+BcArgs stage_bc(sac_batch* b, int s);
+BatchStageArgs stage_args(sac_batch* b, int s, const Tile* tiles, int n);
+
+// one fused RK stage s of batch b on b->stream: c_tot of the stage input, the
+// fused kernel, the boundary fill (with the RK4 combinations of stages 3 and 4)
+template <typename S>
+void enqueue_fused_stage(sac_batch* b, int s, bool visc) {
+  BatchStageArgs sa = stage_args(b, s, b->d_cour, b->n_cour);
+  if (visc) launch_batch_ctot<S>(sa, b->stream);
+  sa.tiles = b->d_fused;
+  sa.ntiles = b->n_fused;
+  launch_batch_stage2d<S>(sa, b->fused_shape, b->stream);
+  launch_bound_b<S>(b, stage_bc(b, s), b->np, b->d_gh_all, b->n_gh_all, b->d_dyn);
+}
+
 // one RK4 step of every instance, src/vac.t:439-455 (enqueued on b->stream)
 template <typename S>
 void enqueue_step(sac_batch* b) {
   const int nb = (b->ninst + 255) / 256;
   const int ngrav = grav_mod(b->par.user) ? 1 : 0;
-  kb_zero<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst, 1);
+  const DynPair dp{{b->d_dyn, nullptr}, {b->ninst, 0}};
+  kb_zero<<<nb, 256, 0, b->stream>>>(dp, 1);
   BatchStageArgs cb{};
   cb.a = stage_base(b);
   cb.a.wct = b->P[0];
@@ -318,46 +356,17 @@ void enqueue_step(sac_batch* b) {
   cb.tiles = b->d_cour;
   cb.ntiles = b->n_cour;
   launch_batch_courant<S>(cb, b->par.gamma, b->stream);
-  kb_dt<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst, b->ndim, b->par.courantpar, b->par.dtpar,
-                                   visc_on_b(b) ? 1 : 0, ngrav, b->par.dtcantgrow ? 1 : 0, b->par.eta,
-                                   b->par.dtdiffpar);
+  kb_dt<<<nb, 256, 0, b->stream>>>(dp, b->ndim, b->par.courantpar, b->par.dtpar, visc_on_b(b) ? 1 : 0, ngrav,
+                                   b->par.dtcantgrow ? 1 : 0, b->par.eta, b->par.dtdiffpar);
   void *w = b->P[0], *w1 = b->P[1], *w2 = b->P[2], *w3 = b->P[3];
   const void* wct[4] = {w, w1, w2, w3};
   void* out[4] = {w1, w2, w3, w};
   const int epi[4] = {EPI_PLAIN, EPI_PLAIN, EPI_RK4_S3, EPI_RK4_S4};
   const bool visc = visc_on_b(b);
   for (int s = 0; s < 4; ++s) {
-    kb_zero<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst, 0);
+    kb_zero<<<nb, 256, 0, b->stream>>>(dp, 0);
     if (b->fused) {
-      // c_tot of the stage input, then face, setnu and update in one kernel per tile
-      BatchStageArgs sa{};
-      sa.a = stage_base(b);
-      sa.a.wct = wct[s];
-      sa.a.base = w;
-      sa.a.out = out[s];
-      sa.a.aux1 = w1;
-      sa.a.aux2 = w2;
-      sa.a.epi = epi[s];
-      sa.inst = b->d_inst;
-      sa.dyn = b->d_dyn;
-      sa.stage = s;
-      sa.tiles = b->d_cour;
-      sa.ntiles = b->n_cour;
-      if (visc) launch_batch_ctot<S>(sa, b->stream);
-      sa.tiles = b->d_fused;
-      sa.ntiles = b->n_fused;
-      launch_batch_stage2d<S>(sa, b->fused_shape, b->stream);
-      BcArgs ba = bc_proto(b, out[s]);
-      if (epi[s] == EPI_RK4_S3) {
-        ba.mode = 1;
-        ba.aux1 = w1;
-        ba.aux2 = w2;
-        ba.basep = w;
-      } else if (epi[s] == EPI_RK4_S4) {
-        ba.mode = 2;
-        ba.aux1 = w1;
-      }
-      launch_bound_b<S>(b, ba, b->np, b->d_gh_all, b->n_gh_all, b->d_dyn);
+      enqueue_fused_stage<S>(b, s, visc);
       continue;
     }
     for (Group& gr : b->groups) {
@@ -396,18 +405,130 @@ void enqueue_step(sac_batch* b) {
       launch_bound_b<S>(b, ba, b->np, gr.d_gh, gr.n_gh, b->d_dyn);
     }
   }
-  kb_time<<<nb, 256, 0, b->stream>>>(b->d_dyn, b->ninst);
+  kb_time<<<nb, 256, 0, b->stream>>>(dp);
 }
 
-void drop_graph(sac_batch* b) {
+// the boundary-fill arguments of stage s (the RK4 combinations of stages 3 and 4
+// are fused into the fill, as in the stage's update)
+BcArgs stage_bc(sac_batch* b, int s) {
+  void* out[4] = {b->P[1], b->P[2], b->P[3], b->P[0]};
+  BcArgs ba = bc_proto(b, out[s]);
+  if (s == 2) {
+    ba.mode = 1;
+    ba.aux1 = b->P[1];
+    ba.aux2 = b->P[2];
+    ba.basep = b->P[0];
+  } else if (s == 3) {
+    ba.mode = 2;
+    ba.aux1 = b->P[1];
+  }
+  return ba;
+}
+
+// the fused-stage arguments of stage s over tile list (tiles, n)
+BatchStageArgs stage_args(sac_batch* b, int s, const Tile* tiles, int n) {
+  void *w = b->P[0], *w1 = b->P[1], *w2 = b->P[2], *w3 = b->P[3];
+  const void* wct[4] = {w, w1, w2, w3};
+  void* out[4] = {w1, w2, w3, w};
+  const int epi[4] = {EPI_PLAIN, EPI_PLAIN, EPI_RK4_S3, EPI_RK4_S4};
+  BatchStageArgs sa{};
+  sa.a = stage_base(b);
+  sa.a.wct = wct[s];
+  sa.a.base = w;
+  sa.a.out = out[s];
+  sa.a.aux1 = w1;
+  sa.a.aux2 = w2;
+  sa.a.epi = epi[s];
+  sa.inst = b->d_inst;
+  sa.dyn = b->d_dyn;
+  sa.stage = s;
+  sa.tiles = tiles;
+  sa.ntiles = n;
+  return sa;
+}
+
+// stage s of a joined pair in joint kernels (c_tot when with_ctot, the fused
+// stage, the boundary fill), on the lead's stream
+void enqueue_joint_stage(sac_batch* b, sac_batch* p, int s, bool with_ctot) {
+  cudaStream_t st = b->stream;
+  if (with_ctot) {
+    JointStageArgs jt{};
+    jt.b[0] = stage_args(b, s, b->d_cour, b->n_cour);
+    jt.b[1] = stage_args(p, s, p->d_cour, p->n_cour);
+    launch_joint_ctot(jt, st);
+  }
+  JointStageArgs js{};
+  js.b[0] = stage_args(b, s, b->d_fused, b->n_fused);
+  js.b[1] = stage_args(p, s, p->d_fused, p->n_fused);
+  launch_joint_stage2d(js, b->fused_shape, st);
+  JointBoundArgs jb{};
+  sac_batch* both[2] = {b, p};
+  for (int k = 0; k < 2; ++k) {
+    jb.proto[k] = stage_bc(both[k], s);
+    jb.inst[k] = both[k]->d_inst;
+    jb.chunks[k] = both[k]->d_gh_all;
+    jb.n[k] = both[k]->n_gh_all;
+    jb.dyn[k] = both[k]->d_dyn;
+  }
+  launch_joint_bound(jb, b->np, st);
+}
+
+// one RK4 step of the instances of a joined pair, every kernel covering both
+// batches: b holds the FP64 instances, p the FP32 ones (same parameters, both 2D
+// on the fused stage); the steps and their order are those of enqueue_step
+void enqueue_joint(sac_batch* b, sac_batch* p) {
+  const DynPair dp{{b->d_dyn, p->d_dyn}, {b->ninst, p->ninst}};
+  const int nb = (dp.total() + 255) / 256;
+  const int ngrav = grav_mod(b->par.user) ? 1 : 0;
+  cudaStream_t st = b->stream;
+  kb_zero<<<nb, 256, 0, st>>>(dp, 1);
+  JointStageArgs jc{};
+  jc.b[0] = stage_args(b, 0, b->d_cour, b->n_cour);
+  jc.b[1] = stage_args(p, 0, p->d_cour, p->n_cour);
+  launch_joint_courant(jc, b->par.gamma, st);
+  kb_dt<<<nb, 256, 0, st>>>(dp, b->ndim, b->par.courantpar, b->par.dtpar, visc_on_b(b) ? 1 : 0, ngrav,
+                            b->par.dtcantgrow ? 1 : 0, b->par.eta, b->par.dtdiffpar);
+  const bool visc = visc_on_b(b);
+  for (int s = 0; s < 4; ++s) {
+    kb_zero<<<nb, 256, 0, st>>>(dp, 0);
+    enqueue_joint_stage(b, p, s, visc);
+  }
+  kb_time<<<nb, 256, 0, st>>>(dp);
+}
+
+// one RK4 step of a joined pair as two branches of the graph: the partner's own
+// kernels on its own stream beside the lead's (both forked from and joined back
+// to the lead's stream)
+void enqueue_forked(sac_batch* b, sac_batch* p) {
+  cudaEventRecord(b->ev_fork, b->stream);
+  cudaStreamWaitEvent(p->own_stream, b->ev_fork, 0);
+  p->stream = p->own_stream;
+  enqueue_step<float>(p);
+  p->stream = b->stream;
+  cudaEventRecord(b->ev_join, p->own_stream);
+  enqueue_step<double>(b);
+  cudaStreamWaitEvent(b->stream, b->ev_join, 0);
+}
+
+void drop_exec(sac_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec), b->exec = nullptr;
   if (b->graph) cudaGraphDestroy(b->graph), b->graph = nullptr;
+}
+
+// a batch's graph, and the joint graph that also reads its arrays
+void drop_graph(sac_batch* b) {
+  drop_exec(b);
+  if (b->lead) drop_exec(b->lead);
 }
 
 sac_status build_graph(sac_batch* b) {
   drop_graph(b);
   BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-  if (b->prec == SAC_PREC_FP32)
+  if (b->partner && b->join_form == 1)
+    enqueue_forked(b, b->partner);
+  else if (b->partner)
+    enqueue_joint(b, b->partner);
+  else if (b->prec == SAC_PREC_FP32)
     enqueue_step<float>(b);
   else
     enqueue_step<double>(b);
@@ -447,6 +568,73 @@ sac_status build_lists(sac_batch* b) {
   }
   return SAC_OK;
 }
+
+// the parameters two joined batches share: all but the precision
+bool same_family(const sac_batch* a, const sac_batch* b) {
+  const sac_params &x = a->par, &y = b->par;
+  if (a->ndim != b->ndim || a->ndir != b->ndir || a->dev != b->dev) return false;
+  if (x.gamma != y.gamma || x.eta != y.eta || x.nu != y.nu || x.courantpar != y.courantpar || x.dtpar != y.dtpar ||
+      x.dtdiffpar != y.dtdiffpar || x.dtcantgrow != y.dtcantgrow || x.sourceunsplit != y.sourceunsplit ||
+      x.divbfix != y.divbfix || x.user != y.user || x.alias_nu_grav3 != y.alias_nu_grav3)
+    return false;
+  for (int d = 0; d < 3; ++d)
+    if (x.grav[d] != y.grav[d]) return false;
+  for (int i = 0; i < 16; ++i)
+    if (x.userpar[i] != y.userpar[i]) return false;
+  return std::strcmp(x.typeadvance, y.typeadvance) == 0;
+}
+
+// ms of one RK stage of a joined pair in form f (stage 0: it reads w and writes
+// the scratch w1 only), on the lead's stream, after one untimed run
+double join_stage_ms(sac_batch* b, sac_batch* p, int f, cudaEvent_t e0, cudaEvent_t e1) {
+  const bool visc = visc_on_b(b);
+  auto zero = [](sac_batch* x, InstDyn* d2, int n2) {
+    const DynPair dp{{x->d_dyn, d2}, {x->ninst, n2}};
+    kb_zero<<<(dp.total() + 255) / 256, 256, 0, x->stream>>>(dp, 0);
+  };
+  auto run = [&]() {
+    if (f == 0) {
+      zero(b, p->d_dyn, p->ninst);
+      enqueue_joint_stage(b, p, 0, visc);
+      return;
+    }
+    cudaEventRecord(b->ev_fork, b->stream);
+    cudaStreamWaitEvent(p->own_stream, b->ev_fork, 0);
+    p->stream = p->own_stream;
+    zero(p, nullptr, 0);
+    enqueue_fused_stage<float>(p, 0, visc);
+    p->stream = b->stream;
+    cudaEventRecord(b->ev_join, p->own_stream);
+    zero(b, nullptr, 0);
+    enqueue_fused_stage<double>(b, 0, visc);
+    cudaStreamWaitEvent(b->stream, b->ev_join, 0);
+  };
+  run();
+  cudaEventRecord(e0, b->stream);
+  for (int r = 0; r < 3; ++r) run();
+  cudaEventRecord(e1, b->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  return ms / 3;
+}
+
+// ends a join (lead: the FP64 batch); the partner gets its own stream back
+void unjoin(sac_batch* lead) {
+  sac_batch* p = lead->partner;
+  if (!p) return;
+  cudaSetDevice(lead->dev);
+  cudaStreamSynchronize(lead->stream);
+  drop_exec(lead);
+  if (lead->ev_fork) cudaEventDestroy(lead->ev_fork), lead->ev_fork = nullptr;
+  if (lead->ev_join) cudaEventDestroy(lead->ev_join), lead->ev_join = nullptr;
+  p->stream = p->own_stream;
+  p->own_stream = nullptr;
+  p->lead = nullptr;
+  lead->partner = nullptr;
+}
+
+bool joined(const sac_batch* b) { return b->lead || b->partner; }
 
 // frees the device arrays; the group ranges stay (they depend on the sizes only)
 void free_all(sac_batch* b) {
@@ -547,6 +735,8 @@ sac_status sac_batch_create(const sac_params* p, int ndim, int ndir, int ninst, 
 
 void sac_batch_destroy(sac_batch* b) {
   if (!b) return;
+  if (b->partner) unjoin(b);
+  if (b->lead) unjoin(b->lead);
   cudaSetDevice(b->dev);
   if (b->stream) cudaStreamSynchronize(b->stream);
   free_all(b);
@@ -559,6 +749,7 @@ const char* sac_batch_last_error(const sac_batch* b) { return b ? b->err.c_str()
 // x: the instances' full-grid coordinate blocks x(ixG^T,ndim) one after another
 sac_status sac_batch_set_grid(sac_batch* b, const double* x) {
   if (!b || !x) return SAC_ERR_ARG;
+  if (joined(b)) return bfail(b, SAC_ERR_STATE, "sac_batch_unjoin first");
   BK(cudaSetDevice(b->dev));
   const int ndim = b->ndim;
   std::vector<double> hdx((size_t)ndim * b->totX);
@@ -654,6 +845,7 @@ sac_status sac_batch_set_grid(sac_batch* b, const double* x) {
 // (fixed, fixed1, grad1) are not available in the batch
 sac_status sac_batch_set_boundaries(sac_batch* b, const char* typeB) {
   if (!b || !typeB) return SAC_ERR_ARG;
+  if (joined(b)) return bfail(b, SAC_ERR_STATE, "sac_batch_unjoin first");
   if (!b->grid_set) return bfail(b, SAC_ERR_STATE, "sac_batch_set_grid first");
   BK(cudaSetDevice(b->dev));
   const int nB = 2 * b->ndim;
@@ -785,6 +977,7 @@ sac_status sac_batch_getboundary(sac_batch* b) {
 sac_status sac_batch_advance(sac_batch* b, int nsteps) {
   if (!b || nsteps < 0) return SAC_ERR_ARG;
   if (!b->bc_init) return bfail(b, SAC_ERR_STATE, "call sac_batch_getboundary first");
+  if (b->lead) return bfail(b, SAC_ERR_STATE, "joined: sac_batch_advance on the FP64 batch advances this one");
   BK(cudaSetDevice(b->dev));
   if (!b->exec) {
     sac_status st = build_graph(b);
@@ -827,6 +1020,7 @@ void* sac_batch_get_stream(const sac_batch* b) { return b ? (void*)b->stream : n
 // tile_out[2] receives the chosen shape, ms_out the time per update pass.
 sac_status sac_batch_tune(sac_batch* b, int* tile_out, double* ms_out) {
   if (!b) return SAC_ERR_ARG;
+  if (joined(b)) return bfail(b, SAC_ERR_STATE, "tune each batch before sac_batch_join");
   if (!b->bc_init) return bfail(b, SAC_ERR_STATE, "call sac_batch_getboundary first");
   BK(cudaSetDevice(b->dev));
   const dim3 cands[] = {dim3(32, 4, 1), dim3(32, 8, 1), dim3(64, 4, 1), dim3(16, 16, 1), dim3(128, 2, 1),
@@ -979,6 +1173,7 @@ sac_status sac_batch_tune(sac_batch* b, int* tile_out, double* ms_out) {
 // setnu / update passes
 sac_status sac_batch_set_stage(sac_batch* b, int fused, int shape) {
   if (!b) return SAC_ERR_ARG;
+  if (joined(b)) return bfail(b, SAC_ERR_STATE, "joined batches keep the fused stage; sac_batch_unjoin first");
   if (fused && !fused_ok(b))
     return bfail(b, SAC_ERR_UNSUPPORTED, "the fused stage covers 2D instances without Powell's or the resistive term");
   if (shape < 0 || shape >= kStage2dShapeCount) return bfail(b, SAC_ERR_ARG, "no such tile shape");
@@ -995,6 +1190,87 @@ sac_status sac_batch_set_stage(sac_batch* b, int fused, int shape) {
 
 // the stage form in use: fused (0/1), its tile shape, and the tuner's timings of
 // one stage (three passes, fused; 0 before sac_batch_tune)
+sac_status sac_batch_join(sac_batch* lead, sac_batch* partner) {
+  if (!lead || !partner || lead == partner) return SAC_ERR_ARG;
+  if (joined(lead) || joined(partner)) return bfail(lead, SAC_ERR_STATE, "a batch is joined already");
+  if (lead->prec != SAC_PREC_FP64 || partner->prec != SAC_PREC_FP32)
+    return bfail(lead, SAC_ERR_ARG, "the lead holds FP64 instances and the partner FP32 ones");
+  if (!same_family(lead, partner))
+    return bfail(lead, SAC_ERR_ARG, "joined batches need the same parameters, ndim, ndir and device");
+  if (!fused_ok(lead))
+    return bfail(lead, SAC_ERR_UNSUPPORTED,
+                 "joined batches run the fused stage: 2D instances without Powell's or the resistive term");
+  if (!lead->bc_init || !partner->bc_init)
+    return bfail(lead, SAC_ERR_STATE, "call sac_batch_getboundary on both batches first");
+  sac_batch* b = lead;  // BK reports on the lead
+  BK(cudaSetDevice(lead->dev));
+  BK(cudaStreamSynchronize(lead->stream));
+  BK(cudaStreamSynchronize(partner->stream));
+  const int shape = lead->fused_shape;
+  for (sac_batch* x : {lead, partner}) {
+    if (!x->fused || x->fused_shape != shape) {
+      x->fused = true;
+      x->fused_shape = shape;
+      sac_status st = build_lists(x);
+      if (st != SAC_OK) return bfail(lead, st, x->err);
+    }
+    drop_exec(x);
+  }
+  BK(cudaEventCreateWithFlags(&lead->ev_fork, cudaEventDisableTiming));
+  BK(cudaEventCreateWithFlags(&lead->ev_join, cudaEventDisableTiming));
+  partner->own_stream = partner->stream;
+  partner->stream = lead->stream;
+  partner->lead = lead;
+  lead->partner = partner;
+  // time one stage in both forms and keep the faster.  The stage kernels skip
+  // instances with dt = 0 (before the first step): time them with a tiny
+  // nonzero dt, then restore both instance tables (c_tot and max nu included)
+  std::vector<InstDyn> save[2], tmp[2];
+  sac_batch* both[2] = {lead, partner};
+  for (int k = 0; k < 2; ++k) {
+    save[k].resize(both[k]->ninst);
+    BK(cudaMemcpy(save[k].data(), both[k]->d_dyn, sizeof(InstDyn) * both[k]->ninst, cudaMemcpyDeviceToHost));
+    tmp[k] = save[k];
+    for (auto& d : tmp[k])
+      if (d.dt == 0.0) d.dt = 1e-300;
+    BK(cudaMemcpy(both[k]->d_dyn, tmp[k].data(), sizeof(InstDyn) * both[k]->ninst, cudaMemcpyHostToDevice));
+  }
+  cudaEvent_t e0, e1;
+  BK(cudaEventCreate(&e0));
+  BK(cudaEventCreate(&e1));
+  for (int f = 0; f < 2; ++f) lead->join_ms[f] = join_stage_ms(lead, partner, f, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  BK(cudaGetLastError());
+  for (int k = 0; k < 2; ++k)
+    BK(cudaMemcpy(both[k]->d_dyn, save[k].data(), sizeof(InstDyn) * both[k]->ninst, cudaMemcpyHostToDevice));
+  lead->join_form = lead->join_ms[1] < lead->join_ms[0] ? 1 : 0;
+  return SAC_OK;
+}
+
+sac_status sac_batch_set_join_form(sac_batch* lead, int form) {
+  if (!lead || form < 0 || form > 1) return SAC_ERR_ARG;
+  if (!lead->partner) return bfail(lead, SAC_ERR_STATE, "not the lead of a joined pair");
+  lead->join_form = form;
+  drop_exec(lead);
+  return SAC_OK;
+}
+
+sac_status sac_batch_get_join(const sac_batch* lead, int* form, double* ms_joint, double* ms_forked) {
+  if (!lead) return SAC_ERR_ARG;
+  if (form) *form = lead->partner ? lead->join_form : -1;
+  if (ms_joint) *ms_joint = lead->join_ms[0];
+  if (ms_forked) *ms_forked = lead->join_ms[1];
+  return SAC_OK;
+}
+
+sac_status sac_batch_unjoin(sac_batch* lead) {
+  if (!lead) return SAC_ERR_ARG;
+  if (lead->lead) return bfail(lead, SAC_ERR_STATE, "sac_batch_unjoin takes the FP64 batch of the pair");
+  unjoin(lead);
+  return SAC_OK;
+}
+
 sac_status sac_batch_get_stage(const sac_batch* b, int* fused, int* shape, double* ms_three, double* ms_fused) {
   if (!b) return SAC_ERR_ARG;
   if (fused) *fused = b->fused ? 1 : 0;

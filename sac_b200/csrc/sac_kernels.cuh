@@ -417,14 +417,14 @@ __global__ void k_bound(const __grid_constant__ BcArgs a, long nslab0, long nsla
 // batched: persistent CTAs of 256 threads walk the ghost chunks of all instances.
 // The instance's arguments live in shared memory, written once per chunk by one
 // thread: a per-thread copy would put the whole struct on every thread's stack.
+// One chunk t per call (a whole block); a: the block's shared copy.
 template <typename S>
-__global__ void __launch_bounds__(256) kb_bound(const __grid_constant__ BcArgs proto, const InstInfo* __restrict__ inst,
-                                                const GhostChunk* __restrict__ chunks, int nchunks, int nvar,
-                                                const InstDyn* __restrict__ dyn) {
-  __shared__ BcArgs a;
-  for (int t = blockIdx.x; t < nchunks; t += gridDim.x) {
+__device__ __forceinline__ void bound_chunk(const BcArgs& proto, const InstInfo* __restrict__ inst,
+                                            const GhostChunk* __restrict__ chunks, int t, int nvar,
+                                            const InstDyn* __restrict__ dyn, BcArgs& a) {
+  {
     const GhostChunk ch = chunks[t];
-    if (dyn && dyn[ch.inst].dt == 0.0) continue;  // a finished instance keeps its state (uniform per block)
+    if (dyn && dyn[ch.inst].dt == 0.0) return;  // a finished instance keeps its state (uniform per block)
     __syncthreads();  // the previous chunk's readers are done with a
     if (threadIdx.x == 0) {
       a = proto;
@@ -444,6 +444,14 @@ __global__ void __launch_bounds__(256) kb_bound(const __grid_constant__ BcArgs p
     const long k = (long)ch.start + threadIdx.x;
     if (k < ns[0] + ns[1] + ns[2]) bound_cell<S>(a, k, ns, 0, nvar);
   }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) kb_bound(const __grid_constant__ BcArgs proto, const InstInfo* __restrict__ inst,
+                                                const GhostChunk* __restrict__ chunks, int nchunks, int nvar,
+                                                const InstDyn* __restrict__ dyn) {
+  __shared__ BcArgs a;
+  for (int t = blockIdx.x; t < nchunks; t += gridDim.x) bound_chunk<S>(proto, inst, chunks, t, nvar, dyn, a);
 }
 
 // Store fixB of region (d,up) for variable iw after the first fill

@@ -955,15 +955,15 @@ __global__ void __launch_bounds__(256, sizeof(S) == 8 ? SAC_BATCH_UPDATE_MINB_F6
   }
 }
 
-// getdt_courant per instance: max over its mesh of cmax/dx (src/vac.t:667-694)
+// getdt_courant per instance: max over its mesh of cmax/dx (src/vac.t:667-694),
+// for tile t of b's list (a whole block; sh: 32 doubles of shared memory)
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256) kb_courant(const BatchStageArgs b, double gamma) {
-  __shared__ double sh[32];
+__device__ __forceinline__ void courant_tile(const BatchStageArgs& b, int t, double gamma, double* sh) {
   constexpr int E = NDIR + 1;
-  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+  {
     const Tile tl = b.tiles[t];
     const InstDyn& Dy = b.dyn[tl.inst];
-    if (Dy.tmax > 0.0 && Dy.t >= Dy.tmax) continue;  // finished: its dt will be 0
+    if (Dy.tmax > 0.0 && Dy.t >= Dy.tmax) return;  // finished: its dt will be 0
     const InstInfo I = b.inst[tl.inst];  // a register copy: stores cannot alias it
     const Geom& g = I.g;
     int p[3];
@@ -1003,6 +1003,12 @@ __global__ void __launch_bounds__(256) kb_courant(const BatchStageArgs b, double
     }
     block_max_to(&b.dyn[tl.inst].courant, best, sh);
   }
+}
+
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) kb_courant(const BatchStageArgs b, double gamma) {
+  __shared__ double sh[32];
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) courant_tile<NDIM, NDIR, S>(b, t, gamma, sh);
 }
 
 // ---------------------------------------------------------------------------

@@ -56,11 +56,10 @@ struct Tile2D {
 // c_tot of the stage per instance: getcmax's maxima over the mesh of the stage
 // input, the k_face arithmetic (face_eval with no fluxes), one atomic per block
 template <int NDIM, int NDIR, typename S>
-__global__ void __launch_bounds__(256) kb_ctot(const __grid_constant__ BatchStageArgs b, double gamma) {
-  __shared__ double sh[32];
-  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+__device__ __forceinline__ void ctot_tile(const BatchStageArgs& b, int t, double gamma, double* sh) {
+  {
     const Tile tl = b.tiles[t];
-    if (b.dyn[tl.inst].dt == 0.0) continue;  // finished (tmax): nothing to compute
+    if (b.dyn[tl.inst].dt == 0.0) return;  // finished (tmax): nothing to compute
     const InstInfo I = b.inst[tl.inst];
     const Geom& g = I.g;
     int p[3];
@@ -76,21 +75,26 @@ __global__ void __launch_bounds__(256) kb_ctot(const __grid_constant__ BatchStag
   }
 }
 
-// the fused stage over a tile list of 2D instances (blockDim = TX*TY threads)
+template <int NDIM, int NDIR, typename S>
+__global__ void __launch_bounds__(256) kb_ctot(const __grid_constant__ BatchStageArgs b, double gamma) {
+  __shared__ double sh[32];
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) ctot_tile<NDIM, NDIR, S>(b, t, gamma, sh);
+}
+
+// the fused stage of tile t of a tile list of 2D instances (a whole block of
+// TX*TY threads; smraw: the tile memory, shred: 32 doubles of shared memory)
 template <int NDIR, typename S, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY) kb_stage2d(const __grid_constant__ BatchStageArgs b) {
+__device__ __forceinline__ void stage2d_tile(const BatchStageArgs& b, int t, unsigned char* smraw, double* shred) {
   using L = Tile2D<NDIR, S, TX, TY>;
   constexpr int NDIM = 2, H = L::H, BW = L::BW, BH = L::BH, NT = TX * TY;
   constexpr int E = NDIR + 1;
-  extern __shared__ __align__(16) unsigned char smraw[];
   S* sm = reinterpret_cast<S*>(smraw);
-  __shared__ double shred[32];
   const int tid = threadIdx.x;
-  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+  {
     const Tile tl = b.tiles[t];
     const InstDyn& Dy = b.dyn[tl.inst];
     const bool live = Dy.dt != 0.0;  // uniform over the block
-    if (!live) continue;
+    if (!live) return;
     const InstInfo I = b.inst[tl.inst];
     const Geom& g = I.g;
     const int x0 = tl.p[0], y0 = tl.p[1];  // the tile's first mesh cell
@@ -201,6 +205,13 @@ __global__ void __launch_bounds__(TX * TY) kb_stage2d(const __grid_constant__ Ba
     }
     if (b.a.visc_on) block_max_to(&b.dyn[tl.inst].maxnu, numax, shred);
   }
+}
+
+template <int NDIR, typename S, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY) kb_stage2d(const __grid_constant__ BatchStageArgs b) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ double shred[32];
+  for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) stage2d_tile<NDIR, S, TX, TY>(b, t, smraw, shred);
 }
 
 // shared-memory bytes of the fused 2D stage for a tile shape

@@ -138,6 +138,23 @@ extern template void launch_batch_ctot<float>(const BatchStageArgs&, cudaStream_
 extern template cudaError_t launch_batch_stage2d<double>(const BatchStageArgs&, int, cudaStream_t);
 extern template cudaError_t launch_batch_stage2d<float>(const BatchStageArgs&, int, cudaStream_t);
 
+// two batches stepped together (stage_joint.cu): b[0] holds FP64 instances, b[1]
+// FP32 ones; each kernel walks b[0]'s tiles, then b[1]'s
+struct JointStageArgs {
+  BatchStageArgs b[2];
+};
+struct JointBoundArgs {
+  BcArgs proto[2];
+  const InstInfo* inst[2];
+  const GhostChunk* chunks[2];
+  int n[2];
+  const InstDyn* dyn[2];
+};
+void launch_joint_courant(const JointStageArgs& j, double gamma, cudaStream_t st);
+void launch_joint_ctot(const JointStageArgs& j, cudaStream_t st);
+cudaError_t launch_joint_stage2d(const JointStageArgs& j, int shape, cudaStream_t st);
+void launch_joint_bound(const JointBoundArgs& j, int nvar, cudaStream_t st);
+
 extern template void launch_batch_face<double>(const BatchStageArgs&, double, cudaStream_t);
 extern template void launch_batch_face<float>(const BatchStageArgs&, double, cudaStream_t);
 extern template void launch_batch_nu<double>(const BatchStageArgs&, cudaStream_t);

@@ -23,6 +23,11 @@ class GemmDesc(ctypes.Structure):
         ("c_b", ctypes.c_long), ("c_msplit", ctypes.c_int), ("c_bf16", ctypes.c_int), ("c_mode", ctypes.c_int),
         ("alpha", ctypes.c_float), ("bias_n", VP), ("add", VP), ("act", ctypes.c_int), ("pre", VP),
         ("err", VP), ("b_n1", ctypes.c_long), ("b_nsplit", ctypes.c_int), ("wait_tries", ctypes.c_int),
+        ("K2", ctypes.c_int), ("a2_msplit", ctypes.c_int), ("a2_mn_major", ctypes.c_int),
+        ("a2", VP), ("a2_m0", ctypes.c_long), ("a2_m1", ctypes.c_long), ("a2_k", ctypes.c_long),
+        ("a2_b", ctypes.c_long),
+        ("b2", VP), ("b2_n", ctypes.c_long), ("b2_k", ctypes.c_long), ("b2_b", ctypes.c_long),
+        ("b2_m", ctypes.c_long), ("b2_mn_major", ctypes.c_int), ("b2_mdiv", ctypes.c_int),
     ]
 
 
@@ -58,8 +63,9 @@ def gemm(M, N, K, a, b, c, *, batch=1, ksplit=1, a_m0=None, a_m1=0, a_k=1, a_b=0
          a_mn_major=False, b_n=None, b_k=1, b_b=0, b_mn_major=False, b_n1=0, b_nsplit=None,
          c_m0=None, c_m1=0, c_n=1, c_b=0,
          c_msplit=None, c_bf16=False, c_mode=0, alpha=1.0, bias_n=0, add=0, act=0, pre=0, err=0, stream=0,
-         wait_tries=0):
-    """Thin call of sac_fno_gemm with integer device pointers (0 = none)."""
+         wait_tries=0, second=None):
+    """Thin call of sac_fno_gemm with integer device pointers (0 = none).  second:
+    a dict of the second product's fields (K2, a2, b2, a2_m0, ... b2_mdiv)."""
     lib = load()
     d = GemmDesc()
     d.M, d.N, d.K, d.batch, d.ksplit = M, N, K, batch, ksplit
@@ -80,6 +86,10 @@ def gemm(M, N, K, a, b, c, *, batch=1, ksplit=1, a_m0=None, a_m1=0, a_k=1, a_b=0
     d.c_bf16, d.c_mode, d.alpha = int(bool(c_bf16)), c_mode, alpha
     d.bias_n, d.add, d.act, d.pre, d.err = bias_n or None, add or None, act, pre or None, err or None
     d.wait_tries = wait_tries
+    if second:
+        d.a2_msplit = 1 << 30
+        for k, v in second.items():
+            setattr(d, k, int(v))
     check(lib.sac_fno_gemm(ctypes.byref(d), VP(stream) if stream else None), lib)
 
 

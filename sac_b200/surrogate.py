@@ -71,6 +71,7 @@ def make_solver(A, om, n=(256, 256), dtpar=None, precision=params.PREC_FP32, gro
         b.upload(np.concatenate([w0] * k), i0, k)
     b.set_driver(A, om)
     b.getboundary()
+    b.tune()  # the stage form and tile the batch runs fastest with (the fused 2D stage)
     return b, P0
 
 

@@ -1,7 +1,12 @@
 """The FNO of libsacfno.so (tcgen05 forward and backward kernels) against the
 float64 CPU oracle (oracle/fno_ref.py) on the same BF16-rounded weights and
 inputs.  The GPU keeps activations in BF16 and its DFT tables in BF16, so the
-bar is a relative L2 of 2e-2 on the output and 5e-2 per gradient group."""
+bar is a relative L2 of 2e-2 on the output and 5e-2 per gradient group.
+
+Two shapes: CFG, where every layer runs as separate GEMMs, and WIDE (F a multiple
+of 128, hidden 128), where each Fourier layer accumulates its spectral term into
+the channel-mixing GEMM's tile and inference runs the projection in one kernel
+that keeps the hidden channels on chip."""
 import numpy as np
 import pytest
 
@@ -13,6 +18,8 @@ from sac_b200 import build, fno_abi  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 CFG = dict(S=64, F=64, width=32, layers=2, hidden=32, cin=16, cout=6)
+WIDE = dict(S=64, F=128, width=32, layers=2, hidden=128, cin=16, cout=6)
+SHAPES = pytest.mark.parametrize("cfg", [CFG, WIDE], ids=["separate", "fused"])
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -20,13 +27,13 @@ def _lib():
     build.build_fno()
 
 
-def _net(B=2, seed=3):
-    return fno_abi.Net(max_batch=B, seed=seed, **CFG)
+def _net(B=2, seed=3, cfg=CFG):
+    return fno_abi.Net(max_batch=B, seed=seed, **cfg)
 
 
-def _layout():
-    return fno_ref.Layout(width=CFG["width"], layers=CFG["layers"], cin=CFG["cin"], cout=CFG["cout"],
-                          hidden=CFG["hidden"])
+def _layout(cfg=CFG):
+    return fno_ref.Layout(width=cfg["width"], layers=cfg["layers"], cin=cfg["cin"], cout=cfg["cout"],
+                          hidden=cfg["hidden"])
 
 
 def _oracle_theta(net, lay):
@@ -43,9 +50,9 @@ def _rel(a, b):
     return np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-30)
 
 
-def _inputs(B, seed):
+def _inputs(B, seed, cfg=CFG):
     g = torch.Generator().manual_seed(seed)
-    x = torch.randn(B, CFG["cin"], CFG["S"], CFG["F"], generator=g).to(torch.bfloat16)
+    x = torch.randn(B, cfg["cin"], cfg["S"], cfg["F"], generator=g).to(torch.bfloat16)
     return x
 
 
@@ -59,12 +66,13 @@ def test_layout_matches_the_oracle():
     assert net.nparam == lay.n
 
 
-def test_forward_matches_oracle():
+@SHAPES
+def test_forward_matches_oracle(cfg):
     B = 2
-    net, lay = _net(B), _layout()
-    x = _inputs(B, 1)
+    net, lay = _net(B, cfg=cfg), _layout(cfg)
+    x = _inputs(B, 1, cfg)
     xd = x.cuda()
-    y = torch.zeros(B, CFG["cout"], CFG["S"], CFG["F"], device="cuda")
+    y = torch.zeros(B, cfg["cout"], cfg["S"], cfg["F"], device="cuda")
     torch.cuda.synchronize()
     net.forward(xd.data_ptr(), y.data_ptr(), B)
     net.check()
@@ -73,16 +81,17 @@ def test_forward_matches_oracle():
     assert err < 2e-2, err
 
 
-def test_gradients_match_oracle():
+@SHAPES
+def test_gradients_match_oracle(cfg):
     B = 2
-    net, lay = _net(B), _layout()
-    x = _inputs(B, 2)
+    net, lay = _net(B, cfg=cfg), _layout(cfg)
+    x = _inputs(B, 2, cfg)
     g = torch.Generator().manual_seed(5)
-    dy = torch.zeros(B, net.cpad, CFG["S"], CFG["F"])
-    dy[:, :CFG["cout"]] = torch.randn(B, CFG["cout"], CFG["S"], CFG["F"], generator=g)
+    dy = torch.zeros(B, net.cpad, cfg["S"], cfg["F"])
+    dy[:, :cfg["cout"]] = torch.randn(B, cfg["cout"], cfg["S"], cfg["F"], generator=g)
     dy = dy.to(torch.bfloat16)
     xd, dyd = x.cuda(), dy.cuda()
-    y = torch.zeros(B, CFG["cout"], CFG["S"], CFG["F"], device="cuda")
+    y = torch.zeros(B, cfg["cout"], cfg["S"], cfg["F"], device="cuda")
     torch.cuda.synchronize()
     net.zero_grad()
     net.forward(xd.data_ptr(), y.data_ptr(), B)
@@ -91,10 +100,10 @@ def test_gradients_match_oracle():
     ggpu = net.get_grads().astype(np.float64)
     th = _oracle_theta(net, lay)
     _, tape = fno_ref.forward(lay, th, x.double().numpy())
-    go = fno_ref.backward(lay, th, tape, dy[:, :CFG["cout"]].double().numpy())
+    go = fno_ref.backward(lay, th, tape, dy[:, :cfg["cout"]].double().numpy())
     for name, (o, n) in lay.segs.items():
         if name in ("Q2", "Q2b"):
-            n = CFG["cout"] * (CFG["hidden"] if name == "Q2" else 1)
+            n = cfg["cout"] * (cfg["hidden"] if name == "Q2" else 1)
         err = _rel(ggpu[o:o + n], go[o:o + n])
         assert err < 5e-2, (name, err)
 
@@ -126,13 +135,16 @@ def test_adam_training_reduces_the_loss():
     assert losses[-1] < 0.2 * losses[0], losses[::10]
 
 
-def test_inference_pass_equals_training_forward():
+@SHAPES
+def test_inference_pass_equals_training_forward(cfg):
+    # WIDE: the fused projection rounds the hidden channels to BF16 and sums them
+    # in the same order as the two GEMMs of the training forward
     B = 2
-    net = _net(B)
-    xd = _inputs(B, 4).cuda()
-    y1 = torch.zeros(B, CFG["cout"], CFG["S"], CFG["F"], device="cuda")
+    net = _net(B, cfg=cfg)
+    xd = _inputs(B, 4, cfg).cuda()
+    y1 = torch.zeros(B, cfg["cout"], cfg["S"], cfg["F"], device="cuda")
     y2 = torch.zeros_like(y1)
-    dy = torch.zeros(B, net.cpad, CFG["S"], CFG["F"], dtype=torch.bfloat16, device="cuda")
+    dy = torch.zeros(B, net.cpad, cfg["S"], cfg["F"], dtype=torch.bfloat16, device="cuda")
     torch.cuda.synchronize()
     net.forward(xd.data_ptr(), y1.data_ptr(), B)
     net.infer(xd.data_ptr(), y2.data_ptr(), B)

@@ -75,6 +75,43 @@ def test_split_rows_batches_and_transposed_store():
         _close(c[z], ref, _scale(A, b[z]).reshape(G, S, N).permute(0, 2, 1))
 
 
+@pytest.mark.parametrize("K,K2,amn", [(32, 48, True), (64, 40, False), (16, 136, True)])
+def test_second_product_accumulates_into_the_tile(K, K2, amn):
+    # C[z][n][p] = sum_k A[z][k][p] B[n][k] + sum_j A2[p % F][j] B2[z][n][p // F][j]: the
+    # fused spectral term of a Fourier layer, B2's block chosen by the tile's row
+    nb, F, S, N = 2, 256, 3, 32
+    M = S * F
+    a = _bf((nb, K, M), 11) if amn else _bf((nb, M, K), 11)
+    b = _bf((N, K), 12)
+    a2 = _bf((F, K2), 13)
+    b2 = _bf((nb, N, S, K2), 14)
+    c = torch.zeros(nb, N, M, dtype=torch.float32, device="cuda")
+    kw = dict(a_mn_major=True, a_m0=1, a_k=M, a_b=K * M) if amn else dict(a_m0=K, a_b=M * K)
+    fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), c.data_ptr(), batch=nb, b_n=K, c_m0=1, c_n=M, c_b=N * M,
+                 second=dict(K2=K2, a2=a2.data_ptr(), a2_msplit=F, a2_m0=K2, a2_k=1, b2=b2.data_ptr(),
+                             b2_n=S * K2, b2_k=1, b2_b=N * S * K2, b2_m=K2, b2_mdiv=F), **kw)
+    torch.cuda.synchronize()
+    for z in range(nb):
+        A = a[z].T if amn else a[z]  # M x K
+        A2 = a2.repeat(S, 1)  # row p -> A2[p % F]
+        B2 = b2[z].permute(1, 0, 2)  # S x N x K2
+        ref = _ref(A, b) + torch.cat([_ref(A2[s * F:(s + 1) * F], B2[s]) for s in range(S)])
+        sc = _scale(A, b) + torch.cat([_scale(A2[s * F:(s + 1) * F], B2[s]) for s in range(S)])
+        _close(c[z].T, ref, sc)
+
+
+def test_second_product_argument_checks():
+    a, b = _bf((256, 32), 1), _bf((32, 32), 2)
+    a2, b2 = _bf((256, 48), 3), _bf((32, 48), 4)
+    c = torch.zeros(256, 32, dtype=torch.float32, device="cuda")
+    base = dict(K2=48, a2=a2.data_ptr(), a2_m0=48, a2_k=1, b2=b2.data_ptr(), b2_n=48, b2_k=1, b2_mdiv=256)
+    for bad in (dict(b2_mdiv=200), dict(K2=44), dict(b2=0), dict(a2_k=2)):
+        with pytest.raises(fno_abi.FnoError):
+            fno_abi.gemm(256, 32, 32, a.data_ptr(), b.data_ptr(), c.data_ptr(), second={**base, **bad})
+    with pytest.raises(fno_abi.FnoError):  # no split K with a second product
+        fno_abi.gemm(256, 32, 32, a.data_ptr(), b.data_ptr(), c.data_ptr(), ksplit=2, c_mode=2, second=base)
+
+
 def test_epilogue_bias_add_gelu_and_grad():
     M, N, K = 256, 32, 64
     a, b = _bf((M, K), 7), _bf((N, K), 8)
