@@ -47,10 +47,94 @@ __global__ void k_f2bf(bf16* dst, const float* src, long n) {
     dst[i] = __float2bfloat16(src[i]);
 }
 
-// mode-wise complex channel mixing, one block per (q, ky) mode
+// mode-wise complex channel mixing, one block per ky and 8 consecutive kx rows
+// q0..q0+7 (so that each row of Z and P is read and written in 32-byte runs):
 //   U = Z[q,ky]-Z[48+q,24+ky] + i(Z[q,24+ky]+Z[48+q,ky]),  O[o] = sum_i U[i] R[i,o]
 //   P[ky][q]=Or, P[ky][48+q]=Oi, P[24+ky][q]=Oi, P[24+ky][48+q]=-Or
+// Shared memory: R of the 8 modes as [i][o][j] and U as [(b,i)][j], j = q - q0
+// fastest, so that a warp's reads of both are conflict-free.
+constexpr int kMixQ = 8;
 __global__ void __launch_bounds__(256) k_mix_fwd(const float* __restrict__ zt, const bf16* __restrict__ Rr,
+                                                 const bf16* __restrict__ Ri, bf16* __restrict__ pt, int B, int W,
+                                                 int m2) {
+  extern __shared__ float sh[];
+  float* rr = sh;
+  float* ri = rr + kMixQ * W * W;
+  float* ur = ri + kMixQ * W * W;
+  float* ui = ur + kMixQ * B * W;
+  const int ky = blockIdx.x % m2, q0 = (blockIdx.x / m2) * kMixQ;
+  const int WW = W * W;
+  // the loads of each loop are issued in groups of 8 before their stores, so that
+  // a thread has several in flight (one block per SM leaves few warps to hide them)
+  for (int t0 = threadIdx.x; t0 < kMixQ * WW; t0 += 8 * blockDim.x) {
+    bf16 vr[8], vi[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < kMixQ * WW) {
+        const int j = t / WW, e = t - j * WW;  // e = i*W + o of mode (q0 + j, ky)
+        const long moff = ((long)(q0 + j) * m2 + ky) * WW;
+        vr[u] = Rr[moff + e];
+        vi[u] = Ri[moff + e];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < kMixQ * WW) {
+        const int j = t / WW, e = t - j * WW;
+        rr[e * kMixQ + j] = __bfloat162float(vr[u]);
+        ri[e * kMixQ + j] = __bfloat162float(vi[u]);
+      }
+    }
+  }
+  const int JR = kJ * kR;
+  for (int t0 = threadIdx.x; t0 < kMixQ * B * W; t0 += 4 * blockDim.x) {
+    float z0[4], z1[4], z2[4], z3[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < kMixQ * B * W) {
+        const int bc = t / kMixQ, q = q0 + (t % kMixQ);
+        const float* z = zt + (long)bc * JR;
+        z0[u] = z[ky * kR + q];
+        z1[u] = z[(m2 + ky) * kR + 48 + q];
+        z2[u] = z[(m2 + ky) * kR + q];
+        z3[u] = z[ky * kR + 48 + q];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < kMixQ * B * W) {
+        ur[t] = z0[u] - z1[u];
+        ui[t] = z2[u] + z3[u];
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kMixQ * B * W; t += blockDim.x) {
+    const int bo = t / kMixQ, j = t % kMixQ, b = bo / W, o = bo % W, q = q0 + j;
+    float orr = 0.f, oii = 0.f;
+    for (int i = 0; i < W; ++i) {
+      const float a = ur[(b * W + i) * kMixQ + j], c = ui[(b * W + i) * kMixQ + j];
+      const float xr = rr[(i * W + o) * kMixQ + j], xi = ri[(i * W + o) * kMixQ + j];
+      orr += a * xr - c * xi;
+      oii += a * xi + c * xr;
+    }
+    bf16* p = pt + (long)bo * JR;
+    p[ky * kR + q] = __float2bfloat16(orr);
+    p[ky * kR + 48 + q] = __float2bfloat16(oii);
+    p[(m2 + ky) * kR + q] = __float2bfloat16(oii);
+    p[(m2 + ky) * kR + 48 + q] = __float2bfloat16(-orr);
+  }
+}
+
+// the same mixing with one block per (q, ky) mode, for widths whose 8-mode
+// shared memory would not fit
+//   U = Z[q,ky]-Z[48+q,24+ky] + i(Z[q,24+ky]+Z[48+q,ky]),  O[o] = sum_i U[i] R[i,o]
+//   P[ky][q]=Or, P[ky][48+q]=Oi, P[24+ky][q]=Oi, P[24+ky][48+q]=-Or
+__global__ void __launch_bounds__(256) k_mix_fwd_mode(const float* __restrict__ zt, const bf16* __restrict__ Rr,
                                                  const bf16* __restrict__ Ri, bf16* __restrict__ pt, int B, int W,
                                                  int m2) {
   extern __shared__ float sh[];
@@ -261,6 +345,7 @@ struct sac_fno {
   std::string err;
   cudaStream_t st = nullptr;
   int S = 0, F = 0, W = 0, L = 0, H = 0, cin = 0, cout = 0, cpad = 0, m1 = 0, m2 = 0, nmodes = 0;
+  bool mix_grouped = false;  // k_mix_fwd's 8-mode blocks fit in shared memory
   long P = 0;
   // parameters: FP32 masters, BF16 copies, gradients, Adam moments (one buffer each)
   long nparam = 0;
@@ -401,9 +486,15 @@ int forward(sac_fno* n, const bf16* x, float* y, int B, bool train) {
     }
     // spectral mixing
     {
-      const size_t sm = sizeof(float) * (2 * W * W + 2 * B * W);
-      k_mix_fwd<<<n->nmodes, 256, sm, n->st>>>(n->zt[l], n->wb + n->sRr[l].off, n->wb + n->sRi[l].off, n->pt, B,
-                                               W, n->m2);
+      if (n->mix_grouped) {
+        const size_t sm = sizeof(float) * kMixQ * (2 * W * W + 2 * B * W);
+        k_mix_fwd<<<n->nmodes / kMixQ, 256, sm, n->st>>>(n->zt[l], n->wb + n->sRr[l].off, n->wb + n->sRi[l].off,
+                                                         n->pt, B, W, n->m2);
+      } else {
+        const size_t sm = sizeof(float) * (2 * W * W + 2 * B * W);
+        k_mix_fwd_mode<<<n->nmodes, 256, sm, n->st>>>(n->zt[l], n->wb + n->sRr[l].off, n->wb + n->sRi[l].off,
+                                                      n->pt, B, W, n->m2);
+      }
       FK(cudaGetLastError());
     }
     // F4: Y[(b,o)][s][j'] = sum_r P[(b,o),j'][r] Fx[r][s]   (rows (b,o,j'))
@@ -812,6 +903,20 @@ int sac_fno_create(const sac_fno_config* cfg, sac_fno** out) {
   if (cudaSetDevice(cfg->device) != cudaSuccess || cudaStreamCreateWithFlags(&n->st, cudaStreamNonBlocking)) {
     delete n;
     return fail(nullptr, "sac_fno_create: no device");
+  }
+  {  // the grouped forward mode mixing holds R and U of 8 modes for the whole batch
+    const size_t mix = sizeof(float) * kMixQ * (2 * (size_t)n->W * n->W + 2 * (size_t)n->Bmax * n->W);
+    n->mix_grouped = mix <= 227 * 1024 && (2 * n->m1) % kMixQ == 0 &&
+                     cudaFuncSetAttribute(k_mix_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mix) ==
+                         cudaSuccess;
+    cudaGetLastError();  // a refused attribute leaves the per-mode form
+    const size_t one = sizeof(float) * (2 * (size_t)n->W * n->W + 2 * (size_t)n->Bmax * n->W);
+    if (!n->mix_grouped &&
+        cudaFuncSetAttribute(k_mix_fwd_mode, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)one) != cudaSuccess) {
+      cudaStreamDestroy(n->st);
+      delete n;
+      return fail(nullptr, "sac_fno_create: width and max_batch too large for the mode mixing's shared memory");
+    }
   }
   // parameter segments (each a multiple of 8 elements, 16-byte aligned in bf16)
   long off = 0;

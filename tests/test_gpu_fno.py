@@ -3,10 +3,11 @@ float64 CPU oracle (oracle/fno_ref.py) on the same BF16-rounded weights and
 inputs.  The GPU keeps activations in BF16 and its DFT tables in BF16, so the
 bar is a relative L2 of 2e-2 on the output and 5e-2 per gradient group.
 
-Two shapes: CFG, where every layer runs as separate GEMMs, and WIDE (F a multiple
-of 128, hidden 128), where each Fourier layer accumulates its spectral term into
-the channel-mixing GEMM's tile and inference runs the projection in one kernel
-that keeps the hidden channels on chip."""
+Three shapes: CFG, where every layer runs as separate GEMMs; WIDE (F a multiple
+of 128, hidden 128), where each Fourier layer's channel-mixing GEMM accumulates
+the spectral term as its second product and inference runs the projection in one
+kernel that keeps the hidden channels on chip; DUAL, the same layers at width 48
+(a 48-column tile)."""
 import numpy as np
 import pytest
 
@@ -19,7 +20,8 @@ pytestmark = pytest.mark.gpu
 
 CFG = dict(S=64, F=64, width=32, layers=2, hidden=32, cin=16, cout=6)
 WIDE = dict(S=64, F=128, width=32, layers=2, hidden=128, cin=16, cout=6)
-SHAPES = pytest.mark.parametrize("cfg", [CFG, WIDE], ids=["separate", "fused"])
+DUAL = dict(S=64, F=128, width=48, layers=2, hidden=32, cin=16, cout=6)
+SHAPES = pytest.mark.parametrize("cfg", [CFG, WIDE, DUAL], ids=["separate", "fused", "dual"])
 
 
 @pytest.fixture(scope="module", autouse=True)

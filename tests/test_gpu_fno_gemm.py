@@ -122,16 +122,19 @@ def test_epilogue_bias_add_gelu_and_grad():
     fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), out.data_ptr(), c_bf16=True, bias_n=bias.data_ptr(),
                  add=add.data_ptr(), act=1, pre=pre.data_ptr())
     torch.cuda.synchronize()
+    # GELU is the tanh form, evaluated with the SFU's tanh (relative error ~5e-4)
     z = _ref(a, b) + bias.double() + add.double()
     torch.testing.assert_close(pre.double(), z, rtol=1e-2, atol=1e-2)
-    ref = torch.nn.functional.gelu(z)
+    ref = torch.nn.functional.gelu(z, approximate="tanh")
     torch.testing.assert_close(out.double(), ref, rtol=1e-2, atol=1e-2)
     g = torch.zeros(M, N, dtype=torch.float32, device="cuda")
     fno_abi.gemm(M, N, K, a.data_ptr(), b.data_ptr(), g.data_ptr(), act=2, pre=pre.data_ptr())
     torch.cuda.synchronize()
     x = pre.double().requires_grad_(True)
-    torch.nn.functional.gelu(x).sum().backward()
-    torch.testing.assert_close(g.double(), _ref(a, b) * x.grad, rtol=1e-4, atol=1e-3)
+    torch.nn.functional.gelu(x, approximate="tanh").sum().backward()
+    acc = _ref(a, b)
+    err = (g.double() - acc * x.grad).abs()
+    assert (err <= 5e-3 * acc.abs() + 1e-4).all(), err.max().item()  # GELU' moves up to ~5x the tanh error
 
 
 def test_split_k_atomic_and_accumulate():
