@@ -213,110 +213,6 @@ __device__ __forceinline__ void nu_cell(const Stage2Args& a, const Geom& g, cons
   }
 }
 
-// setnu's face quotients of one pair along one dimension for consecutive
-// positions pstart..pend-1 (pend > pstart) of a line: the window a(p-2..p+3), its
-// five first and three third differences are those of face_quotient, carried
-// from one position to the next, so each new position loads one value and forms
-// one d1 and one d3; every value is the same expression as face_quotient's, so
-// the quotients are the same bit for bit.  q and out point at the line's p = 0.
-template <typename S>
-__device__ __forceinline__ void march_quotients(const S* __restrict__ q, S* __restrict__ out, long s, int pstart,
-                                                int pend, int lo, int hi, S pre) {
-  auto at = [&](int p) {  // the mirrored layer beyond the two ghosts, src/vacusr.viscosity.t:378-400
-    if (p <= lo - 3) p = lo + 3;
-    if (p >= hi + 3) p = hi - 3;
-    return __ldg(q + (long)p * s);
-  };
-  auto d3f = [](S a0, S a1, S a2, S a3) { return fabsT(sub_rn(mul_rn(S(3), sub_rn(a2, a1)), sub_rn(a3, a0))); };
-  S a0 = at(pstart - 2), a1 = at(pstart - 1), a2 = at(pstart), a3 = at(pstart + 1), a4 = at(pstart + 2),
-    a5 = at(pstart + 3);
-  S d1a = fabsT(a1 - a0), d1b = fabsT(a2 - a1), d1c = fabsT(a3 - a2), d1d = fabsT(a4 - a3), d1e = fabsT(a5 - a4);
-  S d3a = d3f(a0, a1, a2, a3), d3b = d3f(a1, a2, a3, a4), d3c = d3f(a2, a3, a4, a5);
-  for (int p = pstart;; ++p) {
-    const S md3 = fmaxT(fmaxT(d3a, d3b), d3c);
-    const S md1 = fmaxT(fmaxT(fmaxT(fmaxT(d1a, d1b), d1c), d1d), d1e);
-    const S r = pre * md3 / md1;  // c_tot*c_hyp*md3R/md1R, :424
-    out[(long)p * s] = (md1 > S(0)) ? r : S(0);
-    if (p + 1 >= pend) break;
-    const S an = at(p + 4);
-    d1a = d1b, d1b = d1c, d1c = d1d, d1d = d1e, d1e = fabsT(an - a5);
-    d3a = d3b, d3b = d3c, d3c = d3f(a3, a4, a5, an);
-    a3 = a4, a4 = a5, a5 = an;
-  }
-}
-
-// k_nu in 3D with the lines marched: a thread takes one x1 position and a YC x ZC
-// block of (x2, x3) positions of the face domain (lo-1 .. hi in every dimension);
-// the x1 pairs per cell (face_quotient), the x2 pairs marched along x2 for each
-// x3, the x3 pairs along x3 for each x2
-template <int NDIR, typename S, int YC, int ZC>
-__global__ void __launch_bounds__(256, 4) k_nu_march(const Stage2Args a) {
-  constexpr int NDIM = 3, E = NDIR + 1;
-  using PR = Pairs<NDIM>;
-  const Geom& g = a.g;
-  const int e0 = g.hi[0] - g.lo[0] + 2, e1 = g.hi[1] - g.lo[1] + 2, e2 = g.hi[2] - g.lo[2] + 2;
-  const int n1 = (e1 + YC - 1) / YC, n2 = (e2 + ZC - 1) / ZC;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= (long)e0 * n1 * n2) return;
-  const int x = (int)(t % e0) + g.lo[0] - 1;
-  const int yb = (int)((t / e0) % n1), zb = (int)(t / ((long)e0 * n1));
-  const int y0 = yb * YC + g.lo[1] - 1, z0 = zb * ZC + g.lo[2] - 1;
-  const int y1 = min(y0 + YC, g.hi[1] + 1), z1 = min(z0 + ZC, g.hi[2] + 1);  // exclusive
-  const long s1 = g.st[1], s2 = g.st[2];
-  S p04[NDIM], p4[NDIM];
-#pragma unroll
-  for (int k = 0; k < NDIM; ++k) {
-    const double ct = __longlong_as_double((long long)a.ctot[k]);
-    p04[k] = (S)(ct * 0.04);  // c_hyp, :284-290
-    p4[k] = (S)(ct * 0.4);
-  }
-  auto W = [&](int iw) { return (const S*)a.fW[iw]; };
-  auto Df = [&](int i) { return (const S*)a.fD[i]; };
-  auto Qw = [&](int ip) { return (S*)a.fQ[ip]; };
-  // the pair sources of dimension k: rho, the "173" energy, v_l, b_l (l != k)
-  auto pair_of = [&](int k, int j, const S*& q, int& ip, S& pre) {
-    if (j == 0) {
-      q = W(0), ip = PR::rho(k), pre = p04[k];
-    } else if (j == 1) {
-      q = Df(NDIR + 1), ip = PR::e(k), pre = p04[k];
-    } else if (j < 2 + NDIM) {
-      q = Df(1 + (j - 2)), ip = PR::v(j - 2, k), pre = p4[k];
-    } else {
-      const int m = j - 2 - NDIM, l = m < k ? m : m + 1;  // the b_l with l != k
-      q = W(E + 1 + l), ip = PR::b(l, k), pre = p04[k];
-    }
-  };
-  constexpr int NPK = 2 + NDIM + (NDIM - 1);  // pairs per dimension
-  for (int y = y0; y < y1; ++y)
-    for (int z = z0; z < z1; ++z) {
-      const int c = x + (int)s1 * y + (int)s2 * z;
-#pragma unroll
-      for (int j = 0; j < NPK; ++j) {
-        const S* q;
-        int ip;
-        S pre;
-        pair_of(0, j, q, ip, pre);
-        Qw(ip)[c] = face_quotient(q, c, 1, x, g.lo[0], g.hi[0], pre);
-      }
-    }
-#pragma unroll 1
-  for (int j = 0; j < NPK; ++j) {
-    const S* q;
-    int ip;
-    S pre;
-    pair_of(1, j, q, ip, pre);
-    for (int z = z0; z < z1; ++z) {
-      const long base = x + s2 * z;
-      march_quotients(q + base, Qw(ip) + base, s1, y0, y1, g.lo[1], g.hi[1], pre);
-    }
-    pair_of(2, j, q, ip, pre);
-    for (int y = y0; y < y1; ++y) {
-      const long base = x + s1 * y;
-      march_quotients(q + base, Qw(ip) + base, s2, z0, z1, g.lo[2], g.hi[2], pre);
-    }
-  }
-}
-
 // The fused 2D stage's view of one cell for update_cell: the stencil fields in
 // shared-memory tiles of row stride st1 (each pointer offset so that [c] is the
 // cell), the cell's box index c and its index cg in the instance's global blocks.
@@ -1139,21 +1035,10 @@ void launch_face(const Stage2Args& a0, int do_ctot, cudaStream_t st) {
   });
 }
 
-#ifndef SAC_NU_MARCH
-#define SAC_NU_MARCH 1  // 3D: k_nu_march (lines marched along x2 and x3)
-#endif
-
 template <typename S>
 void launch_nu(const Stage2Args& a0, cudaStream_t st) {
   Stage2Args a = a0;
   fill_field_ptrs(a, sizeof(S));
-  if (SAC_NU_MARCH && a.g.ndim == 3) {
-    constexpr int YC = 4, ZC = 4;
-    const long e0 = a.g.hi[0] - a.g.lo[0] + 2, e1 = a.g.hi[1] - a.g.lo[1] + 2, e2 = a.g.hi[2] - a.g.lo[2] + 2;
-    const long nt = e0 * ((e1 + YC - 1) / YC) * ((e2 + ZC - 1) / ZC);
-    k_nu_march<3, S, YC, ZC><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(a);  // 3D is ndir 3 (dispatch_nd)
-    return;
-  }
   long nb = 1;
   for (int d = 0; d < a.g.ndim; ++d) nb *= (a.g.hi[d] - a.g.lo[d] + 2);
   dispatch_nd(a.g, [&](auto ND, auto NR) {
