@@ -155,15 +155,19 @@ def features_host(A, om, t, omega_ac):
 # training
 # ---------------------------------------------------------------------------
 class Surrogate:
-    def __init__(self, S=256, F=256, batch=16, seed=0, width=32, layers=4, hidden=128):
+    def __init__(self, S=256, F=256, batch=16, seed=0, width=32, layers=4, hidden=128, infer_batch=None):
+        """batch: the training minibatch; infer_batch: the samples per inference
+        call of predict (default: batch)."""
         torch = _torch()
+        self.BI = infer_batch or batch
+        nmax = max(batch, self.BI)
         self.net = fno_abi.Net(S=S, F=F, width=width, layers=layers, hidden=hidden, cin=16, cout=NST,
-                               max_batch=batch, seed=seed)
+                               max_batch=nmax, seed=seed)
         self.B, self.S, self.F = batch, S, F
         self.stream = torch.cuda.ExternalStream(self.net.stream)
         dev = "cuda"
-        self.x = torch.zeros(batch, 16, S, F, dtype=torch.bfloat16, device=dev)
-        self.y = torch.zeros(batch, NST, S, F, dtype=torch.float32, device=dev)
+        self.x = torch.zeros(nmax, 16, S, F, dtype=torch.bfloat16, device=dev)
+        self.y = torch.zeros(nmax, NST, S, F, dtype=torch.float32, device=dev)
         self.dy = torch.zeros(batch, self.net.cpad, S, F, dtype=torch.bfloat16, device=dev)
         self.loss = torch.zeros(1, dtype=torch.float32, device=dev)
         self.tgt = torch.zeros(batch, NST, S, F, dtype=torch.bfloat16, device=dev)
@@ -261,24 +265,22 @@ class Surrogate:
         [n][6][S][F] (raw perturbation, packed layout of sac_batch_gather)."""
         torch = _torch()
         n = state.shape[0]
-        sc_in = np.tile(1.0 / self.sx, n) / np.repeat(A, NST)
-        sc_out = np.tile(self.sd, n) * np.repeat(A, NST)
-        for i0 in range(0, n, self.B):
-            B = min(self.B, n - i0)
-            sl = slice(i0, i0 + B)
-            with torch.cuda.stream(self.stream):
-                self.scale[:B * NST] = torch.as_tensor(sc_in[i0 * NST:(i0 + B) * NST], dtype=torch.float32,
-                                                       device="cuda")
-                f = features_host(A[sl], om[sl], np.full(B, t), self.omega_ac)
-                self.feat[:B * NFEAT] = torch.as_tensor(f.reshape(-1), device="cuda")
-                blk = state[sl]
-            self.net.features(blk.data_ptr(), False, self.scale.data_ptr(), self.feat.data_ptr(), NFEAT,
-                              self.x.data_ptr(), B, NST)
+        # the window's scales and features of all n instances in one copy each, so
+        # that the host enqueues the chunks without waiting on the stream
+        sc = np.concatenate([np.tile(1.0 / self.sx, n) / np.repeat(A, NST), np.tile(self.sd, n) * np.repeat(A, NST)])
+        f = features_host(A, om, np.full(n, t), self.omega_ac).reshape(-1)
+        with torch.cuda.stream(self.stream):
+            scd = torch.as_tensor(sc, dtype=torch.float32).pin_memory().to("cuda", non_blocking=True)
+            fd = torch.as_tensor(f, dtype=torch.float32).pin_memory().to("cuda", non_blocking=True)
+        fsz = 4  # bytes per float32
+        for i0 in range(0, n, self.BI):
+            B = min(self.BI, n - i0)
+            blk = state[i0:i0 + B]
+            self.net.features(blk.data_ptr(), False, scd.data_ptr() + i0 * NST * fsz, fd.data_ptr() + i0 * NFEAT * fsz,
+                              NFEAT, self.x.data_ptr(), B, NST)
             self.net.infer(self.x.data_ptr(), self.y.data_ptr(), B)
-            with torch.cuda.stream(self.stream):
-                self.scale[:B * NST] = torch.as_tensor(sc_out[i0 * NST:(i0 + B) * NST], dtype=torch.float32,
-                                                       device="cuda")
-            self.net.apply(blk.data_ptr(), self.y.data_ptr(), self.scale.data_ptr(), B, NST)
+            self.net.apply(blk.data_ptr(), self.y.data_ptr(), scd.data_ptr() + (n + i0) * NST * fsz, B, NST)
+        self._keep = (scd, fd)  # alive until the stream has used them
 
     def save(self, path):
         np.savez(path, params=self.net.get_params(), sx=self.sx, sd=self.sd)
@@ -452,6 +454,7 @@ def main(argv=None):
     ap.add_argument("--time-limit", type=float, default=None)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--infer-batch", type=int, default=64, help="samples per inference call in the roll-outs")
     ap.add_argument("--M", type=int, default=16)
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
@@ -472,7 +475,7 @@ def main(argv=None):
     dt = a.dt if a.dt else stable_dt(n)
     nwin = a.steps // a.window
     log(f"fixed dt {dt:.4e}, {nwin} windows of {a.window} steps")
-    sur = Surrogate(S=n[1], F=n[0], batch=a.batch, seed=a.seed)
+    sur = Surrogate(S=n[1], F=n[0], batch=a.batch, seed=a.seed, infer_batch=a.infer_batch)
     hist, val, gen_s = [], {}, 0.0
     if a.weights:
         sur.load(a.weights)
