@@ -2,11 +2,13 @@
 """Benchmark of the perturbation-MHD hot path on B200.
 
 Headline workload: the 3D gravitationally stratified atmosphere at 512x512x512
-mesh cells (the precision-comparison configuration), FP64, RK4
+mesh cells, the precision-comparison configuration: FP64, RK4
 (typeadvance='fourstep'), hyperdiffusion, gravity, bottom velocity driver,
-fixed/open x1 boundaries and periodic x2/x3 (sac_b200.problems.stratified).  The
-same workload at 128^3 (the stratified-atmosphere configuration) is measured
-beside it.  One step = one time step of the reference's main loop: getdt + advect
+fixed/open x1 boundaries and periodic x2/x3, and an initial state of 64 seeded
+random-phase Fourier modes (|k| <= 16, amplitude 1e-4, divergence-free b')
+(sac_b200.problems.stratified(perturb=1e-4)).  The stratified-atmosphere
+configuration at 128^3, which starts at rest and is stirred by the driver, is
+measured beside it.  One step = one time step of the reference's main loop: getdt + advect
 (four RK stages with their boundary fills) on the resident state.  Metric:
 cell-updates per second (one mesh cell advanced by one full RK4 step), for the
 FP64 path and the FP32-perturbation path.
@@ -46,9 +48,20 @@ STAGES_PER_STEP = 4
 CPU_SAMPLE_N = 128  # the CPU legs time whole RK4 steps of the stratified workload on this cube
 
 
-def workload(n=128, precision="fp64"):
-    P = problems.stratified(n=(n, n, n))
-    return P
+MODES_AMP = 1e-4  # the precision-comparison configuration's random-mode amplitude
+
+
+def perturb_for(n, init):
+    """The initial perturbation amplitude of the n^3 workload: the 64 random modes
+    of the precision-comparison configuration ('modes'), the state at rest of the
+    128^3 configuration ('rest'), or by size ('auto': modes unless n == 128)."""
+    if init == "modes" or (init == "auto" and n != 128):
+        return MODES_AMP
+    return None
+
+
+def workload(n=128, perturb=None):
+    return problems.stratified(n=(n, n, n), perturb=perturb)
 
 
 def load_peaks():
@@ -125,7 +138,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # the CPU legs (oracle = C++ restatement of the reference)
 # ---------------------------------------------------------------------------
-def cpu_steps(n=CPU_SAMPLE_N, threads=None, seconds=12.0, max_steps=64, min_steps=1, warmup=1):
+def cpu_steps(n=CPU_SAMPLE_N, threads=None, seconds=12.0, max_steps=64, min_steps=1, warmup=1, perturb=None):
     """Cell-updates/s of the oracle on the host cores: `warmup` untimed RK4 steps
     (getdt + advect), then timed steps until `seconds` elapse (at least
     min_steps), on the n^3 stratified cube.  Both CPU legs use this."""
@@ -134,7 +147,7 @@ def cpu_steps(n=CPU_SAMPLE_N, threads=None, seconds=12.0, max_steps=64, min_step
     oracle.build()
     if threads is not None:
         oracle.set_threads(threads)
-    P = problems.stratified(n=(n, n, n))
+    P = workload(n, perturb)
     o = oracle.Oracle(P.params)
     o.set_grid(P.ndim, P.ndir, P.ixGhi, P.ixM, P.x)
     o.set_boundaries(P.typeB_packed, P.nB)
@@ -161,19 +174,23 @@ def cpu_steps(n=CPU_SAMPLE_N, threads=None, seconds=12.0, max_steps=64, min_step
     used = threads if threads is not None else oracle.max_threads()
     if threads is not None:
         oracle.set_threads(oracle.max_threads())
-    return {"value": P.ncells * k / el, "steps": k, "seconds": el, "threads": used, "cells": P.ncells, "n": n}
+    return {"value": P.ncells * k / el, "steps": k, "seconds": el, "threads": used, "cells": P.ncells, "n": n,
+            "perturb": perturb}
 
 
 def cpu_sample_text(r):
+    state = "64 random modes, amplitude 1e-4" if r.get("perturb") else "at rest, driven"
     return (f"{r['steps']} RK4 steps (getdt+advect) in {r['seconds']:.1f} s on the full {r['n']}^3 stratified "
-            f"cube, C++ FP64 restatement of the reference (the Fortran reference cannot be built: no Fortran "
+            f"cube ({state}), C++ FP64 restatement of the reference (the Fortran reference cannot be built: no Fortran "
             f"compiler), {r['threads']} OpenMP thread(s); a whole RK4 step of the 512^3 grid would take minutes on "
             f"the host, so the cube is the bounded sample of the workload, per cell")
 
 
-def headline_config(n, world):
+def headline_config(n, world, perturb=None):
+    state = ("initial state 64 seeded random modes |k|<=16, amplitude 1e-4, div-free b'" if perturb
+             else "initial state at rest")
     return {"workload": f"stratified atmosphere {n}^3, FP64 and FP32-perturbation paths, RK4, hyperdiffusion, "
-                        f"gravity, driver",
+                        f"gravity, driver, {state}",
             "cells_per_step": n ** 3, "parallelism": f"replicas{world}",
             "l2": f"no flush: the FP64 context holds ~{(n + 4) ** 3 * 800 / 1e9:.1f} GB per replica (state, RK "
                   f"arrays and per-stage intermediates), far larger than the 126 MB L2",
@@ -186,13 +203,14 @@ def reference_arm(args, rank, world):
     from oracle import oracle
 
     oracle.build()
-    r = cpu_steps(warmup=args.warmup, seconds=0.0, min_steps=args.steps, max_steps=args.steps)
+    r = cpu_steps(warmup=args.warmup, seconds=0.0, min_steps=args.steps, max_steps=args.steps,
+                  perturb=perturb_for(args.n, args.init))
     v = r["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": headline_config(args.n, world),
+        "config": headline_config(args.n, world, perturb_for(args.n, args.init)),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["threads"], "kind": "port", "sample": cpu_sample_text(r)},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -305,19 +323,21 @@ def timed_steps(args, P, ctx, lib, local_rank, world, clocks=True):
 SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 
-def issue_ceiling(path, value, sm_mhz):
+def issue_ceiling(path, value, sm_mhz, perturb=None):
     """The instruction-issue wall of a path: the warp instructions one RK4 step
-    issues per mesh cell (all kernels of the step, ncu instruction counts at 128^3,
-    profiles/stage_instructions_stratified128.json) against the SM issue peak of
-    one warp instruction per scheduler and clock, at the sampled SM clock."""
+    issues per mesh cell (all kernels of the step, ncu instruction counts at 128^3
+    from the same initial state, profiles/stage_instructions_stratified128.json)
+    against the SM issue peak of one warp instruction per scheduler and clock, at
+    the sampled SM clock."""
     p = os.path.join(ROOT, "profiles", "stage_instructions_stratified128.json")
     if not os.path.exists(p) or not sm_mhz:
         return None
     with open(p) as f:
         d = json.load(f)
-    if path not in d.get("warp_instr_per_step", {}):
+    key = "warp_instr_per_step_modes" if perturb else "warp_instr_per_step"
+    if path not in d.get(key, {}):
         return None
-    per_cell = d["warp_instr_per_step"][path] / d["cells"]
+    per_cell = d[key][path] / d["cells"]
     peak = SM_COUNT * SCHEDULERS_PER_SM * sm_mhz * 1e6
     ceiling = peak / per_cell
     return {"warp_instr_per_cell_update": per_cell, "peak_warp_instr_per_s": peak, "unit": "cell-updates/s",
@@ -335,13 +355,13 @@ def roofline(b_cell_update, cells, kern, peak, peak_kind, tr_name, label):
             "kernel": label, "bytes_per_launch": b_launch, "avg_launch_ms": upd_ms / upd_n if upd_n else None}
 
 
-def measure(args, n, local_rank, world, legs, clocks=True):
+def measure(args, n, local_rank, world, legs, clocks=True, perturb=None):
     """The FP64 and FP32 legs (and e2e) of the stratified workload at n^3: each a
     context of its own on the rank's GPU, created, timed and released in turn."""
     import torch
     import torch.distributed as dist
 
-    P = workload(n)
+    P = workload(n, perturb)
     cells = P.ncells
     nbytes = P.nw * int(np.prod(P.ixGhi)) * 8
     out = {"cells": cells, "nbytes": nbytes}
@@ -414,10 +434,12 @@ def ours(args, rank, world, local_rank):
     sbuild.build()
     torch.cuda.set_device(local_rank)
     legs = set(args.legs.split(","))
-    main = measure(args, args.n, local_rank, world, legs)
+    pert = perturb_for(args.n, args.init)
+    main = measure(args, args.n, local_rank, world, legs, perturb=pert)
     small = None
     if args.n != 128 and "small" in legs:
-        small = measure(args, 128, local_rank, world, legs & {"fp64", "fp32"}, clocks=False)
+        small = measure(args, 128, local_rank, world, legs & {"fp64", "fp32"}, clocks=False,
+                        perturb=perturb_for(128, args.init))
     if rank != 0:
         return 0
     peak, peak_kind = load_peaks()
@@ -429,17 +451,17 @@ def ours(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": lead["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if "r64" in main else "f32", "data": "synthetic",
-        "config": headline_config(args.n, world),
+        "config": headline_config(args.n, world, pert),
         "gpu_launches": lead["launches"],
         "clocks": lead["clocks"],
     }
     sm_mhz = (lead["clocks"] or {}).get("sm_mhz")
     if "fp64" in summ:
         line["roofline"] = summ["fp64"]["roofline"]
-        line["roofline"]["issue"] = issue_ceiling("fp64", summ["fp64"]["value"] / world, sm_mhz)
+        line["roofline"]["issue"] = issue_ceiling("fp64", summ["fp64"]["value"] / world, sm_mhz, pert)
         line["kernels_ms_per_step"] = summ["fp64"]["kernels_ms_per_step"]
     if "fp32" in summ:
-        summ["fp32"]["roofline"]["issue"] = issue_ceiling("fp32", summ["fp32"]["value"] / world, sm_mhz)
+        summ["fp32"]["roofline"]["issue"] = issue_ceiling("fp32", summ["fp32"]["value"] / world, sm_mhz, pert)
     if "e2e" in main:
         line["e2e"] = {"value": main["e2e"], "unit": UNIT, "h2d_bytes_per_step": main["nbytes"],
                        "d2h_bytes_per_step": main["nbytes"],
@@ -449,10 +471,10 @@ def ours(args, rank, world, local_rank):
     if small is not None:
         line["stratified_128"] = leg_summary(small, args, peak, peak_kind)
     if world == 1 and not args.no_cpu and "cpu" in legs:
-        r = cpu_steps()
+        r = cpu_steps(perturb=pert)
         line["cpu_baseline"] = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "port",
                                 "sample": cpu_sample_text(r)}
-        r1 = cpu_steps(n=64, threads=1, seconds=8.0, max_steps=8)
+        r1 = cpu_steps(n=64, threads=1, seconds=8.0, max_steps=8, perturb=pert)
         line["cpu_baseline_1core"] = {"value": r1["value"], "unit": UNIT, "cores": 1, "kind": "port",
                                       "sample": cpu_sample_text(r1)}
     print(json.dumps(line), flush=True)
@@ -614,6 +636,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=512, help="mesh cells per dimension of the headline line (default 512)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--init", default="auto", choices=["auto", "modes", "rest"],
+                    help="initial state: the 64 random modes of the precision-comparison configuration, the state "
+                         "at rest of the 128^3 configuration, or auto (modes unless --n 128)")
     ap.add_argument("--legs", default="fp64,e2e,fp32,small,cpu",
                     help="comma list of fp64, e2e, fp32, small (the 128^3 legs beside a larger --n), cpu "
                          "(profiling runs select one kernel family)")
