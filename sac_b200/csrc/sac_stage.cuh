@@ -182,8 +182,10 @@ __device__ __forceinline__ S face_quotient(const S* __restrict__ q, int c, int s
     d3[j] = fabsT(sub_rn(mul_rn(S(3), sub_rn(a[j + 2], a[j + 1])), sub_rn(a[j + 3], a[j])));
   const S md3 = fmaxT(fmaxT(d3[0], d3[1]), d3[2]);
   const S md1 = fmaxT(fmaxT(fmaxT(fmaxT(d1[0], d1[1]), d1[2]), d1[3]), d1[4]);
-  const S r = pre * md3 / md1;  // c_tot*c_hyp*md3R/md1R, :424
-  return (md1 > S(0)) ? r : S(0);
+  // zero where the window is flat (md1 == 0): branch before dividing, since 0/0
+  // leaves the division's fast path, and a state at rest is flat almost everywhere
+  if (!(md1 > S(0))) return S(0);
+  return pre * md3 / md1;  // c_tot*c_hyp*md3R/md1R, :424
 }
 
 // k_nu body at local cell c with local coordinates p: every setnu pair's face
