@@ -599,9 +599,20 @@ int forward(sac_fno* n, const bf16* x, float* y, int B, bool train) {
     pa.wait_tries = n->wait_tries;
     static int per_sm = 0;
     if (!per_sm) {
+      // resident CTAs per SM from the kernel's own limits: shared memory (with the
+      // largest carveout), TMEM (kProjH of 512 columns each) and registers
       FK(cudaFuncSetAttribute(k_proj_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kProjSmem));
-      FK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_proj_infer, kThreads, kProjSmem));
-      if (per_sm < 1) per_sm = 1;
+      FK(cudaFuncSetAttribute(k_proj_infer, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+      cudaFuncAttributes fa{};
+      FK(cudaFuncGetAttributes(&fa, k_proj_infer));
+      int dev = 0, smem_sm = 0, regs_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+      cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+      const int by_smem = smem_sm / (kProjSmem + (int)fa.sharedSizeBytes + 1024);
+      const int by_tmem = 512 / kProjH;
+      const int by_regs = fa.numRegs > 0 ? regs_sm / (fa.numRegs * kThreads) : by_tmem;
+      per_sm = std::max(1, std::min(std::min(by_smem, by_tmem), by_regs));
     }
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
