@@ -207,8 +207,18 @@ __device__ __forceinline__ void stage2d_tile(const BatchStageArgs& b, int t, uns
   }
 }
 
+// resident CTAs per SM the fused stage is compiled for: FP64 2 (its 97.6 KB of
+// tile memory allows no more; 128 registers), FP32 4 (64 registers, no spills for
+// ndir 2)
+#ifndef SAC_STAGE2D_MINB_F64
+#define SAC_STAGE2D_MINB_F64 2
+#endif
+#ifndef SAC_STAGE2D_MINB_F32
+#define SAC_STAGE2D_MINB_F32 4
+#endif
 template <int NDIR, typename S, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY) kb_stage2d(const __grid_constant__ BatchStageArgs b) {
+__global__ void __launch_bounds__(TX * TY, sizeof(S) == 4 ? SAC_STAGE2D_MINB_F32 : SAC_STAGE2D_MINB_F64)
+    kb_stage2d(const __grid_constant__ BatchStageArgs b) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double shred[32];
   for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) stage2d_tile<NDIR, S, TX, TY>(b, t, smraw, shred);
