@@ -171,6 +171,103 @@ __global__ void __launch_bounds__(256) k_mix_fwd_mode(const float* __restrict__ 
   }
 }
 
+// backward of k_mix_fwd with one block per ky and 8 consecutive kx rows (the
+// per-mode k_mix_bwd below, regrouped as k_mix_fwd is): dZ (bf16) and dR += (fp32).
+// Shared memory: R as [o][i][j] (a warp of the dZ phase reads consecutive i),
+// U as [(b,i)][j] and G as [(b,o)][j], j = q - q0 fastest; the loads are issued
+// in groups.  The sums run over o and over b in the per-mode kernel's order.
+__global__ void __launch_bounds__(256) k_mix_bwd_g(const float* __restrict__ dpt, const float* __restrict__ zt,
+                                                   const bf16* __restrict__ Rr, const bf16* __restrict__ Ri,
+                                                   bf16* __restrict__ dzt, float* __restrict__ dRr,
+                                                   float* __restrict__ dRi, int B, int W, int m2) {
+  extern __shared__ float sh[];
+  float* rr = sh;
+  float* ri = rr + kMixQ * W * W;
+  float* ur = ri + kMixQ * W * W;
+  float* ui = ur + kMixQ * B * W;
+  float* gr = ui + kMixQ * B * W;
+  float* gi = gr + kMixQ * B * W;
+  const int ky = blockIdx.x % m2, q0 = (blockIdx.x / m2) * kMixQ;
+  const int WW = W * W, JR = kJ * kR;
+  for (int t0 = threadIdx.x; t0 < kMixQ * WW; t0 += 8 * blockDim.x) {
+    bf16 vr[8], vi[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < kMixQ * WW) {
+        const int j = t / WW, e = t - j * WW;  // e = i*W + o of mode (q0 + j, ky)
+        const long moff = ((long)(q0 + j) * m2 + ky) * WW;
+        vr[u] = Rr[moff + e];
+        vi[u] = Ri[moff + e];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < kMixQ * WW) {
+        const int j = t / WW, e = t - j * WW, i = e / W, o = e - i * W;
+        rr[(o * W + i) * kMixQ + j] = __bfloat162float(vr[u]);
+        ri[(o * W + i) * kMixQ + j] = __bfloat162float(vi[u]);
+      }
+    }
+  }
+  for (int t0 = threadIdx.x; t0 < kMixQ * B * W; t0 += 2 * blockDim.x) {
+    float z[2][4], g[2][4];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < kMixQ * B * W) {
+        const int bc = t / kMixQ, q = q0 + (t % kMixQ);
+        const float* zz = zt + (long)bc * JR;
+        const float* gg = dpt + (long)bc * JR;
+        z[u][0] = zz[ky * kR + q], z[u][1] = zz[(m2 + ky) * kR + 48 + q];
+        z[u][2] = zz[(m2 + ky) * kR + q], z[u][3] = zz[ky * kR + 48 + q];
+        g[u][0] = gg[ky * kR + q], g[u][1] = gg[(m2 + ky) * kR + 48 + q];
+        g[u][2] = gg[ky * kR + 48 + q], g[u][3] = gg[(m2 + ky) * kR + q];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < kMixQ * B * W) {
+        ur[t] = z[u][0] - z[u][1];
+        ui[t] = z[u][2] + z[u][3];
+        gr[t] = g[u][0] - g[u][1];
+        gi[t] = g[u][2] + g[u][3];
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kMixQ * B * W; t += blockDim.x) {  // t = ((b, i), j)
+    const int bi = t / kMixQ, j = t % kMixQ, b = bi / W, i = bi % W, q = q0 + j;
+    float dur = 0.f, dui = 0.f;
+    for (int o = 0; o < W; ++o) {
+      const float a = gr[(b * W + o) * kMixQ + j], c = gi[(b * W + o) * kMixQ + j];
+      const float xr = rr[(o * W + i) * kMixQ + j], xi = ri[(o * W + i) * kMixQ + j];
+      dur += a * xr + c * xi;
+      dui += -a * xi + c * xr;
+    }
+    bf16* p = dzt + (long)bi * JR;
+    p[ky * kR + q] = __float2bfloat16(dur);
+    p[(m2 + ky) * kR + 48 + q] = __float2bfloat16(-dur);
+    p[(m2 + ky) * kR + q] = __float2bfloat16(dui);
+    p[ky * kR + 48 + q] = __float2bfloat16(dui);
+  }
+  for (int t = threadIdx.x; t < kMixQ * WW; t += blockDim.x) {  // t = ((i, o), j)
+    const int io = t / kMixQ, j = t % kMixQ, i = io / W, o = io % W;
+    float sr = 0.f, si = 0.f;
+    for (int b = 0; b < B; ++b) {
+      const float a = gr[(b * W + o) * kMixQ + j], c = gi[(b * W + o) * kMixQ + j];
+      const float u = ur[(b * W + i) * kMixQ + j], v = ui[(b * W + i) * kMixQ + j];
+      sr += a * u + c * v;
+      si += -a * v + c * u;
+    }
+    const long moff = ((long)(q0 + j) * m2 + ky) * WW;
+    dRr[moff + io] += sr;
+    dRi[moff + io] += si;
+  }
+}
+
 // backward of k_mix_fwd: dZ (bf16) and dR += (fp32), one block per mode
 __global__ void __launch_bounds__(256) k_mix_bwd(const float* __restrict__ dpt, const float* __restrict__ zt,
                                                  const bf16* __restrict__ Rr, const bf16* __restrict__ Ri,
@@ -346,6 +443,7 @@ struct sac_fno {
   cudaStream_t st = nullptr;
   int S = 0, F = 0, W = 0, L = 0, H = 0, cin = 0, cout = 0, cpad = 0, m1 = 0, m2 = 0, nmodes = 0;
   bool mix_grouped = false;  // k_mix_fwd's 8-mode blocks fit in shared memory
+  size_t mix_bwd_max = 0;     // the shared memory k_mix_bwd_g may take (0: not used)
   long P = 0;
   // parameters: FP32 masters, BF16 copies, gradients, Adam moments (one buffer each)
   long nparam = 0;
@@ -765,9 +863,16 @@ int backward(sac_fno* n, const bf16* dy) {
       GK(d);
     }
     {  // B3: mixing backward -> dZ, dR
-      const size_t sm = sizeof(float) * (2 * W * W + 4 * B * W);
-      k_mix_bwd<<<n->nmodes, 256, sm, n->st>>>(n->dpt, n->zt[l], n->wb + n->sRr[l].off, n->wb + n->sRi[l].off,
-                                               n->dzt, gw + n->sRr[l].off, gw + n->sRi[l].off, B, W, n->m2);
+      const size_t smg = sizeof(float) * kMixQ * (2 * W * W + 4 * B * W);
+      if (smg <= n->mix_bwd_max) {
+        k_mix_bwd_g<<<n->nmodes / kMixQ, 256, smg, n->st>>>(n->dpt, n->zt[l], n->wb + n->sRr[l].off,
+                                                           n->wb + n->sRi[l].off, n->dzt, gw + n->sRr[l].off,
+                                                           gw + n->sRi[l].off, B, W, n->m2);
+      } else {
+        const size_t sm = sizeof(float) * (2 * W * W + 4 * B * W);
+        k_mix_bwd<<<n->nmodes, 256, sm, n->st>>>(n->dpt, n->zt[l], n->wb + n->sRr[l].off, n->wb + n->sRi[l].off,
+                                                 n->dzt, gw + n->sRr[l].off, gw + n->sRi[l].off, B, W, n->m2);
+      }
       FK(cudaGetLastError());
     }
     {  // B2: dT[(b,c),j][s] = sum_r dZ[(b,c),j][r] Fx[r][s]  (rows s)
@@ -921,6 +1026,13 @@ int sac_fno_create(const sac_fno_config* cfg, sac_fno** out) {
                      cudaFuncSetAttribute(k_mix_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mix) ==
                          cudaSuccess;
     cudaGetLastError();  // a refused attribute leaves the per-mode form
+    // the grouped backward holds R, U and G of 8 modes for the training batch
+    const size_t mb = std::min<size_t>(227 * 1024, sizeof(float) * kMixQ *
+                                                       (2 * (size_t)n->W * n->W + 4 * (size_t)n->Bmax * n->W));
+    if ((2 * n->m1) % kMixQ == 0 &&
+        cudaFuncSetAttribute(k_mix_bwd_g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mb) == cudaSuccess)
+      n->mix_bwd_max = mb;
+    cudaGetLastError();
     const size_t one = sizeof(float) * (2 * (size_t)n->W * n->W + 2 * (size_t)n->Bmax * n->W);
     if (!n->mix_grouped &&
         cudaFuncSetAttribute(k_mix_fwd_mode, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)one) != cudaSuccess) {
